@@ -1,0 +1,197 @@
+/*
+ * mqw.h — C ABI of the B200-native multi-stage quantum-walk simulator.
+ *
+ * The reference (Asa-Hopkins/MultiStageQW) has no library API: its whole
+ * product is the command `MultiQW n m filename [start problems]`
+ * (MultiQW.cpp:241-458). This header exposes that path as plain C entry
+ * points — plain pointers and sizes, no CUDA or torch types — so that a host
+ * program in any language can bind it (ctypes, cgo, JNI, N-API). The
+ * `MultiQW` binary built from multistageqw_b200/csrc/multiqw_cli.cpp is the
+ * drop-in replacement of the reference command and sits on top of this ABI.
+ *
+ * Conventions
+ *  - Every call returns an mqw_status; nothing aborts the process.
+ *  - The caller owns host buffers; a context owns its device buffers.
+ *  - One context per host thread. Calls on one context are serialised by the
+ *    caller.
+ *  - Instance layout (MultiQW.cpp:270-323): per instance n(n+1)/2 float64
+ *    values; first the n(n-1)/2 couplings J(i,j) for i = 1..n-1, j = 0..i-1
+ *    in that loop order, then the n fields h(0..n-1).
+ *  - Ground-state probabilities are reported per instance as the mean over
+ *    the evaluated time samples (MultiQW.cpp:454).
+ */
+#ifndef MQW_H
+#define MQW_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MQW_ABI_VERSION 1
+#define MQW_SAMPLES 100  /* time samples per stage, MultiQW.cpp:257 */
+#define MQW_MAX_N 30     /* 2^30 amplitudes; the reference overflows at n >= 31 (MultiQW.cpp:246) */
+#define MQW_MAX_M 64     /* stages per walk */
+
+typedef enum mqw_status {
+  MQW_OK = 0,
+  MQW_ERR_INVALID = 1,     /* bad argument (n, m, count, null pointer, ...) */
+  MQW_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+  MQW_ERR_NOMEM = 3,       /* device or host allocation failed */
+  MQW_ERR_IO = 4,          /* instance file missing, unreadable or too short */
+  MQW_ERR_TIMEOUT = 5,     /* a device-side bounded wait gave up */
+  MQW_ERR_UNSUPPORTED = 6, /* configuration not supported by this build */
+  MQW_ERR_NO_DEVICE = 7    /* no CUDA device, or the device is not sm_100 */
+} mqw_status;
+
+typedef enum mqw_precision {
+  MQW_FP32 = 0, /* complex64 state, FP32 recurrence (the reference's precision) */
+  MQW_FP64 = 1  /* complex128 state, FP64 recurrence (the GPU oracle) */
+} mqw_precision;
+
+typedef struct mqw_options {
+  int precision;   /* mqw_precision, default MQW_FP32 */
+  int samples;     /* samples evaluated per instance, 1..100, default 100.
+                      The time draws are always the reference's 100 per
+                      stage; fewer samples evaluates the first ones. */
+  double cheb_tol; /* Chebyshev tail tolerance, default 1e-6 (MultiQW.cpp:440) */
+  int group;       /* trajectories per grid-path launch, 0 = autotuned */
+  int resident_max_n; /* largest n run with a whole state in one CTA's shared
+                         memory, 0 = default (13 for FP32, 12 for FP64) */
+  const float* stage_scale; /* optional [count][m][2] multipliers applied to
+                               (gamma_i, t_i) of each stage (a learned
+                               schedule); NULL = the paper heuristic */
+} mqw_options;
+
+typedef struct mqw_diag_info {
+  double e0;     /* lowest energy (reference arithmetic)           */
+  double emax;   /* highest energy                                  */
+  double mid;    /* (emax + e0) / 2, subtracted from H_P            */
+  float e_abs;   /* (emax - e0) / 2, the spectral half-width        */
+  uint32_t e_loc;/* ground-state index, first minimum in Gray order */
+} mqw_diag_info;
+
+typedef struct mqw_run_stats {
+  long long instances;
+  long long trajectories;   /* instance x sample walks */
+  long long terms;          /* summed Chebyshev degree over all stages */
+  double term_amps;         /* sum over trajectories and stages of K * 2^n */
+  long long launches;       /* kernels launched by the library */
+  long long term_launches;  /* grid-path Clenshaw-term launches */
+  double kernel_ms;         /* device time of the propagation phase (CUDA
+                               events on the launching stream) */
+  double h2d_bytes;         /* host-to-device bytes copied by the plan */
+  double d2h_bytes;         /* device-to-host bytes copied by the plan */
+} mqw_run_stats;
+
+typedef struct mqw_ctx mqw_ctx;
+typedef struct mqw_plan mqw_plan;
+
+/* ---- context --------------------------------------------------------- */
+
+/* Create a context on CUDA device `device`. Fails with MQW_ERR_NO_DEVICE if
+ * the device is absent or not a Blackwell sm_100 part. */
+mqw_status mqw_create(mqw_ctx** ctx, int device);
+void mqw_destroy(mqw_ctx* ctx);
+/* Message of the last failing call on this context (never NULL). */
+const char* mqw_last_error(const mqw_ctx* ctx);
+const char* mqw_status_string(mqw_status s);
+void mqw_default_options(mqw_options* opt);
+int mqw_abi_version(void);
+
+/* ---- host-side pieces (no GPU needed) ------------------------------------ */
+
+/* Upper-tail normal quantile Phi^{-1}(1-p) as float.
+ * Replaces my_normcdfinvf (MultiQW.cpp:80-86). */
+float mqw_inv_norm_upper(float p);
+
+/* Couplings (n*n, symmetric, halved: J(i,j) = float(raw)/2) and fields.
+ * Replaces the instance unpacking of MultiQW.cpp:306-323. */
+mqw_status mqw_load_instance(int n, const double* raw, float* J, float* h);
+
+/* Per-stage hopping rates gamma[m], first-stage-exact time lower bounds
+ * short_t[m], the 100 time samples per stage times[m][100] (libstdc++
+ * std::mt19937 seeded 29552825458725, re-seeded per instance) and
+ * total_t = sum(short_t). For m == 1 the times are sorted and differenced
+ * (cumulative evolution). Replaces MultiQW.cpp:365-430. */
+mqw_status mqw_schedule(int n, int m, const double* raw, float* gammas,
+                        float* short_t, float* times, float* total_t);
+
+/* Read `problems` instances starting at instance `start` from a reference
+ * instance file. Unlike the reference (which silently repeats the previous
+ * instance past the end of the file, MultiQW.cpp:303), a short file is an
+ * MQW_ERR_IO. Replaces MultiQW.cpp:268-271, 303-304. */
+mqw_status mqw_read_instances(const char* filename, int n, long long start,
+                              long long problems, double* raw_out);
+
+/* ---- device pieces ------------------------------------------------------- */
+
+/* Ising diagonal of one instance on the GPU with the reference's arithmetic
+ * (float Gray-code increments accumulated in double, MultiQW.cpp:325-362):
+ * hp[2^n] = float(E) - float(mid) (nullable), energies[2^n] in double
+ * (nullable), and the ground-state index / spectral bounds in *info. */
+mqw_status mqw_build_diag(mqw_ctx* ctx, int n, const double* raw, float* hp,
+                          double* energies, mqw_diag_info* info);
+
+/* Chebyshev coefficients of exp(i s x) on [-1,1] computed on the GPU in FP64
+ * (Jacobi–Anger, tail-sum truncation at `tol`), cast to float:
+ * coeffs[count][max_k], degrees[count]. Replaces the call to
+ * Chebyshev<double>::RCF_odd_even(f, 1e-6) at MultiQW.cpp:436-440. */
+mqw_status mqw_cheb_coeffs(mqw_ctx* ctx, int count, const double* s,
+                           double tol, int max_k, float* coeffs, int* degrees);
+
+/* One Clenshaw propagation out = sum_k c_k T_k(H~) psi on the GPU, with
+ * H~ = (hp - gamma * sum_q X_q) / scale, real c_k for even k and imaginary
+ * for odd k. psi/out are interleaved complex (re, im) of 2^n amplitudes
+ * (float for MQW_FP32, double for MQW_FP64 in `precision`); hp is float.
+ * Replaces Clenshaw (MultiQW.cpp:177-236). */
+mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
+                        const float* coeffs, const float* hp, float gamma,
+                        float scale, const void* psi, void* out);
+
+/* ---- the whole path -------------------------------------------------- */
+
+/* For `count` instances of n spins and m stages in the reference's layout
+ * (raw = count * n(n+1)/2 doubles, host memory): ground-state probability
+ * per instance (p_out, double), total_t per instance (nullable) and the
+ * ground-state index per instance (nullable). opt may be NULL (defaults).
+ * Replaces the problem loop of MultiQW.cpp:296-456. */
+mqw_status mqw_run_problems(mqw_ctx* ctx, int n, int m, const double* raw,
+                            int count, const mqw_options* opt, double* p_out,
+                            float* total_t_out, uint32_t* e_loc_out,
+                            mqw_run_stats* stats);
+
+/* Plans separate host preparation from device execution so a batch can be
+ * executed repeatedly with its inputs resident in device memory. Instances
+ * may have different n and m: n[i], m[i], and raw holds each instance's
+ * n_i(n_i+1)/2 values back to back. */
+mqw_status mqw_plan_create(mqw_ctx* ctx, int count, const int* n,
+                           const int* m, const double* raw,
+                           const mqw_options* opt, mqw_plan** plan);
+/* Run the batch on `stream` (a cudaStream_t, NULL = the context's stream);
+ * returns after the work is queued and the degree read-back it needs. */
+mqw_status mqw_plan_execute(mqw_plan* plan, void* stream);
+/* Copy results to the host (waits for the plan's stream). Any pointer may be
+ * NULL. p_sample (nullable) receives count*samples per-sample values. */
+mqw_status mqw_plan_results(mqw_plan* plan, double* p_out, float* total_t,
+                            uint32_t* e_loc, double* p_sample);
+mqw_status mqw_plan_stats(const mqw_plan* plan, mqw_run_stats* stats);
+void mqw_plan_destroy(mqw_plan* plan);
+
+/* ---- the reference command -------------------------------------------- */
+
+/* Equivalent of `MultiQW n m filename [start problems]` (MultiQW.cpp:241-458):
+ * reads the instances, runs them, prints "total_t P" per problem to stdout
+ * (when print != 0) and appends one float32 per problem to
+ * <out_dir>/output_<n>_<m> (out_dir NULL = current directory). */
+mqw_status mqw_multiqw(mqw_ctx* ctx, int n, int m, const char* filename,
+                       long long start, long long problems,
+                       const char* out_dir, int print);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MQW_H */

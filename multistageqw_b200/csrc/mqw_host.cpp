@@ -1,0 +1,820 @@
+// Host runtime of the C ABI (include/mqw.h): contexts, plans and the launch
+// schedule of the propagation.
+//
+// A plan turns a batch of instances into device work:
+//   1. diagonal   : per n-group, launch_diag (reference-exact energies,
+//                   E_loc, E_abs) into a pooled hp buffer;
+//   2. degrees    : one FP64 thread per (instance, stage, sample) job;
+//                   degrees and onenorms are read back (the only host sync
+//                   inside execute) to lay out the coefficient pool and the
+//                   launch schedule;
+//   3. coefficients: written packed into the pool;
+//   4. propagation: walks with n <= resident_max_n run in one launch of the
+//                   resident kernel (a CTA per walk); larger n run on the
+//                   grid path, one launch per Clenshaw term over groups of up
+//                   to 8 walks of the same n;
+//   5. means      : mean ground-state probability per instance.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/mqw.h"
+#include "mqw_cheb.h"
+#include "mqw_internal.h"
+
+using namespace mqw;
+
+struct mqw_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int sm_count = 0;
+};
+
+namespace {
+
+mqw_status fail(mqw_ctx* ctx, mqw_status s, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    ctx->err = buf;
+  }
+  return s;
+}
+
+#define CK(call)                                                            \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess)                                                  \
+      return fail(ctx, e_ == cudaErrorMemoryAllocation ? MQW_ERR_NOMEM      \
+                                                       : MQW_ERR_CUDA,      \
+                  "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),   \
+                  __FILE__, __LINE__);                                      \
+  } while (0)
+
+// Owning device allocation.
+struct DevMem {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevMem() = default;
+  DevMem(const DevMem&) = delete;
+  DevMem& operator=(const DevMem&) = delete;
+  ~DevMem() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes && p) return cudaSuccess;
+    release();
+    if (b == 0) b = 16;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+int params_per(int n) { return n * (n + 1) / 2; }
+
+void default_opts(mqw_options* o) {
+  o->precision = MQW_FP32;
+  o->samples = MQW_SAMPLES;
+  o->cheb_tol = 1e-6;
+  o->group = 0;
+  o->resident_max_n = 0;
+  o->stage_scale = nullptr;
+}
+
+}  // namespace
+
+struct mqw_plan {
+  mqw_ctx* ctx = nullptr;
+  mqw_options opt{};
+  int count = 0;
+  int precision = 0;
+  int samples = MQW_SAMPLES;
+  std::vector<int> n, m;                 // per instance (caller order)
+  std::vector<int> order;                // instances sorted by n (stable)
+  std::vector<float> total_t;            // caller order
+  // Device inputs (sorted order).
+  std::vector<long long> raw_off;        // doubles offset per sorted instance
+  std::vector<long long> hp_off;         // hp offset per sorted instance
+  std::vector<int> p_off;                // p_sample offset per sorted instance
+  DevMem d_raw, d_hp, d_diag, d_diag_scratch;
+  // Jobs: one per (walk, stage) in walk-major order.
+  std::vector<CoefJob> jobs;
+  std::vector<ResidentWalk> walks;       // all walks (resident and grid)
+  std::vector<int> walk_is_grid;
+  DevMem d_jobs, d_degree, d_onenorm, d_coef_off, d_coef, d_stages, d_walks;
+  DevMem d_p_sample, d_p_mean, d_p_off, d_p_cnt;
+  // Grid-path buffers.
+  DevMem d_state, d_norm_part, d_kappa;
+  // Host copies of the degree read-back.
+  std::vector<int> degree;
+  std::vector<float> onenorm;
+  std::vector<long long> coef_off;
+  mqw_run_stats stats{};
+  bool executed = false;
+  // Propagation-phase timing (recorded on the launching stream).
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  bool timed = false;
+  double create_h2d = 0.0;  // bytes uploaded by plan_create
+  ~mqw_plan() {
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+  }
+};
+
+namespace {
+
+mqw_status check_ctx(mqw_ctx* ctx) {
+  if (!ctx) return MQW_ERR_INVALID;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess)
+    return fail(ctx, MQW_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  return MQW_OK;
+}
+
+int choose_group(const mqw_plan& P, int n) {
+  if (P.opt.group > 0) return std::min(P.opt.group, kMaxGroup);
+  const size_t amp = P.precision == 0 ? 8 : 16;
+  const size_t walk_bytes = 3 * amp * ((size_t)1 << n);
+  // Keep a launch's states within about 96 MB so they stay resident in the
+  // 126 MB L2 between terms, but give every launch at least ~2^20 amplitudes.
+  size_t g = (96u << 20) / walk_bytes;
+  if (((size_t)1 << n) * g < ((size_t)1 << 20)) g = ((size_t)1 << 20) >> n;
+  if (g < 1) g = 1;
+  if (g > (size_t)kMaxGroup) g = kMaxGroup;
+  return (int)g;
+}
+
+// Runs the grid-path walks with index in [w0, w1) (all the same n).
+mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
+                          cudaStream_t stream) {
+  mqw_ctx* ctx = P.ctx;
+  const int n = P.walks[widx[0]].n;
+  const size_t N = (size_t)1 << n;
+  const int lt = std::min(n, kMaxTileLog);
+  const int tiles = (int)(N >> lt);
+  const int G = (int)widx.size();
+  const size_t amp = P.precision == 0 ? 8 : 16;
+  char* base = P.d_state.as<char>();
+  auto buf = [&](int g, int k) -> void* {
+    return base + ((size_t)g * 3 + k) * N * amp;
+  };
+  // Roles: psi = slot pi[g], b_r lives in slot x[g] for even r, y[g] for odd.
+  int pi[kMaxGroup], xs[kMaxGroup], ys[kMaxGroup];
+  for (int g = 0; g < G; g++) {
+    pi[g] = 0;
+    xs[g] = 1;
+    ys[g] = 2;
+    CK(launch_uniform(P.precision, buf(g, pi[g]), n, stream));
+    P.stats.launches++;
+  }
+  double* norm_part = P.d_norm_part.as<double>();
+  double* kappa = P.d_kappa.as<double>();
+  double* p_sample = P.d_p_sample.as<double>();
+  const float* coef = P.d_coef.as<float>();
+  const float* hp = P.d_hp.as<float>();
+  const DiagOut* diag = P.d_diag.as<DiagOut>();
+  int max_stages = 0;
+  for (int g = 0; g < G; g++) max_stages = std::max(max_stages, P.walks[widx[g]].stages);
+  for (int st = 0; st < max_stages; st++) {
+    int K[kMaxGroup], Kmax = 0;
+    for (int g = 0; g < G; g++) {
+      const ResidentWalk& w = P.walks[widx[g]];
+      K[g] = st < w.stages ? P.degree[w.stage_desc_off + st] : 0;
+      Kmax = std::max(Kmax, K[g]);
+    }
+    for (int r = Kmax - 1; r >= 0; r--) {
+      TermParams tp{};
+      tp.n = n;
+      tp.lt = lt;
+      tp.count = G;
+      for (int g = 0; g < G; g++) {
+        TermTraj& T = tp.traj[g];
+        const ResidentWalk& w = P.walks[widx[g]];
+        if (r >= K[g]) {
+          T.mode = kSkip;
+          continue;
+        }
+        const int job = w.stage_desc_off + st;
+        T.mode = (r == K[g] - 1) ? kFirst : (r == K[g] - 2) ? kSecond : kFull;
+        T.b1 = buf(g, ((r + 1) & 1) ? ys[g] : xs[g]);
+        T.b2 = buf(g, (r & 1) ? ys[g] : xs[g]);
+        T.psi = buf(g, pi[g]);
+        T.hp = hp + w.hp_off;
+        T.coef = coef + P.coef_off[job] + r;
+        T.kappa = st == 0 ? nullptr : kappa + g;
+        T.norm_part = norm_part + (size_t)g * tiles;
+        T.gamma = P.jobs[job].gamma;
+        T.scale = P.onenorm[job];
+        T.odd = r & 1;
+        T.final_term = r == 0;
+        P.stats.term_amps += (double)N;
+      }
+      CK(launch_term(P.precision, tp, stream));
+      P.stats.launches++;
+      P.stats.term_launches++;
+    }
+    FinalParams fp{};
+    int fc = 0;
+    for (int g = 0; g < G; g++) {
+      const ResidentWalk& w = P.walks[widx[g]];
+      if (st >= w.stages) continue;
+      FinalTraj& F = fp.traj[fc++];
+      F.norm_part = norm_part + (size_t)g * tiles;
+      F.tiles = tiles;
+      F.kappa = kappa + g;
+      F.out = buf(g, xs[g]);
+      F.diag = diag + w.inst;
+      F.p_out = (w.record_each || st == w.stages - 1)
+                    ? p_sample + w.p_off + (w.record_each ? st : 0)
+                    : nullptr;
+    }
+    fp.count = fc;
+    CK(launch_finalize(P.precision, fp, stream));
+    P.stats.launches++;
+    for (int g = 0; g < G; g++) {
+      if (st >= P.walks[widx[g]].stages) continue;
+      std::swap(pi[g], xs[g]);  // the output (slot x) becomes psi
+    }
+  }
+  return MQW_OK;
+}
+
+mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
+  mqw_ctx* ctx = P.ctx;
+  const int count = P.count;
+  // 1. Diagonals, per group of equal n (instances are sorted by n).
+  DiagOut* d_diag = P.d_diag.as<DiagOut>();
+  for (int s = 0; s < count;) {
+    const int n = P.n[P.order[s]];
+    int e = s;
+    while (e < count && P.n[P.order[e]] == n) e++;
+    CK(launch_diag(n, e - s, P.d_raw.as<double>() + P.raw_off[s],
+                   P.d_hp.as<float>() + P.hp_off[s], nullptr, d_diag + s,
+                   P.d_diag_scratch.p, stream));
+    P.stats.launches += 3;
+    s = e;
+  }
+  // 2. Degrees and onenorms, read back.
+  const int nj = (int)P.jobs.size();
+  CK(launch_cheb_degree(P.d_jobs.as<CoefJob>(), nj, d_diag, P.opt.cheb_tol,
+                        P.d_degree.as<int>(), P.d_onenorm.as<float>(), stream));
+  P.stats.launches++;
+  P.degree.resize(nj);
+  P.onenorm.resize(nj);
+  CK(cudaMemcpyAsync(P.degree.data(), P.d_degree.p, nj * sizeof(int),
+                     cudaMemcpyDeviceToHost, stream));
+  P.stats.d2h_bytes += (double)nj * (sizeof(int) + sizeof(float));
+  CK(cudaMemcpyAsync(P.onenorm.data(), P.d_onenorm.p, nj * sizeof(float),
+                     cudaMemcpyDeviceToHost, stream));
+  CK(cudaStreamSynchronize(stream));
+  // 3. Coefficient pool.
+  P.coef_off.assign(nj + 1, 0);
+  P.stats.terms = 0;
+  for (int j = 0; j < nj; j++) {
+    if (P.degree[j] < 1)
+      return fail(ctx, MQW_ERR_INVALID,
+                  "Chebyshev degree failed for job %d (non-finite time?)", j);
+    P.coef_off[j + 1] = P.coef_off[j] + P.degree[j];
+    P.stats.terms += P.degree[j];
+  }
+  CK(P.d_coef_off.ensure((nj + 1) * sizeof(long long)));
+  CK(cudaMemcpyAsync(P.d_coef_off.p, P.coef_off.data(),
+                     (nj + 1) * sizeof(long long), cudaMemcpyHostToDevice,
+                     stream));
+  P.stats.h2d_bytes += (double)(nj + 1) * sizeof(long long) + (double)nj * sizeof(StageDesc);
+  CK(P.d_coef.ensure(P.coef_off[nj] * sizeof(float)));
+  CK(launch_cheb_coeffs(P.d_jobs.as<CoefJob>(), nj, d_diag, P.opt.cheb_tol,
+                        P.d_coef_off.as<long long>(), P.d_coef.as<float>(),
+                        stream));
+  P.stats.launches++;
+  // 4a. Resident walks.
+  if (!P.ev0) CK(cudaEventCreate(&P.ev0));
+  if (!P.ev1) CK(cudaEventCreate(&P.ev1));
+  CK(cudaEventRecord(P.ev0, stream));
+  std::vector<StageDesc> sdesc(nj);
+  for (int j = 0; j < nj; j++) {
+    sdesc[j].coef_off = P.coef_off[j];
+    sdesc[j].K = P.degree[j];
+    sdesc[j].gamma = P.jobs[j].gamma;
+    sdesc[j].onenorm = P.onenorm[j];
+  }
+  CK(P.d_stages.ensure(nj * sizeof(StageDesc)));
+  CK(cudaMemcpyAsync(P.d_stages.p, sdesc.data(), nj * sizeof(StageDesc),
+                     cudaMemcpyHostToDevice, stream));
+  std::vector<ResidentWalk> res;
+  int res_max_n = 0;
+  std::map<int, std::vector<int>> grid_by_n;
+  for (size_t w = 0; w < P.walks.size(); w++) {
+    if (P.walk_is_grid[w]) {
+      grid_by_n[P.walks[w].n].push_back((int)w);
+    } else {
+      res.push_back(P.walks[w]);
+      res_max_n = std::max(res_max_n, P.walks[w].n);
+    }
+  }
+  P.stats.term_amps = 0;
+  for (size_t w = 0; w < P.walks.size(); w++) {
+    if (P.walk_is_grid[w]) continue;
+    for (int st = 0; st < P.walks[w].stages; st++)
+      P.stats.term_amps += (double)P.degree[P.walks[w].stage_desc_off + st] *
+                           (double)(1u << P.walks[w].n);
+  }
+  if (!res.empty()) {
+    CK(P.d_walks.ensure(res.size() * sizeof(ResidentWalk)));
+    CK(cudaMemcpyAsync(P.d_walks.p, res.data(), res.size() * sizeof(ResidentWalk),
+                       cudaMemcpyHostToDevice, stream));
+    P.stats.h2d_bytes += (double)res.size() * sizeof(ResidentWalk);
+    CK(launch_resident(P.precision, P.d_walks.as<ResidentWalk>(), (int)res.size(),
+                       res_max_n, P.d_stages.as<StageDesc>(),
+                       P.d_coef.as<float>(), P.d_hp.as<float>(), d_diag,
+                       P.d_p_sample.as<double>(), stream));
+    P.stats.launches++;
+  }
+  // 4b. Grid walks, in groups of equal n.
+  for (auto& kv : grid_by_n) {
+    const int n = kv.first;
+    const int G = choose_group(P, n);
+    const size_t N = (size_t)1 << n;
+    const size_t amp = P.precision == 0 ? 8 : 16;
+    const int lt = std::min(n, kMaxTileLog);
+    CK(P.d_state.ensure((size_t)G * 3 * N * amp));
+    CK(P.d_norm_part.ensure((size_t)G * (N >> lt) * sizeof(double)));
+    CK(P.d_kappa.ensure(kMaxGroup * sizeof(double)));
+    const std::vector<int>& ws = kv.second;
+    for (size_t i = 0; i < ws.size(); i += G) {
+      std::vector<int> grp(ws.begin() + i, ws.begin() + std::min(ws.size(), i + G));
+      mqw_status s = run_grid_group(P, grp, stream);
+      if (s != MQW_OK) return s;
+    }
+  }
+  CK(cudaEventRecord(P.ev1, stream));
+  P.timed = true;
+  // 5. Means per instance (sorted order).
+  CK(launch_mean(P.d_p_sample.as<double>(), P.d_p_off.as<int>(),
+                 P.d_p_cnt.as<int>(), count, P.d_p_mean.as<double>(), stream));
+  P.stats.launches++;
+  P.executed = true;
+  return MQW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mqw_abi_version(void) { return MQW_ABI_VERSION; }
+
+const char* mqw_status_string(mqw_status s) {
+  switch (s) {
+    case MQW_OK: return "ok";
+    case MQW_ERR_INVALID: return "invalid argument";
+    case MQW_ERR_CUDA: return "CUDA error";
+    case MQW_ERR_NOMEM: return "out of memory";
+    case MQW_ERR_IO: return "I/O error";
+    case MQW_ERR_TIMEOUT: return "device wait timed out";
+    case MQW_ERR_UNSUPPORTED: return "unsupported";
+    case MQW_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+  }
+  return "unknown status";
+}
+
+void mqw_default_options(mqw_options* opt) {
+  if (opt) default_opts(opt);
+}
+
+mqw_status mqw_create(mqw_ctx** out, int device) {
+  if (!out) return MQW_ERR_INVALID;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev)
+    return MQW_ERR_NO_DEVICE;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return MQW_ERR_NO_DEVICE;
+  if (prop.major != 10) return MQW_ERR_NO_DEVICE;  // built for sm_100a only
+  if (cudaSetDevice(device) != cudaSuccess) return MQW_ERR_NO_DEVICE;
+  std::unique_ptr<mqw_ctx> ctx(new mqw_ctx);
+  ctx->device = device;
+  ctx->sm_count = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return MQW_ERR_CUDA;
+  *out = ctx.release();
+  return MQW_OK;
+}
+
+void mqw_destroy(mqw_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+const char* mqw_last_error(const mqw_ctx* ctx) {
+  if (!ctx) return "null context";
+  return ctx->err.c_str();
+}
+
+mqw_status mqw_read_instances(const char* filename, int n, long long start,
+                              long long problems, double* raw_out) {
+  if (!filename || n < 1 || n > MQW_MAX_N || start < 0 || problems < 0 ||
+      (problems > 0 && !raw_out))
+    return MQW_ERR_INVALID;
+  FILE* f = fopen(filename, "rb");
+  if (!f) return MQW_ERR_IO;
+  const long long per = params_per(n);
+  if (fseeko(f, (off_t)(start * per * 8), SEEK_SET) != 0) {
+    fclose(f);
+    return MQW_ERR_IO;
+  }
+  const size_t want = (size_t)(problems * per);
+  const size_t got = fread(raw_out, sizeof(double), want, f);
+  fclose(f);
+  return got == want ? MQW_OK : MQW_ERR_IO;
+}
+
+mqw_status mqw_plan_create(mqw_ctx* ctx, int count, const int* n, const int* m,
+                           const double* raw, const mqw_options* opt_in,
+                           mqw_plan** out) {
+  mqw_status s = check_ctx(ctx);
+  if (s != MQW_OK) return s;
+  if (!out || count < 1 || !n || !m || !raw)
+    return fail(ctx, MQW_ERR_INVALID, "plan_create: bad arguments");
+  mqw_options opt;
+  default_opts(&opt);
+  if (opt_in) opt = *opt_in;
+  if (opt.precision != MQW_FP32 && opt.precision != MQW_FP64)
+    return fail(ctx, MQW_ERR_INVALID, "precision must be MQW_FP32 or MQW_FP64");
+  if (opt.samples < 1 || opt.samples > MQW_SAMPLES)
+    return fail(ctx, MQW_ERR_INVALID, "samples must be in 1..100");
+  if (!(opt.cheb_tol > 0.0) || opt.cheb_tol >= 1.0)
+    return fail(ctx, MQW_ERR_INVALID, "cheb_tol must be in (0, 1)");
+  for (int i = 0; i < count; i++) {
+    if (n[i] < 1 || n[i] > MQW_MAX_N)
+      return fail(ctx, MQW_ERR_INVALID, "instance %d: n=%d outside 1..%d", i, n[i], MQW_MAX_N);
+    if (m[i] < 1 || m[i] > MQW_MAX_M)
+      return fail(ctx, MQW_ERR_INVALID, "instance %d: m=%d outside 1..%d", i, m[i], MQW_MAX_M);
+  }
+  std::unique_ptr<mqw_plan> P(new mqw_plan);
+  P->ctx = ctx;
+  P->opt = opt;
+  P->count = count;
+  P->precision = opt.precision;
+  P->samples = opt.samples;
+  P->n.assign(n, n + count);
+  P->m.assign(m, m + count);
+  P->total_t.assign(count, 0.0f);
+  std::vector<long long> caller_off(count + 1, 0);
+  for (int i = 0; i < count; i++) caller_off[i + 1] = caller_off[i] + params_per(n[i]);
+  P->order.resize(count);
+  std::iota(P->order.begin(), P->order.end(), 0);
+  std::stable_sort(P->order.begin(), P->order.end(),
+                   [&](int a, int b) { return n[a] < n[b]; });
+  // Raw inputs in sorted order; hp pool offsets; schedules on the host.
+  std::vector<double> raw_sorted;
+  raw_sorted.reserve(caller_off[count]);
+  P->raw_off.resize(count);
+  P->hp_off.resize(count);
+  P->p_off.resize(count);
+  long long hp_total = 0;
+  std::vector<int> p_cnt(count);
+  const int res_max =
+      opt.resident_max_n < 0 ? 0
+      : opt.resident_max_n == 0 ? resident_max_n(opt.precision)
+      : std::min(opt.resident_max_n, resident_max_n(opt.precision));
+  int p_total = 0;
+  std::vector<float> gam(MQW_MAX_M), st(MQW_MAX_M), times(MQW_MAX_M * MQW_SAMPLES);
+  for (int k = 0; k < count; k++) {
+    const int i = P->order[k];
+    const int ni = n[i], mi = m[i];
+    P->raw_off[k] = (long long)raw_sorted.size();
+    raw_sorted.insert(raw_sorted.end(), raw + caller_off[i], raw + caller_off[i + 1]);
+    P->hp_off[k] = hp_total;
+    hp_total += 1ll << ni;
+    float tot = 0.0f;
+    mqw_schedule(ni, mi, raw + caller_off[i], gam.data(), st.data(), times.data(), &tot);
+    P->total_t[i] = tot;
+    if (opt.stage_scale) {
+      for (int s2 = 0; s2 < mi; s2++) {
+        const float fg = opt.stage_scale[((size_t)i * mi + s2) * 2 + 0];
+        const float ft = opt.stage_scale[((size_t)i * mi + s2) * 2 + 1];
+        if (!(fg > 0.0f) || !(ft > 0.0f) || !std::isfinite(fg) || !std::isfinite(ft))
+          return fail(ctx, MQW_ERR_INVALID, "stage_scale must be positive and finite");
+        gam[s2] *= fg;
+        for (int j = 0; j < MQW_SAMPLES; j++) times[s2 * MQW_SAMPLES + j] *= ft;
+      }
+    }
+    P->p_off[k] = p_total;
+    p_cnt[k] = opt.samples;
+    p_total += opt.samples;
+    const bool grid = ni > res_max;
+    auto add_walk = [&](int stages, int record_each, int p_at) {
+      ResidentWalk w;
+      w.inst = k;
+      w.n = ni;
+      w.stages = stages;
+      w.record_each = record_each;
+      w.stage_desc_off = (int)P->jobs.size();
+      w.p_off = p_at;
+      w.hp_off = P->hp_off[k];
+      P->walks.push_back(w);
+      P->walk_is_grid.push_back(grid ? 1 : 0);
+    };
+    if (mi == 1) {
+      // One cumulative walk over the sorted, differenced times.
+      add_walk(opt.samples, 1, P->p_off[k]);
+      for (int j = 0; j < opt.samples; j++)
+        P->jobs.push_back(CoefJob{k, ni, gam[0], times[j]});
+    } else {
+      for (int j = 0; j < opt.samples; j++) {
+        add_walk(mi, 0, P->p_off[k] + j);
+        for (int s2 = 0; s2 < mi; s2++)
+          P->jobs.push_back(CoefJob{k, ni, gam[s2], times[s2 * MQW_SAMPLES + j]});
+      }
+    }
+  }
+  P->stats.instances = count;
+  P->create_h2d = (double)raw_sorted.size() * sizeof(double) + (double)P->jobs.size() * sizeof(CoefJob) +
+                  2.0 * count * sizeof(int);
+  P->stats.trajectories = (long long)p_total;
+  // Uploads.
+  cudaStream_t stream = ctx->stream;
+  CK(P->d_raw.ensure(raw_sorted.size() * sizeof(double)));
+  CK(cudaMemcpyAsync(P->d_raw.p, raw_sorted.data(), raw_sorted.size() * sizeof(double),
+                     cudaMemcpyHostToDevice, stream));
+  CK(P->d_hp.ensure((size_t)hp_total * sizeof(float)));
+  CK(P->d_diag.ensure(count * sizeof(DiagOut)));
+  size_t scratch = 0;
+  for (int k = 0; k < count;) {
+    const int ni = n[P->order[k]];
+    int e = k;
+    while (e < count && n[P->order[e]] == ni) e++;
+    scratch = std::max(scratch, diag_scratch_bytes(ni, e - k));
+    k = e;
+  }
+  CK(P->d_diag_scratch.ensure(scratch));
+  const size_t nj = P->jobs.size();
+  CK(P->d_jobs.ensure(nj * sizeof(CoefJob)));
+  CK(cudaMemcpyAsync(P->d_jobs.p, P->jobs.data(), nj * sizeof(CoefJob),
+                     cudaMemcpyHostToDevice, stream));
+  CK(P->d_degree.ensure(nj * sizeof(int)));
+  CK(P->d_onenorm.ensure(nj * sizeof(float)));
+  CK(P->d_p_sample.ensure((size_t)p_total * sizeof(double)));
+  CK(P->d_p_mean.ensure(count * sizeof(double)));
+  CK(P->d_p_off.ensure(count * sizeof(int)));
+  CK(P->d_p_cnt.ensure(count * sizeof(int)));
+  CK(cudaMemcpyAsync(P->d_p_off.p, P->p_off.data(), count * sizeof(int),
+                     cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(P->d_p_cnt.p, p_cnt.data(), count * sizeof(int),
+                     cudaMemcpyHostToDevice, stream));
+  CK(cudaStreamSynchronize(stream));
+  *out = P.release();
+  return MQW_OK;
+}
+
+mqw_status mqw_plan_execute(mqw_plan* plan, void* stream) {
+  if (!plan) return MQW_ERR_INVALID;
+  mqw_ctx* ctx = plan->ctx;
+  mqw_status s = check_ctx(ctx);
+  if (s != MQW_OK) return s;
+  cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+  plan->stats.h2d_bytes = 0;
+  plan->stats.d2h_bytes = 0;
+  plan->stats.launches = 0;
+  plan->stats.term_launches = 0;
+  plan->timed = false;
+  return plan_execute(*plan, st);
+}
+
+mqw_status mqw_plan_results(mqw_plan* plan, double* p_out, float* total_t,
+                            uint32_t* e_loc, double* p_sample) {
+  if (!plan) return MQW_ERR_INVALID;
+  mqw_ctx* ctx = plan->ctx;
+  mqw_status s = check_ctx(ctx);
+  if (s != MQW_OK) return s;
+  if (!plan->executed) return fail(ctx, MQW_ERR_INVALID, "plan not executed");
+  CK(cudaDeviceSynchronize());
+  const int count = plan->count;
+  std::vector<double> pm(count);
+  std::vector<DiagOut> dg(count);
+  CK(cudaMemcpy(pm.data(), plan->d_p_mean.p, count * sizeof(double), cudaMemcpyDeviceToHost));
+  plan->stats.d2h_bytes += (double)count * (sizeof(double) + sizeof(DiagOut));
+  CK(cudaMemcpy(dg.data(), plan->d_diag.p, count * sizeof(DiagOut), cudaMemcpyDeviceToHost));
+  std::vector<double> ps;
+  if (p_sample) {
+    ps.resize((size_t)count * plan->samples);
+    CK(cudaMemcpy(ps.data(), plan->d_p_sample.p, ps.size() * sizeof(double),
+                  cudaMemcpyDeviceToHost));
+    plan->stats.d2h_bytes += (double)ps.size() * sizeof(double);
+  }
+  for (int k = 0; k < count; k++) {
+    const int i = plan->order[k];
+    if (p_out) p_out[i] = pm[k];
+    if (e_loc) e_loc[i] = dg[k].e_loc;
+    if (p_sample)
+      std::copy(ps.begin() + plan->p_off[k], ps.begin() + plan->p_off[k] + plan->samples,
+                p_sample + (size_t)i * plan->samples);
+  }
+  if (total_t)
+    for (int i = 0; i < count; i++) total_t[i] = plan->total_t[i];
+  return MQW_OK;
+}
+
+mqw_status mqw_plan_stats(const mqw_plan* plan, mqw_run_stats* stats) {
+  if (!plan || !stats) return MQW_ERR_INVALID;
+  *stats = plan->stats;
+  stats->h2d_bytes += plan->create_h2d;
+  if (plan->timed) {
+    float ms = 0.0f;
+    if (cudaEventSynchronize(plan->ev1) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, plan->ev0, plan->ev1) == cudaSuccess)
+      stats->kernel_ms = ms;
+  }
+  return MQW_OK;
+}
+
+void mqw_plan_destroy(mqw_plan* plan) {
+  if (!plan) return;
+  if (plan->ctx) cudaSetDevice(plan->ctx->device);
+  delete plan;
+}
+
+mqw_status mqw_run_problems(mqw_ctx* ctx, int n, int m, const double* raw,
+                            int count, const mqw_options* opt, double* p_out,
+                            float* total_t_out, uint32_t* e_loc_out,
+                            mqw_run_stats* stats) {
+  mqw_status s = check_ctx(ctx);
+  if (s != MQW_OK) return s;
+  if (count < 0 || !raw || (count > 0 && !p_out))
+    return fail(ctx, MQW_ERR_INVALID, "run_problems: bad arguments");
+  if (count == 0) return MQW_OK;
+  std::vector<int> nv(count, n), mv(count, m);
+  mqw_plan* plan = nullptr;
+  s = mqw_plan_create(ctx, count, nv.data(), mv.data(), raw, opt, &plan);
+  if (s != MQW_OK) return s;
+  s = mqw_plan_execute(plan, nullptr);
+  if (s == MQW_OK) s = mqw_plan_results(plan, p_out, total_t_out, e_loc_out, nullptr);
+  if (s == MQW_OK && stats) mqw_plan_stats(plan, stats);
+  mqw_plan_destroy(plan);
+  return s;
+}
+
+mqw_status mqw_build_diag(mqw_ctx* ctx, int n, const double* raw, float* hp,
+                          double* energies, mqw_diag_info* info) {
+  mqw_status s = check_ctx(ctx);
+  if (s != MQW_OK) return s;
+  if (n < 1 || n > MQW_MAX_N || !raw)
+    return fail(ctx, MQW_ERR_INVALID, "build_diag: bad arguments");
+  const size_t N = (size_t)1 << n;
+  DevMem d_raw, d_hp, d_e, d_out, d_scr;
+  CK(d_raw.ensure(params_per(n) * sizeof(double)));
+  CK(d_hp.ensure(N * sizeof(float)));
+  if (energies) CK(d_e.ensure(N * sizeof(double)));
+  CK(d_out.ensure(sizeof(DiagOut)));
+  CK(d_scr.ensure(diag_scratch_bytes(n, 1)));
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(d_raw.p, raw, params_per(n) * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(launch_diag(n, 1, d_raw.as<double>(), d_hp.as<float>(),
+                 energies ? d_e.as<double>() : nullptr, d_out.as<DiagOut>(), d_scr.p, st));
+  DiagOut o;
+  CK(cudaMemcpyAsync(&o, d_out.p, sizeof o, cudaMemcpyDeviceToHost, st));
+  if (hp) CK(cudaMemcpyAsync(hp, d_hp.p, N * sizeof(float), cudaMemcpyDeviceToHost, st));
+  if (energies) CK(cudaMemcpyAsync(energies, d_e.p, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (info) {
+    info->e0 = o.e0;
+    info->emax = o.emax;
+    info->mid = o.mid;
+    info->e_abs = o.e_abs;
+    info->e_loc = o.e_loc;
+  }
+  return MQW_OK;
+}
+
+mqw_status mqw_cheb_coeffs(mqw_ctx* ctx, int count, const double* s_in,
+                           double tol, int max_k, float* coeffs, int* degrees) {
+  mqw_status s = check_ctx(ctx);
+  if (s != MQW_OK) return s;
+  if (count < 0 || max_k < 1 || (count > 0 && (!s_in || !coeffs || !degrees)))
+    return fail(ctx, MQW_ERR_INVALID, "cheb_coeffs: bad arguments");
+  if (count == 0) return MQW_OK;
+  DevMem d_s, d_c, d_k;
+  CK(d_s.ensure(count * sizeof(double)));
+  CK(d_c.ensure((size_t)count * max_k * sizeof(float)));
+  CK(d_k.ensure(count * sizeof(int)));
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(d_s.p, s_in, count * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(d_c.p, 0, (size_t)count * max_k * sizeof(float), st));
+  CK(launch_cheb_from_s(d_s.as<double>(), count, tol, max_k, d_c.as<float>(),
+                        d_k.as<int>(), st));
+  CK(cudaMemcpyAsync(coeffs, d_c.p, (size_t)count * max_k * sizeof(float),
+                     cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(degrees, d_k.p, count * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MQW_OK;
+}
+
+mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
+                        const float* coeffs, const float* hp, float gamma,
+                        float scale, const void* psi, void* out) {
+  mqw_status s = check_ctx(ctx);
+  if (s != MQW_OK) return s;
+  if ((precision != MQW_FP32 && precision != MQW_FP64) || n < 1 || n > MQW_MAX_N ||
+      K < 1 || !coeffs || !hp || !psi || !out)
+    return fail(ctx, MQW_ERR_INVALID, "clenshaw: bad arguments");
+  const size_t N = (size_t)1 << n;
+  const size_t amp = precision == 0 ? 8 : 16;
+  const int lt = std::min(n, kMaxTileLog);
+  const int tiles = (int)(N >> lt);
+  DevMem d_st, d_hp, d_c, d_np;
+  CK(d_st.ensure(3 * N * amp));
+  CK(d_hp.ensure(N * sizeof(float)));
+  CK(d_c.ensure(K * sizeof(float)));
+  CK(d_np.ensure(tiles * sizeof(double)));
+  cudaStream_t st = ctx->stream;
+  char* b = d_st.as<char>();
+  void* P0 = b;
+  void* X = b + N * amp;
+  void* Y = b + 2 * N * amp;
+  CK(cudaMemcpyAsync(P0, psi, N * amp, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_hp.p, hp, N * sizeof(float), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d_c.p, coeffs, K * sizeof(float), cudaMemcpyHostToDevice, st));
+  for (int r = K - 1; r >= 0; r--) {
+    TermParams tp{};
+    tp.n = n;
+    tp.lt = lt;
+    tp.count = 1;
+    TermTraj& T = tp.traj[0];
+    T.mode = (r == K - 1) ? kFirst : (r == K - 2) ? kSecond : kFull;
+    T.b1 = ((r + 1) & 1) ? Y : X;
+    T.b2 = (r & 1) ? Y : X;
+    T.psi = P0;
+    T.hp = d_hp.as<float>();
+    T.coef = d_c.as<float>() + r;
+    T.kappa = nullptr;
+    T.norm_part = d_np.as<double>();
+    T.gamma = gamma;
+    T.scale = scale;
+    T.odd = r & 1;
+    T.final_term = r == 0;
+    CK(launch_term(precision, tp, st));
+  }
+  CK(cudaMemcpyAsync(out, X, N * amp, cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  return MQW_OK;
+}
+
+mqw_status mqw_multiqw(mqw_ctx* ctx, int n, int m, const char* filename,
+                       long long start, long long problems,
+                       const char* out_dir, int print) {
+  mqw_status s = check_ctx(ctx);
+  if (s != MQW_OK) return s;
+  if (!filename || n < 1 || n > MQW_MAX_N || m < 1 || m > MQW_MAX_M || start < 0 ||
+      problems < 0 || problems > (1ll << 31))
+    return fail(ctx, MQW_ERR_INVALID, "multiqw: bad arguments");
+  std::vector<double> raw((size_t)problems * params_per(n));
+  s = mqw_read_instances(filename, n, start, problems, raw.data());
+  if (s != MQW_OK)
+    return fail(ctx, s, "cannot read %lld instances of n=%d from '%s' at instance %lld",
+                problems, n, filename, start);
+  std::vector<double> p(problems);
+  std::vector<float> tt(problems);
+  if (problems > 0) {
+    s = mqw_run_problems(ctx, n, m, raw.data(), (int)problems, nullptr, p.data(),
+                         tt.data(), nullptr, nullptr);
+    if (s != MQW_OK) return s;
+  }
+  std::vector<float> res(problems);
+  for (long long i = 0; i < problems; i++) {
+    res[i] = (float)p[i];
+    if (print) printf("%g %g\n", tt[i], res[i]);  // MultiQW.cpp:423, 455
+  }
+  if (print) fflush(stdout);
+  char name[64];
+  snprintf(name, sizeof name, "output_%d_%d", n, m);  // MultiQW.cpp:265
+  std::string path = out_dir && *out_dir ? std::string(out_dir) + "/" + name : name;
+  FILE* f = fopen(path.c_str(), "ab");  // ios::app, MultiQW.cpp:266
+  if (!f) return fail(ctx, MQW_ERR_IO, "cannot open '%s' for append", path.c_str());
+  const size_t w = problems ? fwrite(res.data(), sizeof(float), problems, f) : 0;
+  fclose(f);
+  if (w != (size_t)problems) return fail(ctx, MQW_ERR_IO, "short write to '%s'", path.c_str());
+  return MQW_OK;
+}
+
+}  // extern "C"

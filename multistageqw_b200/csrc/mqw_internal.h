@@ -1,0 +1,154 @@
+// Internal declarations shared by the host runtime (mqw_host.cpp) and the
+// CUDA kernels (mqw_diag.cu, mqw_coeffs.cu, mqw_propagate.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+namespace mqw {
+
+constexpr int kSamples = 100;          // MultiQW.cpp:257
+constexpr int kMaxN = 30;
+constexpr int kMaxGroup = 8;           // trajectories per grid-path launch
+constexpr int kMaxTileLog = 11;        // grid-path tile: 2^11 amplitudes
+constexpr int kDiagChunkLog = 12;      // Gray ranks per diagonal chunk
+constexpr int kMaxChebTop = 16384;     // Miller start-index bound
+
+// Per-instance device-side description (one per instance in a plan).
+struct InstanceDesc {
+  int n, m;
+  int stages;            // m, or 100 cumulative steps when m == 1
+  int raw_off;           // offset of the instance's raw doubles
+  long long hp_off;      // offset of its 2^n diagonal in the hp pool
+  int sched_off;         // offset into gamma[] (m entries)
+  int times_off;         // offset into times[] (m * 100 entries)
+  int traj_off;          // first trajectory index (samples or 1 walk)
+};
+
+// Reference-arithmetic spectral data of one instance.
+struct DiagOut {
+  double e0, emax, mid;
+  float e_abs;
+  uint32_t e_loc;
+};
+
+// Chunk partials of the Gray-code scan.
+struct ChunkPartial {
+  double total;     // sum of the chunk's increments
+  double vmin;      // min over the chunk of the running (chunk-local) sum
+  double vmax;
+  uint32_t rmin;    // Gray rank of the first minimum
+  uint32_t pad;
+};
+
+// ---- diagonal -------------------------------------------------------------
+// Builds hp (float, shifted) and optionally energies (double) for `count`
+// instances of the same n. raw: device pointer to count*n(n+1)/2 doubles.
+// scratch: device buffer of diag_scratch_bytes(n, count) bytes.
+size_t diag_scratch_bytes(int n, int count);
+cudaError_t launch_diag(int n, int count, const double* raw, float* hp,
+                        double* energies, DiagOut* out, void* scratch,
+                        cudaStream_t stream);
+
+// ---- Chebyshev coefficients --------------------------------------------
+// One entry per (instance, stage, sample) "coefficient job".
+struct CoefJob {
+  int inst;        // instance index (DiagOut / n)
+  int n;
+  float gamma;     // hopping rate of the stage
+  float t;         // evolution time of the sample
+};
+// Pass 1: degree of each job (s = fl(fl(e_abs + gamma*n) * t)).
+cudaError_t launch_cheb_degree(const CoefJob* jobs, int count,
+                               const DiagOut* diag, double tol, int* degree,
+                               float* onenorm, cudaStream_t stream);
+// Pass 2: float coefficients at coef + offset[job].
+cudaError_t launch_cheb_coeffs(const CoefJob* jobs, int count,
+                               const DiagOut* diag, double tol,
+                               const long long* offset, float* coef,
+                               cudaStream_t stream);
+// Direct: coefficients for explicit s values (API helper).
+cudaError_t launch_cheb_from_s(const double* s, int count, double tol,
+                               int max_k, float* coef, int* degree,
+                               cudaStream_t stream);
+
+// ---- propagation --------------------------------------------------------
+// Trajectory-stage data for the resident (one-CTA-per-walk) kernel.
+struct ResidentWalk {
+  int inst;            // instance
+  int n;
+  int stages;          // number of Clenshaw stages in the walk
+  int record_each;     // 1: record P after every stage (m == 1 walks)
+  int stage_desc_off;  // first entry in StageDesc table
+  int p_off;           // where P values go (p_sample index)
+  long long hp_off;
+};
+struct StageDesc {
+  long long coef_off;  // offset into the coefficient pool
+  int K;
+  float gamma;
+  float onenorm;       // stored by the degree pass
+};
+
+int resident_max_n(int precision);
+cudaError_t launch_resident(int precision, const ResidentWalk* walks,
+                            int count, int max_n, const StageDesc* stages,
+                            const float* coef, const float* hp,
+                            const DiagOut* diag, double* p_sample,
+                            cudaStream_t stream);
+
+// Grid path: one Clenshaw term for up to kMaxGroup trajectories of the same n.
+enum TermMode : int { kSkip = 0, kFirst = 1, kSecond = 2, kFull = 3 };
+struct TermTraj {
+  const void* b1;      // b_{r+1}
+  void* b2;            // b_{r+2} in, b_r out (in place)
+  const void* psi;     // stage input state
+  const float* hp;     // shifted diagonal
+  const float* coef;   // &coef[r]
+  const double* kappa; // 1/||psi|| of the stage input (nullptr = 1)
+  double* norm_part;   // final term: per-tile |b_0|^2 partials
+  float gamma;
+  float scale;         // onenorm (the final term uses 2*scale)
+  int mode;
+  int odd;             // r odd: coefficient is imaginary
+  int final_term;      // r == 0
+};
+struct TermParams {
+  int n;
+  int lt;              // log2 tile size
+  int count;
+  TermTraj traj[kMaxGroup];
+};
+cudaError_t launch_term(int precision, const TermParams& p,
+                        cudaStream_t stream);
+
+// Finalisation after a stage: kappa[g] = 1/sqrt(sum of partials); when
+// record != 0 also p_out[g] = |out[e_loc]|^2 * kappa^2.
+struct FinalTraj {
+  const double* norm_part;
+  int tiles;
+  double* kappa;
+  const void* out;     // stage output state
+  uint32_t e_loc;      // read on device from DiagOut when diag != nullptr
+  const DiagOut* diag;
+  double* p_out;       // nullptr = no record
+};
+struct FinalParams {
+  int count;
+  FinalTraj traj[kMaxGroup];
+};
+cudaError_t launch_finalize(int precision, const FinalParams& p,
+                            cudaStream_t stream);
+
+// Fill a state with the uniform superposition (float(1/sqrt(N)), 0).
+cudaError_t launch_uniform(int precision, void* psi, int n,
+                           cudaStream_t stream);
+
+// Mean of p_sample rows (fixed order) into p_mean.
+cudaError_t launch_mean(const double* p_sample, const int* p_off,
+                        const int* p_cnt, int count, double* p_mean,
+                        cudaStream_t stream);
+
+}  // namespace mqw

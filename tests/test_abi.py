@@ -1,0 +1,111 @@
+"""CPU tests of the product's C ABI: the library loads and exports every
+entry point declared in include/mqw.h, and its host-side logic (instance
+unpacking, inverse normal, stage schedule, file reading, argument checking)
+agrees bit-for-bit with the oracle. No kernels are launched here."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+
+def test_exports_every_header_symbol(mqw):
+    L = mqw.lib()
+    names = mqw.exported_symbols()
+    assert len(names) >= 20
+    for name in names:
+        assert hasattr(L, name), name
+    assert L.mqw_abi_version() == 1
+
+
+def test_cli_binary_links(mqw):
+    assert os.path.exists(mqw.CLI_PATH)
+    out = subprocess.run(["ldd", mqw.CLI_PATH], capture_output=True, text=True).stdout
+    assert "libmqw.so" in out and "not found" not in out
+
+
+def test_cli_too_few_args_returns_minus_one(mqw):
+    r = subprocess.run([mqw.CLI_PATH, "10", "2"], capture_output=True)
+    assert r.returncode == 255  # `return -1` (MultiQW.cpp:244)
+
+
+def test_inv_norm_matches_oracle(mqw, orc):
+    for n in range(1, 31):
+        for p in (1.0 / (1 << n), 1.0 / (2.718281828459045 * (1 << n)), 0.3, 0.5, 0.9):
+            pf = float(np.float32(p))
+            a = np.float32(mqw.inv_norm_upper(pf))
+            b = np.float32(orc.inv_norm_upper(pf))
+            assert a.view(np.uint32) == b.view(np.uint32), (n, p)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 10, 20, 30])
+def test_load_instance_matches_oracle(mqw, orc, n):
+    raw = orc.sk_instances(n, 1, n)[0]
+    J1, h1 = mqw.load_instance(n, raw)
+    J2, h2 = orc.load_instance(n, raw)
+    assert np.array_equal(J1, J2) and np.array_equal(h1, h2)
+    assert np.array_equal(J1, J1.T) and not np.diag(J1).any()
+
+
+@pytest.mark.parametrize("n,m", [(4, 1), (5, 2), (10, 2), (10, 4), (13, 3), (20, 4), (24, 4), (28, 3), (12, 5), (16, 8)])
+def test_schedule_bit_exact_vs_oracle(mqw, orc, n, m):
+    raw = orc.sk_instances(n, 3, 1000 + n * 7 + m)
+    for r in raw:
+        g1, s1, t1, tot1 = mqw.schedule(n, m, r)
+        g2, s2, t2, tot2 = orc.schedule(n, m, r)
+        assert np.array_equal(g1, g2)
+        assert np.array_equal(s1, s2)
+        assert np.array_equal(t1, t2)
+        assert tot1 == tot2
+
+
+def test_schedule_heuristic_shape(mqw, orc):
+    # gamma_i decreases with the stage index; times lie in [short_t, 2 short_t).
+    raw = orc.sk_instances(12, 1, 3)[0]
+    g, st, t, tot = mqw.schedule(12, 4, raw)
+    assert (np.diff(g) < 0).all()
+    assert ((t >= st[:, None]) & (t < 2 * st[:, None])).all()
+    assert np.isclose(tot, st.sum(), rtol=1e-6)
+
+
+def test_read_instances_and_short_file(mqw, orc, tmp_path):
+    n = 6
+    raw = orc.sk_instances(n, 5, 9)
+    f = tmp_path / "SK_6n"
+    raw.tofile(f)
+    got = mqw.read_instances(str(f), n, 1, 3)
+    assert np.array_equal(got, raw[1:4])
+    with pytest.raises(mqw.MQWError) as e:
+        mqw.read_instances(str(f), n, 3, 3)  # runs past the end
+    assert e.value.status == 4
+    with pytest.raises(mqw.MQWError) as e:
+        mqw.read_instances(str(tmp_path / "missing"), n, 0, 1)
+    assert e.value.status == 4
+
+
+def test_invalid_arguments_return_status(mqw):
+    L = mqw.lib()
+    raw = np.zeros(3, np.float64)
+    g = np.zeros(4, np.float32)
+    t = np.zeros(400, np.float32)
+    P = ctypes.POINTER
+    assert L.mqw_schedule(0, 2, raw.ctypes.data_as(P(ctypes.c_double)), g.ctypes.data_as(P(ctypes.c_float)),
+                          None, t.ctypes.data_as(P(ctypes.c_float)), None) == 1
+    assert L.mqw_schedule(2, 0, raw.ctypes.data_as(P(ctypes.c_double)), g.ctypes.data_as(P(ctypes.c_float)),
+                          None, t.ctypes.data_as(P(ctypes.c_float)), None) == 1
+    assert L.mqw_load_instance(31, raw.ctypes.data_as(P(ctypes.c_double)), None, None) == 1
+    assert L.mqw_create(None, 0) == 1
+
+
+def test_no_gpu_context_fails_loudly(mqw):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(mqw.MQWError) as e:
+        mqw.Context(0)
+    assert e.value.status == 7
+
+
+def test_sk_generator_matches_oracle(mqw, orc):
+    assert np.array_equal(mqw.sk_instances(9, 4, 2), orc.sk_instances(9, 4, 2))

@@ -1,0 +1,191 @@
+"""CPU tests of the oracle: pinned against the reference's own functions
+(golden fixtures made from the partial reference build), against mathematics
+(brute force, scipy) and against its own golden outputs."""
+import hashlib
+import math
+
+import numpy as np
+import pytest
+import scipy.linalg as sl
+import scipy.special as sp
+
+from tests.conftest import load_golden
+from tests.golden.make_golden import step_inputs
+
+
+def test_inv_norm_within_one_ulp_of_reference(orc):
+    g = load_golden("ref_normcdfinv.json")
+    worst = 0
+    for v in g["values"]:
+        p = float(np.uint32(v["p_bits"]).view(np.float32))
+        mine = np.float32(orc.inv_norm_upper(p))
+        ref_bits = np.int64(v["value_bits"])
+        worst = max(worst, abs(int(mine.view(np.uint32)) - int(ref_bits)))
+    # The reference's float approximation is within 4.1 ulp of the exact
+    # quantile; the restatement is correctly rounded.
+    assert worst <= 1
+
+
+def test_clenshaw_step_bit_exact_vs_reference_golden(orc):
+    g = load_golden("ref_clenshaw_step.json")
+    for c in g["cases"]:
+        b1, b2, hp, psi = step_inputs(c["n"], c["seed"])
+        out = b2.copy()
+        orc.clenshaw_step_f32(b1, out, hp, psi, c["n"], c["scale"], c["gamma"], c["coef"])
+        assert hashlib.sha256(out.tobytes()).hexdigest() == c["sha256"], c["n"]
+
+
+def test_clenshaw_step_bit_exact_vs_reference_build(orc):
+    if orc.ref_lib() is None:
+        pytest.skip("partial reference build not present")
+    rng = np.random.default_rng(5)
+    for n in (4, 6, 11, 15, 16, 18):
+        N = 1 << n
+        b1 = rng.standard_normal(N).astype(np.float32)
+        b2 = rng.standard_normal(N).astype(np.float32)
+        hp = (rng.standard_normal(N) * 9).astype(np.float32)
+        psi = rng.standard_normal(N).astype(np.float32)
+        for coef in (0.0, -1.25):
+            x, y = b2.copy(), b2.copy()
+            orc.clenshaw_step_f32(b1, x, hp, psi, n, 44.5, 1.3, coef)
+            orc.ref_clenshaw_step(b1, y, hp, psi, n, 44.5, 1.3, coef)
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32)), (n, coef)
+
+
+def test_pipeline_with_reference_step_is_identical(orc):
+    if orc.ref_lib() is None:
+        pytest.skip("partial reference build not present")
+    raw = orc.sk_instances(9, 2, 3)
+    a = orc.run_problems(9, 3, raw, 2, 10, "f32", use_ref_step=False)
+    b = orc.run_problems(9, 3, raw, 2, 10, "f32", use_ref_step=True)
+    assert np.array_equal(a["p"], b["p"])
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 9, 12])
+def test_energies_track_exact_energies(orc, n):
+    raw = orc.sk_instances(n, 1, 100 + n)[0]
+    E, hp, info = orc.energies_ref(n, raw)
+    Ex = orc.energies_exact(n, raw)
+    assert np.abs(E - Ex).max() < 1e-4 * max(1.0, np.abs(Ex).max())
+    assert info.e_loc == int(np.argmin(Ex))
+    assert math.isclose(info.e0, E.min()) and math.isclose(info.emax, E.max())
+    mid = np.float32(info.mid)
+    assert np.array_equal(hp, (E.astype(np.float32) - mid).astype(np.float32))
+    assert info.e_abs == np.float32((info.emax - info.e0) / 2)
+
+
+def _gray_numpy(n, J, h):
+    """Sequential numpy restatement of the Gray-code sweep, MultiQW.cpp:325-358."""
+    N = 1 << n
+    E = np.empty(N)
+    s0 = np.float32(0)
+    for v in J.ravel():
+        s0 = np.float32(s0 + v)
+    hs = np.float32(0)
+    for v in h:
+        hs = np.float32(hs + v)
+    e = float(np.float32(s0 - hs))
+    E[0] = e
+    st = np.ones((n, n), np.float32)
+    for i in range(1, N):
+        f = (i & -i).bit_length() - 1
+        st[f, :] *= -1
+        st[:, f] *= -1
+        st[f, f] *= -1
+        acc = np.float32(J[f, 0] * st[f, 0])
+        for k in range(1, n):
+            acc = np.float32(acc + np.float32(J[f, k] * st[f, k]))
+        d = np.float32(np.float32(4) * acc - np.float32(2) * h[f] * st[f, f])
+        e += float(d)
+        E[i ^ (i >> 1)] = e
+    return E
+
+
+def test_energies_bit_exact_vs_sequential_restatement(orc):
+    n = 8
+    raw = orc.sk_instances(n, 1, 77)[0]
+    J, h = orc.load_instance(n, raw)
+    E, _, _ = orc.energies_ref(n, raw)
+    assert np.array_equal(E, _gray_numpy(n, J, h))
+
+
+def test_ground_state_first_in_gray_order(orc):
+    # Planted tie: with h = 0, E(z) = E(~z). Dyadic couplings keep every float
+    # increment exact, so the tie survives the reference's arithmetic and the
+    # first of the pair in Gray order must win.
+    n = 6
+    rng = np.random.default_rng(5)
+    raw = np.zeros(n * (n + 1) // 2)
+    raw[: n * (n - 1) // 2] = rng.integers(-8, 9, n * (n - 1) // 2) / 8.0
+    E, _, info = orc.energies_ref(n, raw)
+    N = 1 << n
+    ranks = np.empty(N, np.int64)
+    for r in range(N):
+        ranks[r ^ (r >> 1)] = r
+    best = np.flatnonzero(E == E.min())
+    assert len(best) >= 2
+    assert info.e_loc == best[np.argmin(ranks[best])]
+
+
+@pytest.mark.parametrize("s", [1e-9, 3e-6, 0.2, 1.0, 7.5, 12.3, 37.0, 150.0, 420.0, 1500.0])
+def test_cheb_coeffs_vs_scipy(orc, s):
+    c = orc.cheb_coeffs(s)
+    k = np.arange(len(c))
+    ex = sp.jv(k, s) * np.where(k == 0, 1, 2) * np.where((k // 2) % 2 == 1, -1, 1)
+    assert np.abs(c - ex).max() < 1e-13 * max(1.0, s / 10)
+    tail = 2 * np.abs(sp.jv(np.arange(len(c), len(c) + 400), s)).sum()
+    assert tail <= 1e-6 * (1 + 1e-9)
+    if len(c) > 1:
+        tail_prev = tail + 2 * abs(sp.jv(len(c) - 1, s))
+        assert tail_prev > 1e-6  # K is the smallest degree meeting the rule
+
+
+def test_clenshaw_matches_dense_expm(orc):
+    n = 6
+    N = 1 << n
+    raw = orc.sk_instances(n, 1, 3)[0]
+    E, hp, info = orc.energies_ref(n, raw)
+    g, _, t, _ = orc.schedule(n, 2, raw)
+    X = np.zeros((N, N))
+    for q in range(n):
+        X[np.arange(N), np.arange(N) ^ (1 << q)] = 1.0
+    H = np.diag(hp.astype(np.float64)) - float(g[0]) * X
+    onenorm = float(np.float32(info.e_abs + g[0] * np.float32(n)))
+    for tt in (float(t[0, 0]), float(t[0, 7])):
+        s = float(np.float32(np.float32(onenorm) * np.float32(tt)))
+        c = orc.cheb_coeffs(s).astype(np.float32)
+        psi = np.zeros(2 * N)
+        psi[:N] = 1 / np.sqrt(N)
+        out = orc.clenshaw(n, c, hp.astype(np.float64), float(g[0]), onenorm, psi, True, "f64")
+        # e^{+i s H~} with H~ = H / onenorm; conjugate of e^{-iHt}, same |amplitudes|.
+        ex = sl.expm(1j * (s / onenorm) * H) @ (psi[:N] + 0j)
+        assert np.abs(out[:N] + 1j * out[N:] - ex).max() < 2e-6
+
+
+def test_schedule_m1_cumulative(orc):
+    raw = orc.sk_instances(7, 1, 8)[0]
+    g, st, t, tot = orc.schedule(7, 1, raw)
+    assert t.shape == (1, 100)
+    assert (t[0] >= 0).all()
+    # the differences re-sum to the sorted draws, which lie in [st, 2 st)
+    cum = np.cumsum(t[0].astype(np.float64))
+    assert cum[0] >= st[0] and cum[-1] < 2 * st[0] * (1 + 1e-6)
+
+
+def test_oracle_golden_config1(orc):
+    g = load_golden("oracle_config1.json")
+    raw = orc.sk_instances(g["n"], g["count"], g["seed"])
+    r32 = orc.run_problems(g["n"], g["m"], raw, g["count"], g["samples"], "f32")
+    assert np.array_equal(r32["p"], np.array(g["p_f32"]))
+    assert r32["e_loc"].tolist() == g["e_loc"]
+    assert r32["terms"].tolist() == g["terms"]
+    p64 = np.array(g["p_f64"])
+    assert np.abs(r32["p"] - p64).max() < 1e-6
+
+
+def test_oracle_golden_small(orc):
+    for c in load_golden("oracle_small.json")["cases"]:
+        raw = orc.sk_instances(c["n"], c["count"], c["seed"])
+        r = orc.run_problems(c["n"], c["m"], raw, c["count"], c["samples"], "f64")
+        assert np.allclose(r["p"], c["p_f64"], rtol=0, atol=1e-14), c
+        assert np.abs(np.array(c["p_f32"]) - np.array(c["p_f64"])).max() < 1e-5, c
