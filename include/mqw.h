@@ -126,6 +126,11 @@ mqw_status mqw_schedule(int n, int m, const double* raw, float* gammas,
 mqw_status mqw_read_instances(const char* filename, int n, long long start,
                               long long problems, double* raw_out);
 
+/* Host build of the same coefficient routine the GPU runs (mqw_cheb_coeffs):
+ * bit-identical results, for callers without a GPU and for checking. */
+mqw_status mqw_cheb_coeffs_host(int count, const double* s, double tol,
+                                int max_k, float* coeffs, int* degrees);
+
 /* ---- device pieces ------------------------------------------------------- */
 
 /* Ising diagonal of one instance on the GPU with the reference's arithmetic
@@ -144,7 +149,8 @@ mqw_status mqw_cheb_coeffs(mqw_ctx* ctx, int count, const double* s,
 
 /* One Clenshaw propagation out = sum_k c_k T_k(H~) psi on the GPU, with
  * H~ = (hp - gamma * sum_q X_q) / scale, real c_k for even k and imaginary
- * for odd k. psi/out are interleaved complex (re, im) of 2^n amplitudes
+ * for odd k, 6 <= n <= 30 (grid path). psi/out are interleaved complex
+ * (re, im) of 2^n amplitudes
  * (float for MQW_FP32, double for MQW_FP64 in `precision`); hp is float.
  * Replaces Clenshaw (MultiQW.cpp:177-236). */
 mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,

@@ -103,6 +103,7 @@ def _bind(L):
         "mqw_read_instances": (i, [ctypes.c_char_p, i, ll, ll, _P(d)]),
         "mqw_build_diag": (i, [_vp, i, _P(d), _P(f), _P(d), _P(DiagInfo)]),
         "mqw_cheb_coeffs": (i, [_vp, i, _P(d), d, i, _P(f), _P(i)]),
+        "mqw_cheb_coeffs_host": (i, [i, _P(d), d, i, _P(f), _P(i)]),
         "mqw_clenshaw": (i, [_vp, i, i, i, _P(f), _P(f), f, f, _vp, _vp]),
         "mqw_run_problems": (i, [_vp, i, i, _P(d), i, _P(Options), _P(d), _P(f), _P(ctypes.c_uint32), _P(RunStats)]),
         "mqw_plan_create": (i, [_vp, i, _P(i), _P(i), _P(d), _P(Options), _P(_vp)]),
@@ -190,6 +191,16 @@ def schedule(n: int, m: int, raw):
     _check(None, lib().mqw_schedule(n, m, _ptr(raw, ctypes.c_double), _ptr(g, ctypes.c_float),
                                      _ptr(st, ctypes.c_float), _ptr(t, ctypes.c_float), _ptr(tot, ctypes.c_float)))
     return g, st, t.reshape(m, SAMPLES), float(tot[0])
+
+
+def cheb_coeffs_host(s, tol: float = 1e-6, max_k: int = 4096):
+    """Host build of the GPU's coefficient routine (bit-identical)."""
+    s = np.ascontiguousarray(np.atleast_1d(s), dtype=np.float64)
+    c = np.zeros((len(s), max_k), np.float32)
+    k = np.zeros(len(s), np.int32)
+    _check(None, lib().mqw_cheb_coeffs_host(len(s), _ptr(s, ctypes.c_double), tol, max_k,
+                                            _ptr(c, ctypes.c_float), _ptr(k, ctypes.c_int)))
+    return [c[i, :k[i]].copy() for i in range(len(s))], k
 
 
 def read_instances(filename: str, n: int, start: int, problems: int) -> np.ndarray:

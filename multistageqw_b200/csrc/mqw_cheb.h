@@ -81,6 +81,7 @@ MQW_HD inline int cheb_coeffs_stream(double s, double tol, float* out,
         found = true;
       }
     }
+    if (!found && km == 0) found = true;  // K = 1: only c_0 is kept
     if (found && out && km < max_k) {
       double v = fm / norm;
       if (km > 0) v *= ((km / 2) & 1) ? -2.0 : 2.0;

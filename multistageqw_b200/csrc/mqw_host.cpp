@@ -34,11 +34,41 @@
 
 using namespace mqw;
 
+// Owning device allocation.
+struct DevMem {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevMem() = default;
+  DevMem(const DevMem&) = delete;
+  DevMem& operator=(const DevMem&) = delete;
+  ~DevMem() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  cudaError_t ensure(size_t b) {
+    if (b <= bytes && p) return cudaSuccess;
+    release();
+    if (b == 0) b = 16;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e == cudaSuccess) bytes = b;
+    return e;
+  }
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// A context owns the reusable device scratch that plans share: the grid-path
+// state slots, norm partials, the coefficient pool and its tables, and the
+// diagonal's chunk partials. Plans of one context are executed one at a time
+// (the ABI's threading rule), so sharing is safe and repeated calls do not
+// pay for allocation.
 struct mqw_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
   std::string err;
   int sm_count = 0;
+  DevMem state, norm_part, kappa, coef, coef_off, stages, walks, diag_scratch;
 };
 
 namespace {
@@ -64,30 +94,6 @@ mqw_status fail(mqw_ctx* ctx, mqw_status s, const char* fmt, ...) {
                   "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_),   \
                   __FILE__, __LINE__);                                      \
   } while (0)
-
-// Owning device allocation.
-struct DevMem {
-  void* p = nullptr;
-  size_t bytes = 0;
-  DevMem() = default;
-  DevMem(const DevMem&) = delete;
-  DevMem& operator=(const DevMem&) = delete;
-  ~DevMem() { release(); }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    bytes = 0;
-  }
-  cudaError_t ensure(size_t b) {
-    if (b <= bytes && p) return cudaSuccess;
-    release();
-    if (b == 0) b = 16;
-    cudaError_t e = cudaMalloc(&p, b);
-    if (e == cudaSuccess) bytes = b;
-    return e;
-  }
-  template <typename T> T* as() const { return static_cast<T*>(p); }
-};
 
 int params_per(int n) { return n * (n + 1) / 2; }
 
@@ -115,15 +121,14 @@ struct mqw_plan {
   std::vector<long long> raw_off;        // doubles offset per sorted instance
   std::vector<long long> hp_off;         // hp offset per sorted instance
   std::vector<int> p_off;                // p_sample offset per sorted instance
-  DevMem d_raw, d_hp, d_diag, d_diag_scratch;
+  DevMem d_raw, d_hp, d_diag;
   // Jobs: one per (walk, stage) in walk-major order.
   std::vector<CoefJob> jobs;
   std::vector<ResidentWalk> walks;       // all walks (resident and grid)
   std::vector<int> walk_is_grid;
-  DevMem d_jobs, d_degree, d_onenorm, d_coef_off, d_coef, d_stages, d_walks;
+  DevMem d_jobs, d_degree, d_onenorm;
   DevMem d_p_sample, d_p_mean, d_p_off, d_p_cnt;
-  // Grid-path buffers.
-  DevMem d_state, d_norm_part, d_kappa;
+  size_t diag_scratch_bytes = 0;
   // Host copies of the degree read-back.
   std::vector<int> degree;
   std::vector<float> onenorm;
@@ -150,46 +155,54 @@ mqw_status check_ctx(mqw_ctx* ctx) {
   return MQW_OK;
 }
 
+int walk_slots(const PassGeomHost& geo) { return geo.nu > 0 ? 4 : 3; }
+
 int choose_group(const mqw_plan& P, int n) {
   if (P.opt.group > 0) return std::min(P.opt.group, kMaxGroup);
   const size_t amp = P.precision == 0 ? 8 : 16;
-  const size_t walk_bytes = 3 * amp * ((size_t)1 << n);
-  // Keep a launch's states within about 96 MB so they stay resident in the
-  // 126 MB L2 between terms, but give every launch at least ~2^20 amplitudes.
-  size_t g = (96u << 20) / walk_bytes;
+  const size_t walk_bytes =
+      (walk_slots(pass_geom(P.precision, n)) * amp + sizeof(float)) * ((size_t)1 << n);
+  // Keep a launch's working set within ~60 MB (about one die's share of the
+  // 126 MB L2, which both dies' SMs read from), but give every launch at
+  // least ~2^20 amplitudes.
+  size_t g = (60u << 20) / walk_bytes;
   if (((size_t)1 << n) * g < ((size_t)1 << 20)) g = ((size_t)1 << 20) >> n;
   if (g < 1) g = 1;
   if (g > (size_t)kMaxGroup) g = kMaxGroup;
   return (int)g;
 }
 
-// Runs the grid-path walks with index in [w0, w1) (all the same n).
+// Runs a group of grid-path walks (all the same n) through all their stages.
+// Each walk owns the state slots psi, b and the partial P; when some axes are
+// read from global memory (nu > 0) b is double-buffered (b_r in slot x for
+// even r and y for odd r), otherwise it is updated in place, which keeps a
+// walk at 3 vectors so that two walks of n = 20 stay resident in L2. Pass r
+// uses tiling 1 for even r and tiling 2 for odd r.
 mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
                           cudaStream_t stream) {
   mqw_ctx* ctx = P.ctx;
   const int n = P.walks[widx[0]].n;
   const size_t N = (size_t)1 << n;
-  const int lt = std::min(n, kMaxTileLog);
-  const int tiles = (int)(N >> lt);
+  const PassGeomHost geo = pass_geom(P.precision, n);
+  const int tiles = (int)(N >> geo.L);
   const int G = (int)widx.size();
   const size_t amp = P.precision == 0 ? 8 : 16;
-  char* base = P.d_state.as<char>();
+  const int slots = walk_slots(geo);
+  char* base = P.ctx->state.as<char>();
   auto buf = [&](int g, int k) -> void* {
-    return base + ((size_t)g * 3 + k) * N * amp;
+    return base + ((size_t)g * slots + k) * N * amp;
   };
-  // Roles: psi = slot pi[g], b_r lives in slot x[g] for even r, y[g] for odd.
-  int pi[kMaxGroup], xs[kMaxGroup], ys[kMaxGroup];
+  int pi[kMaxGroup], xs[kMaxGroup];
+  const int ps = 2;
+  const int ys = geo.nu > 0 ? 3 : -1;  // -1: b in place
   for (int g = 0; g < G; g++) {
     pi[g] = 0;
     xs[g] = 1;
-    ys[g] = 2;
-    CK(launch_uniform(P.precision, buf(g, pi[g]), n, stream));
-    P.stats.launches++;
   }
-  double* norm_part = P.d_norm_part.as<double>();
-  double* kappa = P.d_kappa.as<double>();
+  double* norm_part = P.ctx->norm_part.as<double>();
+  double* kappa = P.ctx->kappa.as<double>();
   double* p_sample = P.d_p_sample.as<double>();
-  const float* coef = P.d_coef.as<float>();
+  const float* coef = P.ctx->coef.as<float>();
   const float* hp = P.d_hp.as<float>();
   const DiagOut* diag = P.d_diag.as<DiagOut>();
   int max_stages = 0;
@@ -202,33 +215,38 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
       Kmax = std::max(Kmax, K[g]);
     }
     for (int r = Kmax - 1; r >= 0; r--) {
-      TermParams tp{};
-      tp.n = n;
-      tp.lt = lt;
-      tp.count = G;
+      PassParams pp{};
+      pp.n = n;
+      pp.L = geo.L;
+      pp.a = geo.a;
+      pp.tiling = (r & 1) ? 2 : 1;
+      pp.count = G;
       for (int g = 0; g < G; g++) {
-        TermTraj& T = tp.traj[g];
+        PassWalk& W = pp.walk[g];
         const ResidentWalk& w = P.walks[widx[g]];
-        if (r >= K[g]) {
-          T.mode = kSkip;
-          continue;
-        }
+        W.active = r < K[g];
+        if (!W.active) continue;
         const int job = w.stage_desc_off + st;
-        T.mode = (r == K[g] - 1) ? kFirst : (r == K[g] - 2) ? kSecond : kFull;
-        T.b1 = buf(g, ((r + 1) & 1) ? ys[g] : xs[g]);
-        T.b2 = buf(g, (r & 1) ? ys[g] : xs[g]);
-        T.psi = buf(g, pi[g]);
-        T.hp = hp + w.hp_off;
-        T.coef = coef + P.coef_off[job] + r;
-        T.kappa = st == 0 ? nullptr : kappa + g;
-        T.norm_part = norm_part + (size_t)g * tiles;
-        T.gamma = P.jobs[job].gamma;
-        T.scale = P.onenorm[job];
-        T.odd = r & 1;
-        T.final_term = r == 0;
+        if (ys < 0) {
+          W.bin = W.bout = buf(g, xs[g]);
+        } else {
+          W.bin = buf(g, (r & 1) ? xs[g] : ys);
+          W.bout = buf(g, (r & 1) ? ys : xs[g]);
+        }
+        W.part = buf(g, ps);
+        W.psi = buf(g, pi[g]);
+        W.hp = hp + w.hp_off;
+        W.coef = coef + P.coef_off[job];
+        W.kappa = st == 0 ? nullptr : kappa + g;
+        W.norm_part = norm_part + (size_t)g * tiles;
+        W.gamma = P.jobs[job].gamma;
+        W.scale = P.onenorm[job];
+        W.r = r;
+        W.K = K[g];
+        W.psi_uniform = st == 0;  // every walk starts from the uniform state
         P.stats.term_amps += (double)N;
       }
-      CK(launch_term(P.precision, tp, stream));
+      CK(launch_pass(P.precision, pp, stream));
       P.stats.launches++;
       P.stats.term_launches++;
     }
@@ -262,6 +280,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
   mqw_ctx* ctx = P.ctx;
   const int count = P.count;
   // 1. Diagonals, per group of equal n (instances are sorted by n).
+  CK(ctx->diag_scratch.ensure(P.diag_scratch_bytes));
   DiagOut* d_diag = P.d_diag.as<DiagOut>();
   for (int s = 0; s < count;) {
     const int n = P.n[P.order[s]];
@@ -269,7 +288,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     while (e < count && P.n[P.order[e]] == n) e++;
     CK(launch_diag(n, e - s, P.d_raw.as<double>() + P.raw_off[s],
                    P.d_hp.as<float>() + P.hp_off[s], nullptr, d_diag + s,
-                   P.d_diag_scratch.p, stream));
+                   P.ctx->diag_scratch.p, stream));
     P.stats.launches += 3;
     s = e;
   }
@@ -296,14 +315,14 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     P.coef_off[j + 1] = P.coef_off[j] + P.degree[j];
     P.stats.terms += P.degree[j];
   }
-  CK(P.d_coef_off.ensure((nj + 1) * sizeof(long long)));
-  CK(cudaMemcpyAsync(P.d_coef_off.p, P.coef_off.data(),
+  CK(P.ctx->coef_off.ensure((nj + 1) * sizeof(long long)));
+  CK(cudaMemcpyAsync(P.ctx->coef_off.p, P.coef_off.data(),
                      (nj + 1) * sizeof(long long), cudaMemcpyHostToDevice,
                      stream));
   P.stats.h2d_bytes += (double)(nj + 1) * sizeof(long long) + (double)nj * sizeof(StageDesc);
-  CK(P.d_coef.ensure(P.coef_off[nj] * sizeof(float)));
+  CK(P.ctx->coef.ensure(P.coef_off[nj] * sizeof(float)));
   CK(launch_cheb_coeffs(P.d_jobs.as<CoefJob>(), nj, d_diag, P.opt.cheb_tol,
-                        P.d_coef_off.as<long long>(), P.d_coef.as<float>(),
+                        P.ctx->coef_off.as<long long>(), P.ctx->coef.as<float>(),
                         stream));
   P.stats.launches++;
   // 4a. Resident walks.
@@ -317,8 +336,8 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     sdesc[j].gamma = P.jobs[j].gamma;
     sdesc[j].onenorm = P.onenorm[j];
   }
-  CK(P.d_stages.ensure(nj * sizeof(StageDesc)));
-  CK(cudaMemcpyAsync(P.d_stages.p, sdesc.data(), nj * sizeof(StageDesc),
+  CK(P.ctx->stages.ensure(nj * sizeof(StageDesc)));
+  CK(cudaMemcpyAsync(P.ctx->stages.p, sdesc.data(), nj * sizeof(StageDesc),
                      cudaMemcpyHostToDevice, stream));
   std::vector<ResidentWalk> res;
   int res_max_n = 0;
@@ -339,13 +358,13 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
                            (double)(1u << P.walks[w].n);
   }
   if (!res.empty()) {
-    CK(P.d_walks.ensure(res.size() * sizeof(ResidentWalk)));
-    CK(cudaMemcpyAsync(P.d_walks.p, res.data(), res.size() * sizeof(ResidentWalk),
+    CK(P.ctx->walks.ensure(res.size() * sizeof(ResidentWalk)));
+    CK(cudaMemcpyAsync(P.ctx->walks.p, res.data(), res.size() * sizeof(ResidentWalk),
                        cudaMemcpyHostToDevice, stream));
     P.stats.h2d_bytes += (double)res.size() * sizeof(ResidentWalk);
-    CK(launch_resident(P.precision, P.d_walks.as<ResidentWalk>(), (int)res.size(),
-                       res_max_n, P.d_stages.as<StageDesc>(),
-                       P.d_coef.as<float>(), P.d_hp.as<float>(), d_diag,
+    CK(launch_resident(P.precision, P.ctx->walks.as<ResidentWalk>(), (int)res.size(),
+                       res_max_n, P.ctx->stages.as<StageDesc>(),
+                       P.ctx->coef.as<float>(), P.d_hp.as<float>(), d_diag,
                        P.d_p_sample.as<double>(), stream));
     P.stats.launches++;
   }
@@ -355,10 +374,10 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     const int G = choose_group(P, n);
     const size_t N = (size_t)1 << n;
     const size_t amp = P.precision == 0 ? 8 : 16;
-    const int lt = std::min(n, kMaxTileLog);
-    CK(P.d_state.ensure((size_t)G * 3 * N * amp));
-    CK(P.d_norm_part.ensure((size_t)G * (N >> lt) * sizeof(double)));
-    CK(P.d_kappa.ensure(kMaxGroup * sizeof(double)));
+    const PassGeomHost geo = pass_geom(P.precision, n);
+    CK(P.ctx->state.ensure((size_t)G * walk_slots(geo) * N * amp));
+    CK(P.ctx->norm_part.ensure((size_t)G * (N >> geo.L) * sizeof(double)));
+    CK(P.ctx->kappa.ensure(kMaxGroup * sizeof(double)));
     const std::vector<int>& ws = kv.second;
     for (size_t i = 0; i < ws.size(); i += G) {
       std::vector<int> grp(ws.begin() + i, ws.begin() + std::min(ws.size(), i + G));
@@ -523,7 +542,7 @@ mqw_status mqw_plan_create(mqw_ctx* ctx, int count, const int* n, const int* m,
     P->p_off[k] = p_total;
     p_cnt[k] = opt.samples;
     p_total += opt.samples;
-    const bool grid = ni > res_max;
+    const bool grid = ni > res_max && ni >= 6;  // the grid path needs n >= 6
     auto add_walk = [&](int stages, int record_each, int p_at) {
       ResidentWalk w;
       w.inst = k;
@@ -568,7 +587,7 @@ mqw_status mqw_plan_create(mqw_ctx* ctx, int count, const int* n, const int* m,
     scratch = std::max(scratch, diag_scratch_bytes(ni, e - k));
     k = e;
   }
-  CK(P->d_diag_scratch.ensure(scratch));
+  P->diag_scratch_bytes = scratch;
   const size_t nj = P->jobs.size();
   CK(P->d_jobs.ensure(nj * sizeof(CoefJob)));
   CK(cudaMemcpyAsync(P->d_jobs.p, P->jobs.data(), nj * sizeof(CoefJob),
@@ -735,15 +754,15 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
                         float scale, const void* psi, void* out) {
   mqw_status s = check_ctx(ctx);
   if (s != MQW_OK) return s;
-  if ((precision != MQW_FP32 && precision != MQW_FP64) || n < 1 || n > MQW_MAX_N ||
+  if ((precision != MQW_FP32 && precision != MQW_FP64) || n < 6 || n > MQW_MAX_N ||
       K < 1 || !coeffs || !hp || !psi || !out)
-    return fail(ctx, MQW_ERR_INVALID, "clenshaw: bad arguments");
+    return fail(ctx, MQW_ERR_INVALID, "clenshaw: bad arguments (n must be in 6..30)");
   const size_t N = (size_t)1 << n;
   const size_t amp = precision == 0 ? 8 : 16;
-  const int lt = std::min(n, kMaxTileLog);
-  const int tiles = (int)(N >> lt);
+  const PassGeomHost geo = pass_geom(precision, n);
+  const int tiles = (int)(N >> geo.L);
   DevMem d_st, d_hp, d_c, d_np;
-  CK(d_st.ensure(3 * N * amp));
+  CK(d_st.ensure(4 * N * amp));
   CK(d_hp.ensure(N * sizeof(float)));
   CK(d_c.ensure(K * sizeof(float)));
   CK(d_np.ensure(tiles * sizeof(double)));
@@ -752,28 +771,33 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
   void* P0 = b;
   void* X = b + N * amp;
   void* Y = b + 2 * N * amp;
+  void* Pt = b + 3 * N * amp;
   CK(cudaMemcpyAsync(P0, psi, N * amp, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(d_hp.p, hp, N * sizeof(float), cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(d_c.p, coeffs, K * sizeof(float), cudaMemcpyHostToDevice, st));
   for (int r = K - 1; r >= 0; r--) {
-    TermParams tp{};
-    tp.n = n;
-    tp.lt = lt;
-    tp.count = 1;
-    TermTraj& T = tp.traj[0];
-    T.mode = (r == K - 1) ? kFirst : (r == K - 2) ? kSecond : kFull;
-    T.b1 = ((r + 1) & 1) ? Y : X;
-    T.b2 = (r & 1) ? Y : X;
-    T.psi = P0;
-    T.hp = d_hp.as<float>();
-    T.coef = d_c.as<float>() + r;
-    T.kappa = nullptr;
-    T.norm_part = d_np.as<double>();
-    T.gamma = gamma;
-    T.scale = scale;
-    T.odd = r & 1;
-    T.final_term = r == 0;
-    CK(launch_term(precision, tp, st));
+    PassParams pp{};
+    pp.n = n;
+    pp.L = geo.L;
+    pp.a = geo.a;
+    pp.tiling = (r & 1) ? 2 : 1;
+    pp.count = 1;
+    PassWalk& W = pp.walk[0];
+    W.active = 1;
+    W.bin = (r & 1) ? X : Y;
+    W.bout = (r & 1) ? Y : X;
+    W.part = Pt;
+    W.psi = P0;
+    W.hp = d_hp.as<float>();
+    W.coef = d_c.as<float>();
+    W.kappa = nullptr;
+    W.norm_part = d_np.as<double>();
+    W.gamma = gamma;
+    W.scale = scale;
+    W.r = r;
+    W.K = K;
+    W.psi_uniform = 0;
+    CK(launch_pass(precision, pp, st));
   }
   CK(cudaMemcpyAsync(out, X, N * amp, cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));

@@ -12,7 +12,7 @@ namespace mqw {
 constexpr int kSamples = 100;          // MultiQW.cpp:257
 constexpr int kMaxN = 30;
 constexpr int kMaxGroup = 8;           // trajectories per grid-path launch
-constexpr int kMaxTileLog = 11;        // grid-path tile: 2^11 amplitudes
+constexpr int kMaxTileLog = 13;        // grid-path tile: up to 2^13 amplitudes
 constexpr int kDiagChunkLog = 12;      // Gray ranks per diagonal chunk
 constexpr int kMaxChebTop = 16384;     // Miller start-index bound
 
@@ -99,29 +99,43 @@ cudaError_t launch_resident(int precision, const ResidentWalk* walks,
                             const DiagOut* diag, double* p_sample,
                             cudaStream_t stream);
 
-// Grid path: one Clenshaw term for up to kMaxGroup trajectories of the same n.
-enum TermMode : int { kSkip = 0, kFirst = 1, kSecond = 2, kFull = 3 };
-struct TermTraj {
-  const void* b1;      // b_{r+1}
-  void* b2;            // b_{r+2} in, b_r out (in place)
+// Grid path: one fused pass over tiles for up to kMaxGroup walks of the same
+// n. Pass r completes b_r (from the partial P_r and the axes the previous
+// pass could not see) and starts b_{r-1} (the partial P_{r-1} over the axes
+// internal to this pass's tiling). Passes alternate between two tilings:
+//   T1: 2^L consecutive amplitudes (axes [0, L));
+//   T2: 2^(L-a) rows of 2^a consecutive amplitudes, one row per value of the
+//       top L-a axes (axes [0, a) and [n-L+a, n)).
+// Axes in neither tiling ([L, n-L+a), when n > 2L-a) are read from global
+// memory during the finish.
+struct PassWalk {
+  const void* bin;     // b_{r+1}; may equal bout only when no axis is read
+                       // from global memory (nu == 0)
+  void* bout;          // b_r
+  void* part;          // P_r in, P_{r-1} out (in place)
   const void* psi;     // stage input state
   const float* hp;     // shifted diagonal
-  const float* coef;   // &coef[r]
+  const float* coef;   // coefficient list of this walk-stage (index r)
   const double* kappa; // 1/||psi|| of the stage input (nullptr = 1)
-  double* norm_part;   // final term: per-tile |b_0|^2 partials
+  double* norm_part;   // r == 0: per-tile |b_0|^2 partials
   float gamma;
-  float scale;         // onenorm (the final term uses 2*scale)
-  int mode;
-  int odd;             // r odd: coefficient is imaginary
-  int final_term;      // r == 0
+  float scale;         // onenorm
+  int r;               // term completed by this pass
+  int K;               // degree of this walk-stage
+  int psi_uniform;     // psi is the uniform state (psi0, 0): not read
+  int active;
 };
-struct TermParams {
-  int n;
-  int lt;              // log2 tile size
+struct PassParams {
+  int n, L, a;
+  int tiling;          // 1 or 2
   int count;
-  TermTraj traj[kMaxGroup];
+  PassWalk walk[kMaxGroup];
 };
-cudaError_t launch_term(int precision, const TermParams& p,
+struct PassGeomHost {
+  int L, a, nu;        // tile log, row log, axes read from global memory
+};
+PassGeomHost pass_geom(int precision, int n);
+cudaError_t launch_pass(int precision, const PassParams& p,
                         cudaStream_t stream);
 
 // Finalisation after a stage: kappa[g] = 1/sqrt(sum of partials); when

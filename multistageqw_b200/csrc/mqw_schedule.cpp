@@ -11,6 +11,7 @@
 #include <random>
 
 #include "../../include/mqw.h"
+#include "mqw_cheb.h"
 
 namespace {
 
@@ -112,6 +113,20 @@ mqw_status mqw_schedule(int n, int m, const double* raw, float* gammas,
     for (int j = MQW_SAMPLES - 1; j >= 1; j--) times[j] -= times[j - 1];
   }
   if (total_t_out) *total_t_out = total_t;
+  return MQW_OK;
+}
+
+mqw_status mqw_cheb_coeffs_host(int count, const double* s, double tol,
+                                int max_k, float* coeffs, int* degrees) {
+  if (count < 0 || max_k < 1 || (count > 0 && (!s || !coeffs || !degrees)) ||
+      !(tol > 0.0))
+    return MQW_ERR_INVALID;
+  for (int i = 0; i < count; i++) {
+    float* out = coeffs + (size_t)i * max_k;
+    std::fill(out, out + max_k, 0.0f);
+    degrees[i] = mqw::cheb_coeffs_stream(s[i], tol, out, max_k);
+    if (degrees[i] < 1) return MQW_ERR_INVALID;
+  }
   return MQW_OK;
 }
 

@@ -109,3 +109,12 @@ def test_no_gpu_context_fails_loudly(mqw):
 
 def test_sk_generator_matches_oracle(mqw, orc):
     assert np.array_equal(mqw.sk_instances(9, 4, 2), orc.sk_instances(9, 4, 2))
+
+
+def test_cheb_host_build_bit_exact_vs_oracle(mqw, orc):
+    s = np.array([1e-9, 2e-7, 1e-3, 0.37, 1.0, 3.3, 12.3, 37.0, 99.9, 150.0, 420.0, 901.5, 2500.0])
+    coeffs, K = mqw.cheb_coeffs_host(s)
+    for i, sv in enumerate(s):
+        ref = orc.cheb_coeffs(sv).astype(np.float32)
+        assert K[i] == len(ref), sv
+        assert np.array_equal(coeffs[i].view(np.uint32), ref.view(np.uint32)), sv

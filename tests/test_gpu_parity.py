@@ -58,7 +58,7 @@ def _planar_to_complex(x):
     return x[:N] + 1j * x[N:]
 
 
-@pytest.mark.parametrize("n", [3, 9, 11, 12, 15])
+@pytest.mark.parametrize("n", [6, 9, 11, 12, 15, 17])
 def test_clenshaw_single_propagation(ctx, orc, n):
     N = 1 << n
     raw = orc.sk_instances(n, 1, 40 + n)[0]
