@@ -13,7 +13,9 @@
  *  - Every call returns an mqw_status; nothing aborts the process.
  *  - The caller owns host buffers; a context owns its device buffers.
  *  - One context per host thread. Calls on one context are serialised by the
- *    caller.
+ *    caller, and plan executions of one context must also be ordered on the
+ *    device (one stream, or a synchronisation between them): the plans share
+ *    the context's scratch buffers.
  *  - Instance layout (MultiQW.cpp:270-323): per instance n(n+1)/2 float64
  *    values; first the n(n-1)/2 couplings J(i,j) for i = 1..n-1, j = 0..i-1
  *    in that loop order, then the n fields h(0..n-1).
@@ -63,6 +65,10 @@ typedef struct mqw_options {
   const float* stage_scale; /* optional [count][m][2] multipliers applied to
                                (gamma_i, t_i) of each stage (a learned
                                schedule); NULL = the paper heuristic */
+  int tile_log;    /* grid-path tile (log2 amplitudes), 0 = autotuned */
+  int graph;       /* 1 (default): a plan's second and later executions
+                      replay a CUDA graph of its whole device pipeline;
+                      0: launch kernels one by one every time */
 } mqw_options;
 
 typedef struct mqw_diag_info {

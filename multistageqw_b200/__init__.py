@@ -53,6 +53,8 @@ class Options(ctypes.Structure):
         ("group", ctypes.c_int),
         ("resident_max_n", ctypes.c_int),
         ("stage_scale", ctypes.POINTER(ctypes.c_float)),
+        ("tile_log", ctypes.c_int),
+        ("graph", ctypes.c_int),
     ]
 
 
@@ -148,7 +150,7 @@ def _ptr(a, ct):
 
 
 def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_max_n=0,
-          stage_scale=None):
+          stage_scale=None, tile_log=0, graph=1):
     o = Options()
     lib().mqw_default_options(ctypes.byref(o))
     o.precision = {"fp32": FP32, "fp64": FP64, FP32: FP32, FP64: FP64}[precision]
@@ -156,6 +158,8 @@ def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_ma
     o.cheb_tol = float(cheb_tol)
     o.group = int(group)
     o.resident_max_n = int(resident_max_n)
+    o.tile_log = int(tile_log)
+    o.graph = int(graph)
     keep = None
     if stage_scale is not None:
         keep = np.ascontiguousarray(stage_scale, dtype=np.float32)

@@ -68,7 +68,17 @@ struct mqw_ctx {
   cudaStream_t stream = nullptr;
   std::string err;
   int sm_count = 0;
-  DevMem state, norm_part, kappa, coef, coef_off, stages, walks, diag_scratch;
+  DevMem state, norm_part, kappa, diag_scratch, tune_coef;
+  // Bumped whenever a shared scratch buffer is reallocated: a plan's captured
+  // graph holds the old addresses and is re-captured when this changes.
+  unsigned long long scratch_gen = 1;
+  // Autotuned grid-path geometry per (precision, n): tile cap and group size.
+  std::map<std::pair<int, int>, std::pair<int, int>> tuned;
+  cudaError_t grow(DevMem& m, size_t bytes) {
+    if (bytes <= m.bytes && m.p) return cudaSuccess;
+    scratch_gen++;
+    return m.ensure(bytes);
+  }
 };
 
 namespace {
@@ -104,6 +114,8 @@ void default_opts(mqw_options* o) {
   o->group = 0;
   o->resident_max_n = 0;
   o->stage_scale = nullptr;
+  o->tile_log = 0;
+  o->graph = 1;
 }
 
 }  // namespace
@@ -129,6 +141,14 @@ struct mqw_plan {
   DevMem d_jobs, d_degree, d_onenorm;
   DevMem d_p_sample, d_p_mean, d_p_off, d_p_cnt;
   size_t diag_scratch_bytes = 0;
+  // Coefficient pool and launch tables (plan-owned: a captured graph reads them).
+  DevMem d_coef, d_coef_off, d_stages, d_walks;
+  // Grid-path geometry chosen for each n of the plan: (tile cap, group).
+  std::map<int, std::pair<int, int>> grid_geo;
+  // CUDA graph of the whole device pipeline, replayed by later executes.
+  cudaGraphExec_t gexec = nullptr;
+  unsigned long long graph_gen = 0;
+  bool counting = true;  // stats are counted while issuing eagerly
   // Host copies of the degree read-back.
   std::vector<int> degree;
   std::vector<float> onenorm;
@@ -140,6 +160,7 @@ struct mqw_plan {
   bool timed = false;
   double create_h2d = 0.0;  // bytes uploaded by plan_create
   ~mqw_plan() {
+    if (gexec) cudaGraphExecDestroy(gexec);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
   }
@@ -149,6 +170,9 @@ namespace {
 
 mqw_status check_ctx(mqw_ctx* ctx) {
   if (!ctx) return MQW_ERR_INVALID;
+  // A non-sticky error left by the caller's own CUDA calls is not ours to
+  // report from the launches below.
+  (void)cudaGetLastError();
   cudaError_t e = cudaSetDevice(ctx->device);
   if (e != cudaSuccess)
     return fail(ctx, MQW_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
@@ -157,19 +181,118 @@ mqw_status check_ctx(mqw_ctx* ctx) {
 
 int walk_slots(const PassGeomHost& geo) { return geo.nu > 0 ? 4 : 3; }
 
-int choose_group(const mqw_plan& P, int n) {
-  if (P.opt.group > 0) return std::min(P.opt.group, kMaxGroup);
-  const size_t amp = P.precision == 0 ? 8 : 16;
-  const size_t walk_bytes =
-      (walk_slots(pass_geom(P.precision, n)) * amp + sizeof(float)) * ((size_t)1 << n);
-  // Keep a launch's working set within ~60 MB (about one die's share of the
-  // 126 MB L2, which both dies' SMs read from), but give every launch at
-  // least ~2^20 amplitudes.
-  size_t g = (60u << 20) / walk_bytes;
+size_t walk_bytes(int precision, const PassGeomHost& geo, int n) {
+  const size_t amp = precision == 0 ? 8 : 16;
+  return (walk_slots(geo) * amp + sizeof(float)) * ((size_t)1 << n);
+}
+
+// Default group size: keep a launch's working set within ~60 MB (about one
+// die's share of the 126 MB L2, which both dies' SMs read from), but give
+// every launch at least ~2^20 amplitudes.
+int default_group(int precision, const PassGeomHost& geo, int n) {
+  size_t g = (60u << 20) / walk_bytes(precision, geo, n);
   if (((size_t)1 << n) * g < ((size_t)1 << 20)) g = ((size_t)1 << 20) >> n;
   if (g < 1) g = 1;
   if (g > (size_t)kMaxGroup) g = kMaxGroup;
   return (int)g;
+}
+
+// Times one configuration of the grid path: `reps` full passes (both
+// tilings) over G zero-filled walks. Returns microseconds per walk-pass.
+mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
+                            int G, double* us_per_walk) {
+  const PassGeomHost geo = pass_geom(precision, n, lmax);
+  const size_t N = (size_t)1 << n;
+  const size_t amp = precision == 0 ? 8 : 16;
+  const int slots = walk_slots(geo);
+  CK(ctx->grow(ctx->state, (size_t)G * slots * N * amp + N * sizeof(float)));
+  CK(ctx->grow(ctx->norm_part, (size_t)G * (N >> geo.L) * sizeof(double)));
+  CK(ctx->tune_coef.ensure(64 * sizeof(float)));
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemsetAsync(ctx->state.p, 0, (size_t)G * slots * N * amp + N * sizeof(float), st));
+  CK(cudaMemsetAsync(ctx->tune_coef.p, 0, 64 * sizeof(float), st));
+  char* base = ctx->state.as<char>();
+  const float* hp = reinterpret_cast<const float*>(base + (size_t)G * slots * N * amp);
+  auto issue = [&](int r) -> cudaError_t {
+    PassParams pp{};
+    pp.n = n;
+    pp.L = geo.L;
+    pp.a = geo.a;
+    pp.tiling = (r & 1) ? 2 : 1;
+    pp.count = G;
+    for (int g = 0; g < G; g++) {
+      PassWalk& W = pp.walk[g];
+      char* w = base + (size_t)g * slots * N * amp;
+      W.active = 1;
+      W.bin = w + N * amp;
+      W.bout = w + (slots == 4 ? 3 : 1) * N * amp;
+      W.part = w + 2 * N * amp;
+      W.psi = w;
+      W.hp = hp;
+      W.coef = ctx->tune_coef.as<float>();
+      W.kappa = nullptr;
+      W.norm_part = ctx->norm_part.as<double>() + (size_t)g * (N >> geo.L);
+      W.gamma = 1.0f;
+      W.scale = 64.0f;
+      W.r = r;
+      W.K = 40;
+      W.psi_uniform = 0;
+      W.psi0 = 0.0f;
+    }
+    return launch_pass(precision, pp, st);
+  };
+  for (int r = 4; r >= 1; r--) CK(issue(r));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const int reps = 12;
+  CK(cudaEventRecord(e0, st));
+  for (int r = reps; r >= 1; r--) CK(issue(r));
+  CK(cudaEventRecord(e1, st));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.0f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *us_per_walk = 1000.0 * ms / (reps * G);
+  return MQW_OK;
+}
+
+// Autotuner: picks the grid-path tile cap and group size for (precision, n)
+// by timing the candidates once per context; the result is cached.
+mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, int* lmax, int* G) {
+  const auto key = std::make_pair(precision, n);
+  auto it = ctx->tuned.find(key);
+  if (it != ctx->tuned.end()) {
+    *lmax = it->second.first;
+    *G = it->second.second;
+    return MQW_OK;
+  }
+  const int def_l = precision == 0 ? 12 : 11;
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)8 << 30;
+  const size_t budget = std::min(free_b / 4, (size_t)16 << 30);
+  double best = 1e300;
+  int best_l = def_l, best_g = 1;
+  for (int l = def_l; l >= def_l - 1; l--) {
+    const PassGeomHost geo = pass_geom(precision, n, l);
+    const int g0 = default_group(precision, geo, n);
+    for (int g : {1, 2, 3, 4, g0}) {
+      if (g > kMaxGroup || (size_t)g * walk_bytes(precision, geo, n) > budget) continue;
+      double us = 0.0;
+      mqw_status s = time_grid_config(ctx, precision, n, l, g, &us);
+      if (s != MQW_OK) return s;
+      if (us < best * 0.98) {  // prefer the earlier (larger tile, smaller group) on ties
+        best = us;
+        best_l = l;
+        best_g = g;
+      }
+    }
+  }
+  ctx->tuned[key] = std::make_pair(best_l, best_g);
+  *lmax = best_l;
+  *G = best_g;
+  return MQW_OK;
 }
 
 // Runs a group of grid-path walks (all the same n) through all their stages.
@@ -179,11 +302,10 @@ int choose_group(const mqw_plan& P, int n) {
 // walk at 3 vectors so that two walks of n = 20 stay resident in L2. Pass r
 // uses tiling 1 for even r and tiling 2 for odd r.
 mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
-                          cudaStream_t stream) {
+                          const PassGeomHost& geo, cudaStream_t stream) {
   mqw_ctx* ctx = P.ctx;
   const int n = P.walks[widx[0]].n;
   const size_t N = (size_t)1 << n;
-  const PassGeomHost geo = pass_geom(P.precision, n);
   const int tiles = (int)(N >> geo.L);
   const int G = (int)widx.size();
   const size_t amp = P.precision == 0 ? 8 : 16;
@@ -202,7 +324,7 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
   double* norm_part = P.ctx->norm_part.as<double>();
   double* kappa = P.ctx->kappa.as<double>();
   double* p_sample = P.d_p_sample.as<double>();
-  const float* coef = P.ctx->coef.as<float>();
+  const float* coef = P.d_coef.as<float>();
   const float* hp = P.d_hp.as<float>();
   const DiagOut* diag = P.d_diag.as<DiagOut>();
   int max_stages = 0;
@@ -244,11 +366,14 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
         W.r = r;
         W.K = K[g];
         W.psi_uniform = st == 0;  // every walk starts from the uniform state
-        P.stats.term_amps += (double)N;
+        W.psi0 = (float)(1.0 / std::sqrt((double)N));
+        if (P.counting) P.stats.term_amps += (double)N;
       }
       CK(launch_pass(P.precision, pp, stream));
-      P.stats.launches++;
-      P.stats.term_launches++;
+      if (P.counting) {
+        P.stats.launches++;
+        P.stats.term_launches++;
+      }
     }
     FinalParams fp{};
     int fc = 0;
@@ -267,7 +392,7 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
     }
     fp.count = fc;
     CK(launch_finalize(P.precision, fp, stream));
-    P.stats.launches++;
+    if (P.counting) P.stats.launches++;
     for (int g = 0; g < G; g++) {
       if (st >= P.walks[widx[g]].stages) continue;
       std::swap(pi[g], xs[g]);  // the output (slot x) becomes psi
@@ -276,36 +401,135 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
   return MQW_OK;
 }
 
-mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
+// Diagonals (per group of equal n; instances are sorted by n) and the degree
+// pass.
+mqw_status issue_diag_degree(mqw_plan& P, cudaStream_t stream) {
   mqw_ctx* ctx = P.ctx;
-  const int count = P.count;
-  // 1. Diagonals, per group of equal n (instances are sorted by n).
-  CK(ctx->diag_scratch.ensure(P.diag_scratch_bytes));
   DiagOut* d_diag = P.d_diag.as<DiagOut>();
-  for (int s = 0; s < count;) {
+  for (int s = 0; s < P.count;) {
     const int n = P.n[P.order[s]];
     int e = s;
-    while (e < count && P.n[P.order[e]] == n) e++;
+    while (e < P.count && P.n[P.order[e]] == n) e++;
     CK(launch_diag(n, e - s, P.d_raw.as<double>() + P.raw_off[s],
                    P.d_hp.as<float>() + P.hp_off[s], nullptr, d_diag + s,
                    P.ctx->diag_scratch.p, stream));
-    P.stats.launches += 3;
+    if (P.counting) P.stats.launches += 3;
     s = e;
   }
-  // 2. Degrees and onenorms, read back.
+  CK(launch_cheb_degree(P.d_jobs.as<CoefJob>(), (int)P.jobs.size(), d_diag,
+                        P.opt.cheb_tol, P.d_degree.as<int>(),
+                        P.d_onenorm.as<float>(), stream));
+  if (P.counting) P.stats.launches++;
+  return MQW_OK;
+}
+
+// Coefficients, propagation (resident and grid walks) and the means.
+mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
+  mqw_ctx* ctx = P.ctx;
   const int nj = (int)P.jobs.size();
-  CK(launch_cheb_degree(P.d_jobs.as<CoefJob>(), nj, d_diag, P.opt.cheb_tol,
-                        P.d_degree.as<int>(), P.d_onenorm.as<float>(), stream));
-  P.stats.launches++;
+  DiagOut* d_diag = P.d_diag.as<DiagOut>();
+  CK(launch_cheb_coeffs(P.d_jobs.as<CoefJob>(), nj, d_diag, P.opt.cheb_tol,
+                        P.d_coef_off.as<long long>(), P.d_coef.as<float>(),
+                        stream));
+  if (P.counting) P.stats.launches++;
+  if (P.counting) CK(cudaEventRecord(P.ev0, stream));
+  int res_count = 0, res_max_n = 0;
+  std::map<int, std::vector<int>> grid_by_n;
+  for (size_t w = 0; w < P.walks.size(); w++) {
+    if (P.walk_is_grid[w]) {
+      grid_by_n[P.walks[w].n].push_back((int)w);
+    } else {
+      res_count++;
+      res_max_n = std::max(res_max_n, P.walks[w].n);
+    }
+  }
+  if (res_count > 0) {
+    CK(launch_resident(P.precision, P.d_walks.as<ResidentWalk>(), res_count,
+                       res_max_n, P.d_stages.as<StageDesc>(),
+                       P.d_coef.as<float>(), P.d_hp.as<float>(), d_diag,
+                       P.d_p_sample.as<double>(), stream));
+    if (P.counting) P.stats.launches++;
+  }
+  for (auto& kv : grid_by_n) {
+    const int n = kv.first;
+    const std::pair<int, int> lg = P.grid_geo.at(n);
+    const PassGeomHost geo = pass_geom(P.precision, n, lg.first);
+    const int G = lg.second;
+    const std::vector<int>& ws = kv.second;
+    for (size_t i = 0; i < ws.size(); i += G) {
+      std::vector<int> grp(ws.begin() + i, ws.begin() + std::min(ws.size(), i + G));
+      mqw_status s = run_grid_group(P, grp, geo, stream);
+      if (s != MQW_OK) return s;
+    }
+  }
+  if (P.counting) CK(cudaEventRecord(P.ev1, stream));
+  CK(launch_mean(P.d_p_sample.as<double>(), P.d_p_off.as<int>(),
+                 P.d_p_cnt.as<int>(), P.count, P.d_p_mean.as<double>(), stream));
+  if (P.counting) P.stats.launches++;
+  return MQW_OK;
+}
+
+mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
+  mqw_ctx* ctx = P.ctx;
+  if (!P.ev0) CK(cudaEventCreate(&P.ev0));
+  if (!P.ev1) CK(cudaEventCreate(&P.ev1));
+  // Replay the captured pipeline when the shared scratch it was captured
+  // with is still in place.
+  // (Its timing events bracket the whole graph: the diagonal and coefficient
+  // kernels add < 0.3% to the propagation they time in an eager run.)
+  if (P.gexec && P.graph_gen == ctx->scratch_gen) {
+    CK(cudaEventRecord(P.ev0, stream));
+    CK(cudaGraphLaunch(P.gexec, stream));
+    CK(cudaEventRecord(P.ev1, stream));
+    P.timed = true;
+    P.executed = true;
+    return MQW_OK;
+  }
+  P.counting = true;
+  P.stats.launches = P.stats.term_launches = 0;
+  P.stats.h2d_bytes = P.stats.d2h_bytes = 0;
+  // Geometry and shared scratch for every n of the plan, sized up front so
+  // that nothing is allocated while the pipeline is issued or captured.
+  std::map<int, int> grid_count;
+  for (size_t w = 0; w < P.walks.size(); w++)
+    if (P.walk_is_grid[w]) grid_count[P.walks[w].n]++;
+  size_t state_b = 0, norm_b = 0;
+  for (auto& kv : grid_count) {
+    const int n = kv.first;
+    int lmax = P.opt.tile_log, G = P.opt.group;
+    if (lmax <= 0 || G <= 0) {
+      int tl = 0, tg = 0;
+      mqw_status s = tune_grid(ctx, P.precision, n, &tl, &tg);
+      if (s != MQW_OK) return s;
+      if (lmax <= 0) lmax = tl;
+      if (G <= 0) G = tg;
+    }
+    G = std::min(std::min(G, kMaxGroup), kv.second);
+    const PassGeomHost geo = pass_geom(P.precision, n, lmax);
+    P.grid_geo[n] = std::make_pair(lmax, G);
+    const size_t N = (size_t)1 << n;
+    const size_t amp = P.precision == 0 ? 8 : 16;
+    state_b = std::max(state_b, (size_t)G * walk_slots(geo) * N * amp);
+    norm_b = std::max(norm_b, (size_t)G * (N >> geo.L) * sizeof(double));
+  }
+  CK(ctx->grow(ctx->diag_scratch, P.diag_scratch_bytes));
+  if (state_b) CK(ctx->grow(ctx->state, state_b));
+  if (norm_b) CK(ctx->grow(ctx->norm_part, norm_b));
+  CK(ctx->grow(ctx->kappa, kMaxGroup * sizeof(double)));
+
+  // 1-2. Diagonals and degrees; degrees and onenorms are read back to lay
+  // out the coefficient pool and the launch schedule.
+  mqw_status s = issue_diag_degree(P, stream);
+  if (s != MQW_OK) return s;
+  const int nj = (int)P.jobs.size();
   P.degree.resize(nj);
   P.onenorm.resize(nj);
   CK(cudaMemcpyAsync(P.degree.data(), P.d_degree.p, nj * sizeof(int),
                      cudaMemcpyDeviceToHost, stream));
-  P.stats.d2h_bytes += (double)nj * (sizeof(int) + sizeof(float));
   CK(cudaMemcpyAsync(P.onenorm.data(), P.d_onenorm.p, nj * sizeof(float),
                      cudaMemcpyDeviceToHost, stream));
+  P.stats.d2h_bytes += (double)nj * (sizeof(int) + sizeof(float));
   CK(cudaStreamSynchronize(stream));
-  // 3. Coefficient pool.
   P.coef_off.assign(nj + 1, 0);
   P.stats.terms = 0;
   for (int j = 0; j < nj; j++) {
@@ -315,20 +539,6 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     P.coef_off[j + 1] = P.coef_off[j] + P.degree[j];
     P.stats.terms += P.degree[j];
   }
-  CK(P.ctx->coef_off.ensure((nj + 1) * sizeof(long long)));
-  CK(cudaMemcpyAsync(P.ctx->coef_off.p, P.coef_off.data(),
-                     (nj + 1) * sizeof(long long), cudaMemcpyHostToDevice,
-                     stream));
-  P.stats.h2d_bytes += (double)(nj + 1) * sizeof(long long) + (double)nj * sizeof(StageDesc);
-  CK(P.ctx->coef.ensure(P.coef_off[nj] * sizeof(float)));
-  CK(launch_cheb_coeffs(P.d_jobs.as<CoefJob>(), nj, d_diag, P.opt.cheb_tol,
-                        P.ctx->coef_off.as<long long>(), P.ctx->coef.as<float>(),
-                        stream));
-  P.stats.launches++;
-  // 4a. Resident walks.
-  if (!P.ev0) CK(cudaEventCreate(&P.ev0));
-  if (!P.ev1) CK(cudaEventCreate(&P.ev1));
-  CK(cudaEventRecord(P.ev0, stream));
   std::vector<StageDesc> sdesc(nj);
   for (int j = 0; j < nj; j++) {
     sdesc[j].coef_off = P.coef_off[j];
@@ -336,62 +546,62 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     sdesc[j].gamma = P.jobs[j].gamma;
     sdesc[j].onenorm = P.onenorm[j];
   }
-  CK(P.ctx->stages.ensure(nj * sizeof(StageDesc)));
-  CK(cudaMemcpyAsync(P.ctx->stages.p, sdesc.data(), nj * sizeof(StageDesc),
-                     cudaMemcpyHostToDevice, stream));
   std::vector<ResidentWalk> res;
-  int res_max_n = 0;
-  std::map<int, std::vector<int>> grid_by_n;
-  for (size_t w = 0; w < P.walks.size(); w++) {
-    if (P.walk_is_grid[w]) {
-      grid_by_n[P.walks[w].n].push_back((int)w);
-    } else {
-      res.push_back(P.walks[w]);
-      res_max_n = std::max(res_max_n, P.walks[w].n);
-    }
-  }
   P.stats.term_amps = 0;
   for (size_t w = 0; w < P.walks.size(); w++) {
     if (P.walk_is_grid[w]) continue;
+    res.push_back(P.walks[w]);
     for (int st = 0; st < P.walks[w].stages; st++)
       P.stats.term_amps += (double)P.degree[P.walks[w].stage_desc_off + st] *
                            (double)(1u << P.walks[w].n);
   }
-  if (!res.empty()) {
-    CK(P.ctx->walks.ensure(res.size() * sizeof(ResidentWalk)));
-    CK(cudaMemcpyAsync(P.ctx->walks.p, res.data(), res.size() * sizeof(ResidentWalk),
+  // A re-layout drops any captured graph (its addresses may change).
+  if (P.gexec) {
+    cudaGraphExecDestroy(P.gexec);
+    P.gexec = nullptr;
+  }
+  CK(P.d_coef_off.ensure((nj + 1) * sizeof(long long)));
+  CK(P.d_coef.ensure(P.coef_off[nj] * sizeof(float)));
+  CK(P.d_stages.ensure(nj * sizeof(StageDesc)));
+  CK(P.d_walks.ensure(std::max<size_t>(1, res.size()) * sizeof(ResidentWalk)));
+  CK(cudaMemcpyAsync(P.d_coef_off.p, P.coef_off.data(), (nj + 1) * sizeof(long long),
+                     cudaMemcpyHostToDevice, stream));
+  CK(cudaMemcpyAsync(P.d_stages.p, sdesc.data(), nj * sizeof(StageDesc),
+                     cudaMemcpyHostToDevice, stream));
+  if (!res.empty())
+    CK(cudaMemcpyAsync(P.d_walks.p, res.data(), res.size() * sizeof(ResidentWalk),
                        cudaMemcpyHostToDevice, stream));
-    P.stats.h2d_bytes += (double)res.size() * sizeof(ResidentWalk);
-    CK(launch_resident(P.precision, P.ctx->walks.as<ResidentWalk>(), (int)res.size(),
-                       res_max_n, P.ctx->stages.as<StageDesc>(),
-                       P.ctx->coef.as<float>(), P.d_hp.as<float>(), d_diag,
-                       P.d_p_sample.as<double>(), stream));
-    P.stats.launches++;
-  }
-  // 4b. Grid walks, in groups of equal n.
-  for (auto& kv : grid_by_n) {
-    const int n = kv.first;
-    const int G = choose_group(P, n);
-    const size_t N = (size_t)1 << n;
-    const size_t amp = P.precision == 0 ? 8 : 16;
-    const PassGeomHost geo = pass_geom(P.precision, n);
-    CK(P.ctx->state.ensure((size_t)G * walk_slots(geo) * N * amp));
-    CK(P.ctx->norm_part.ensure((size_t)G * (N >> geo.L) * sizeof(double)));
-    CK(P.ctx->kappa.ensure(kMaxGroup * sizeof(double)));
-    const std::vector<int>& ws = kv.second;
-    for (size_t i = 0; i < ws.size(); i += G) {
-      std::vector<int> grp(ws.begin() + i, ws.begin() + std::min(ws.size(), i + G));
-      mqw_status s = run_grid_group(P, grp, stream);
-      if (s != MQW_OK) return s;
-    }
-  }
-  CK(cudaEventRecord(P.ev1, stream));
+  P.stats.h2d_bytes += (double)(nj + 1) * sizeof(long long) +
+                       (double)nj * sizeof(StageDesc) +
+                       (double)res.size() * sizeof(ResidentWalk);
+  // 3-5. Coefficients, propagation, means.
+  s = issue_rest(P, stream);
+  if (s != MQW_OK) return s;
   P.timed = true;
-  // 5. Means per instance (sorted order).
-  CK(launch_mean(P.d_p_sample.as<double>(), P.d_p_off.as<int>(),
-                 P.d_p_cnt.as<int>(), count, P.d_p_mean.as<double>(), stream));
-  P.stats.launches++;
   P.executed = true;
+  // Capture the whole device pipeline for later executes. The capture runs
+  // on the context's private stream (nothing executes while capturing); the
+  // graph is later launched on whatever stream the caller passes.
+  if (P.opt.graph) {
+    CK(cudaStreamSynchronize(stream));
+    cudaStream_t cs = ctx->stream;
+    P.counting = false;
+    CK(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    mqw_status s1 = issue_diag_degree(P, cs);
+    mqw_status s2 = s1 == MQW_OK ? issue_rest(P, cs) : s1;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(cs, &graph);
+    P.counting = true;
+    if (s2 != MQW_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return s2;
+    }
+    CK(ec);
+    const cudaError_t ei = cudaGraphInstantiate(&P.gexec, graph, 0);
+    cudaGraphDestroy(graph);
+    CK(ei);
+    P.graph_gen = ctx->scratch_gen;
+  }
   return MQW_OK;
 }
 
@@ -613,10 +823,6 @@ mqw_status mqw_plan_execute(mqw_plan* plan, void* stream) {
   mqw_status s = check_ctx(ctx);
   if (s != MQW_OK) return s;
   cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
-  plan->stats.h2d_bytes = 0;
-  plan->stats.d2h_bytes = 0;
-  plan->stats.launches = 0;
-  plan->stats.term_launches = 0;
   plan->timed = false;
   return plan_execute(*plan, st);
 }
@@ -664,6 +870,8 @@ mqw_status mqw_plan_stats(const mqw_plan* plan, mqw_run_stats* stats) {
     if (cudaEventSynchronize(plan->ev1) == cudaSuccess &&
         cudaEventElapsedTime(&ms, plan->ev0, plan->ev1) == cudaSuccess)
       stats->kernel_ms = ms;
+    else
+      (void)cudaGetLastError();  // leave no pending error behind
   }
   return MQW_OK;
 }

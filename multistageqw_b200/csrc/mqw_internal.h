@@ -124,6 +124,7 @@ struct PassWalk {
   int K;               // degree of this walk-stage
   int psi_uniform;     // psi is the uniform state (psi0, 0): not read
   int active;
+  float psi0;          // float(1/sqrt(2^n)), the uniform amplitude
 };
 struct PassParams {
   int n, L, a;
@@ -134,7 +135,9 @@ struct PassParams {
 struct PassGeomHost {
   int L, a, nu;        // tile log, row log, axes read from global memory
 };
-PassGeomHost pass_geom(int precision, int n);
+// Geometry for n; lmax > 0 caps the tile (log2 amplitudes), else the
+// precision's default cap (or MQW_PASS_TILE_LOG) applies.
+PassGeomHost pass_geom(int precision, int n, int lmax = 0);
 cudaError_t launch_pass(int precision, const PassParams& p,
                         cudaStream_t stream);
 

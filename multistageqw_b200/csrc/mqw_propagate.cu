@@ -252,47 +252,136 @@ __device__ __forceinline__ V4<R> shfl4(const V4<R>& v, int lane_mask) {
           __shfl_xor_sync(0xffffffffu, v.w, lane_mask)};
 }
 
-// Sum over tile axes [q0, q1) of the partners of register pair j, where pair
-// index pp = tid | (j << logT): tile bit 0 is inside the pair, bits 1..5 are
-// lane bits (shuffles), bits 6..logT are warp bits (shared memory sx), and
-// the top bits index the thread's own registers v[].
-template <typename R, int RP>
-__device__ __forceinline__ V4<R> axis_sum(const V4<R> (&v)[RP], int j,
-                                          const R* sx, int logT, int q0,
-                                          int q1, int tid) {
-  V4<R> acc{0, 0, 0, 0};
-  if (q0 <= 0 && 0 < q1) add4<R>(acc, V4<R>{v[j].z, v[j].w, v[j].x, v[j].y});
-  const int l1 = min(q1, 6);
-  for (int q = max(q0, 1); q < l1; q++) add4<R>(acc, shfl4<R>(v[j], 1 << (q - 1)));
-  const int w1 = min(q1, logT + 1);
-  const int pp = tid | (j << logT);
-  for (int q = max(q0, 6); q < w1; q++) add4<R>(acc, ld4<R>(sx + 4 * (pp ^ (1 << (q - 1)))));
+// A pair of neighbouring amplitudes as the hot loops carry it. FP32: two
+// 64-bit registers, each a packed (re, im), accumulated with sm_100's
+// add.rn.f32x2 and exchanged with 64-bit shuffles; FP64: two double2.
+template <typename R> struct Pair;
+template <> struct Pair<float> { unsigned long long a, b; };
+template <> struct Pair<double> { double2 a, b; };
+
+__device__ __forceinline__ Pair<float> pld(const float* p) {
+  const ulonglong2 t = *reinterpret_cast<const ulonglong2*>(p);
+  return {t.x, t.y};
+}
+__device__ __forceinline__ Pair<double> pld(const double* p) {
+  return {reinterpret_cast<const double2*>(p)[0], reinterpret_cast<const double2*>(p)[1]};
+}
+__device__ __forceinline__ void pst(float* p, const Pair<float>& v) {
+  *reinterpret_cast<ulonglong2*>(p) = make_ulonglong2(v.a, v.b);
+}
+__device__ __forceinline__ void pst(double* p, const Pair<double>& v) {
+  reinterpret_cast<double2*>(p)[0] = v.a;
+  reinterpret_cast<double2*>(p)[1] = v.b;
+}
+__device__ __forceinline__ Pair<float> pshfl(const Pair<float>& v, int m) {
+  return {__shfl_xor_sync(0xffffffffu, v.a, m), __shfl_xor_sync(0xffffffffu, v.b, m)};
+}
+__device__ __forceinline__ Pair<double> pshfl(const Pair<double>& v, int m) {
+  return {make_double2(__shfl_xor_sync(0xffffffffu, v.a.x, m), __shfl_xor_sync(0xffffffffu, v.a.y, m)),
+          make_double2(__shfl_xor_sync(0xffffffffu, v.b.x, m), __shfl_xor_sync(0xffffffffu, v.b.y, m))};
+}
+__device__ __forceinline__ void padd(Pair<float>& acc, const Pair<float>& v) {
+  asm("add.rn.f32x2 %0, %0, %1;" : "+l"(acc.a) : "l"(v.a));
+  asm("add.rn.f32x2 %0, %0, %1;" : "+l"(acc.b) : "l"(v.b));
+}
+__device__ __forceinline__ void padd(Pair<double>& acc, const Pair<double>& v) {
+  acc.a.x += v.a.x;
+  acc.a.y += v.a.y;
+  acc.b.x += v.b.x;
+  acc.b.y += v.b.y;
+}
+template <typename R> __device__ __forceinline__ Pair<R> pzero();
+template <> __device__ __forceinline__ Pair<float> pzero<float>() { return {0ull, 0ull}; }
+template <> __device__ __forceinline__ Pair<double> pzero<double>() {
+  return {make_double2(0.0, 0.0), make_double2(0.0, 0.0)};
+}
+template <typename R>
+__device__ __forceinline__ Pair<R> pswap(const Pair<R>& v) { return {v.b, v.a}; }
+
+// Register-pair views (no data movement).
+__device__ __forceinline__ V4<float> to4(const Pair<float>& v) {
+  float x, y, z, w;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(x), "=f"(y) : "l"(v.a));
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(z), "=f"(w) : "l"(v.b));
+  return {x, y, z, w};
+}
+__device__ __forceinline__ V4<double> to4(const Pair<double>& v) {
+  return {v.a.x, v.a.y, v.b.x, v.b.y};
+}
+__device__ __forceinline__ Pair<float> from4(const V4<float>& v) {
+  unsigned long long a, b;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(a) : "f"(v.x), "f"(v.y));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(b) : "f"(v.z), "f"(v.w));
+  return {a, b};
+}
+__device__ __forceinline__ Pair<double> from4(const V4<double>& v) {
+  return {make_double2(v.x, v.y), make_double2(v.z, v.w)};
+}
+
+// Sum over tile axes q in [q0, q1) of the partners of register pair j. The
+// pair index of register j is pp = tid | (j << LOGT): tile bit 0 is inside
+// the pair, bits 1..5 are lane bits (shuffles), bits 6..LOGT are warp bits
+// (exchange tile sx in shared memory), and bits above index the thread's own
+// registers v[]. Every loop is unrolled at compile time; [q0, q1) only
+// predicates whole axes.
+template <typename R, int LT, int LOGT, int RP>
+__device__ __forceinline__ Pair<R> axis_sum(const Pair<R> (&v)[RP], int j,
+                                           const R* sx, int q0, int q1,
+                                           int tid) {
+  Pair<R> acc = pzero<R>();
+  if (q0 <= 0) padd(acc, pswap<R>(v[j]));
+#pragma unroll
+  for (int q = 1; q <= 5 && q < LT; q++)
+    if (q >= q0 && q < q1) padd(acc, pshfl(v[j], 1 << (q - 1)));
+  const int pp = tid | (j << LOGT);
+#pragma unroll
+  for (int q = 6; q <= LOGT && q < LT; q++)
+    if (q >= q0 && q < q1) padd(acc, pld(sx + 4 * (pp ^ (1 << (q - 1)))));
 #pragma unroll
   for (int k = 0; (1 << k) < RP; k++) {
-    const int q = logT + 1 + k;
-    if (q >= q0 && q < q1) add4<R>(acc, v[j ^ (1 << k)]);
+    const int q = LOGT + 1 + k;
+    if (q >= q0 && q < q1) padd(acc, v[j ^ (1 << k)]);
   }
   return acc;
 }
 
-template <typename R, int RP, int NU>
-__global__ void __launch_bounds__(kPassThreads, 2) pass_kernel(PassParams p) {
+template <int LT> struct PassShape {
+  static constexpr int kPairs = 1 << (LT - 1);
+  static constexpr int kThreads = kPairs < kPassThreads ? kPairs : kPassThreads;
+  static constexpr int kRP = kPairs / kThreads;
+  static constexpr int kLogT = kThreads >= 512 ? 9 : kThreads >= 256 ? 8 : kThreads >= 128 ? 7 : kThreads >= 64 ? 6 : 5;
+};
+
+// Two CTAs per SM in FP32 (64 registers); FP64 pairs need twice the
+// registers, so FP64 allows one CTA per SM at up to 128 registers.
+template <typename R, int LT>
+__global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 1)
+    pass_kernel(PassParams p) {
+  using S = PassShape<LT>;
+  constexpr int RP = S::kRP, LOGT = S::kLogT, T = S::kThreads;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[32];
   const PassWalk& W = p.walk[blockIdx.y];
   if (!W.active) return;
-  const int n = p.n, L = p.L, a = p.a;
-  const int T = blockDim.x, tid = threadIdx.x;
-  const int logT = 31 - __clz(T);
-  const int npairs = T * RP;
-  R* sx = reinterpret_cast<R*>(smem_raw);    // exchange tile: 2^L complex
-  R* sp = sx + 4 * (size_t)npairs;          // staged P_r, [j][tid] pairs
-  R* ss = sp + 4 * (size_t)npairs;          // staged psi
-  float2* sd = reinterpret_cast<float2*>(ss + 4 * (size_t)npairs);  // staged D
-  const TileMap tm{n, L, a, p.tiling, (size_t)blockIdx.x};
-  // bin and bout may be the same buffer (in-place update when NU == 0: this
-  // CTA is then the only reader and writer of its tile's positions).
-  const R* bin = reinterpret_cast<const R*>(W.bin);
+  const int n = p.n, a = p.a;
+  const int tid = threadIdx.x;
+  R* sx = reinterpret_cast<R*>(smem_raw);  // exchange tile: 2^LT complex
+  R* sp = sx + 4 * S::kPairs;              // staged P_r, [j][tid] pairs
+  R* ss = sp + 4 * S::kPairs;              // staged psi
+  float2* sd = reinterpret_cast<float2*>(ss + 4 * S::kPairs);  // staged D
+  // Global amplitude index of register pair j: g0 + j * gstride (32-bit: n <= 30).
+  const unsigned tile = blockIdx.x;
+  const unsigned pos0 = 2u * tid;
+  unsigned g0, gstride;
+  if (p.tiling == 1) {
+    g0 = (tile << LT) | pos0;
+    gstride = 1u << (LOGT + 1);
+  } else {
+    const unsigned amask = (1u << a) - 1u;
+    g0 = (pos0 & amask) | (tile << a) | ((pos0 >> a) << (n - LT + a));
+    gstride = 1u << (LOGT + 1 + n - LT);
+  }
+  const R* bin = reinterpret_cast<const R*>(W.bin);  // may alias bout (nu == 0)
   R* bout = reinterpret_cast<R*>(W.bout);
   R* __restrict__ part = reinterpret_cast<R*>(W.part);
   const R* __restrict__ psi = reinterpret_cast<const R*>(W.psi);
@@ -300,70 +389,73 @@ __global__ void __launch_bounds__(kPassThreads, 2) pass_kernel(PassParams p) {
   const int r = W.r, K = W.K;
   const bool first = r == K - 1;
   const bool uni = W.psi_uniform;
+  const int nu = n - (2 * LT - a) > 0 ? n - (2 * LT - a) : 0;
   // Finish axes (tile bits): T1 -> [a, min(L, n-L+a)), T2 -> [max(2L-n, a), L);
-  // axes [L, L+NU) are in neither tiling and come from global memory.
-  const int fb0 = p.tiling == 1 ? a : max(2 * L - n, a);
-  const int fb1 = p.tiling == 1 ? min(L, n - L + a) : L;
+  // axes [L, L+nu) are in neither tiling and come from global memory.
+  const int fb0 = p.tiling == 1 ? a : max(2 * LT - n, a);
+  const int fb1 = p.tiling == 1 ? min(LT, n - LT + a) : LT;
 
   // Stage P_r, psi and D for this thread's own pairs.
 #pragma unroll
   for (int j = 0; j < RP; j++) {
-    const size_t gi = tm.index(2 * (tid | (j << logT)));
+    const unsigned gi = g0 + j * gstride;
     const int o = j * T + tid;
-    if (!first) cp_async_pair<R>(sp + 4 * o, part + 2 * gi);
-    if (!uni) cp_async_pair<R>(ss + 4 * o, psi + 2 * gi);
+    if (!first) cp_async_pair<R>(sp + 4 * o, part + 2 * (size_t)gi);
+    if (!uni) cp_async_pair<R>(ss + 4 * o, psi + 2 * (size_t)gi);
     cp_async8(sd + o, hp + gi);
   }
-  V4<R> va[RP];  // b_{r+1}
+  Pair<R> va[RP];  // b_{r+1}
 #pragma unroll
   for (int j = 0; j < RP; j++)
-    va[j] = first ? V4<R>{0, 0, 0, 0}
-                  : ld4<R>(bin + 2 * tm.index(2 * (tid | (j << logT))));
+    va[j] = first ? pzero<R>() : pld(bin + 2 * (size_t)(g0 + j * gstride));
   const double kap = W.kappa ? *W.kappa : 1.0;
   const R scale = (R)W.scale;
   const R gamma = (R)W.gamma;
   const R a_mid = (R)2 / scale, a_fin = (R)2 / ((R)2 * scale);
-  const R psi0 = (R)(float)(1.0 / sqrt((double)((size_t)1 << n)));
-  V4<R> vb[RP];  // b_r
+  const R psi0 = (R)W.psi0;
+  Pair<R> vb[RP];  // b_r
   if (first) {
     const R cr = (R)((double)W.coef[r] * kap);
     cp_async_wait_all();
 #pragma unroll
     for (int j = 0; j < RP; j++) {
       const V4<R> pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * (j * T + tid));
-      vb[j] = cpsi4<R>(cr, r & 1, pv);
+      vb[j] = from4(cpsi4<R>(cr, r & 1, pv));
     }
   } else {
     const R ag = (r == 0 ? a_fin : a_mid) * gamma;
 #pragma unroll
-    for (int j = 0; j < RP; j++) st4<R>(sx + 4 * (tid | (j << logT)), va[j]);
+    for (int j = 0; j < RP; j++) pst(sx + 4 * (tid | (j << LOGT)), va[j]);
     __syncthreads();
     cp_async_wait_all();
 #pragma unroll
     for (int j = 0; j < RP; j++) {
-      V4<R> acc = axis_sum<R, RP>(va, j, sx, logT, fb0, fb1, tid);
-      if (NU > 0) {
-        const size_t gi = tm.index(2 * (tid | (j << logT)));
-        V4<R> gv[NU > 0 ? NU : 1];
+      Pair<R> accp = axis_sum<R, LT, LOGT, RP>(va, j, sx, fb0, fb1, tid);
+      const unsigned gi = g0 + j * gstride;
+      for (int u0 = 0; u0 < nu; u0 += 4) {
+        Pair<R> gv[4];
 #pragma unroll
-        for (int u = 0; u < NU; u++) gv[u] = ld4<R>(bin + 2 * (gi ^ ((size_t)1 << (L + u))));
+        for (int u = 0; u < 4; u++)
+          if (u0 + u < nu) gv[u] = pld(bin + 2 * (size_t)(gi ^ (1u << (LT + u0 + u))));
 #pragma unroll
-        for (int u = 0; u < NU; u++) add4<R>(acc, gv[u]);
+        for (int u = 0; u < 4; u++)
+          if (u0 + u < nu) padd(accp, gv[u]);
       }
+      const V4<R> acc = to4(accp);
       const V4<R> pr = ld4<R>(sp + 4 * (j * T + tid));
-      vb[j] = V4<R>{fma(-ag, acc.x, pr.x), fma(-ag, acc.y, pr.y),
-                    fma(-ag, acc.z, pr.z), fma(-ag, acc.w, pr.w)};
+      vb[j] = from4(V4<R>{fma(-ag, acc.x, pr.x), fma(-ag, acc.y, pr.y),
+                          fma(-ag, acc.z, pr.z), fma(-ag, acc.w, pr.w)});
     }
   }
 #pragma unroll
-  for (int j = 0; j < RP; j++)
-    st4<R>(bout + 2 * tm.index(2 * (tid | (j << logT))), vb[j]);
+  for (int j = 0; j < RP; j++) pst(bout + 2 * (size_t)(g0 + j * gstride), vb[j]);
   if (r == 0) {
     double nrm = 0.0;
 #pragma unroll
-    for (int j = 0; j < RP; j++)
-      nrm += (double)vb[j].x * vb[j].x + (double)vb[j].y * vb[j].y +
-             (double)vb[j].z * vb[j].z + (double)vb[j].w * vb[j].w;
+    for (int j = 0; j < RP; j++) {
+      const V4<R> v = to4(vb[j]);
+      nrm += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
+    }
     const double sum = block_sum<R>(nrm, s_red);
     if (tid == 0) W.norm_part[blockIdx.x] = sum;
     return;
@@ -371,24 +463,26 @@ __global__ void __launch_bounds__(kPassThreads, 2) pass_kernel(PassParams p) {
   // Start P_{r-1} = c psi + a (D b_r - gamma X_Z b_r) - b_{r+1} over all tile axes.
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < RP; j++) st4<R>(sx + 4 * (tid | (j << logT)), vb[j]);
+  for (int j = 0; j < RP; j++) pst(sx + 4 * (tid | (j << LOGT)), vb[j]);
   __syncthreads();
   const int rm = r - 1;
   const R am = rm == 0 ? a_fin : a_mid;
   const R cm = (R)((double)W.coef[rm] * kap);
 #pragma unroll
   for (int j = 0; j < RP; j++) {
-    const V4<R> acc = axis_sum<R, RP>(vb, j, sx, logT, 0, L, tid);
+    const V4<R> acc = to4(axis_sum<R, LT, LOGT, RP>(vb, j, sx, 0, LT, tid));
     const int o = j * T + tid;
     const V4<R> pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * o);
     const float2 d = sd[o];
+    const V4<R> b = to4(vb[j]);
+    const V4<R> b1 = to4(va[j]);
     V4<R> out = cpsi4<R>(cm, rm & 1, pv);
     const R d0 = (R)d.x, d1 = (R)d.y;
-    out.x = fma(am, fma(d0, vb[j].x, -gamma * acc.x), out.x - va[j].x);
-    out.y = fma(am, fma(d0, vb[j].y, -gamma * acc.y), out.y - va[j].y);
-    out.z = fma(am, fma(d1, vb[j].z, -gamma * acc.z), out.z - va[j].z);
-    out.w = fma(am, fma(d1, vb[j].w, -gamma * acc.w), out.w - va[j].w);
-    st4<R>(part + 2 * tm.index(2 * (tid | (j << logT))), out);
+    out.x = fma(am, fma(d0, b.x, -gamma * acc.x), out.x - b1.x);
+    out.y = fma(am, fma(d0, b.y, -gamma * acc.y), out.y - b1.y);
+    out.z = fma(am, fma(d1, b.z, -gamma * acc.z), out.z - b1.z);
+    out.w = fma(am, fma(d1, b.w, -gamma * acc.w), out.w - b1.w);
+    st4<R>(part + 2 * (size_t)(g0 + j * gstride), out);
   }
 }
 
@@ -451,23 +545,32 @@ cudaError_t launch_resident(int precision, const ResidentWalk* walks,
   ResidentArgs a{walks, stages, coef, hp, diag, p_sample};
   const int T = (1 << max_n) < 512 ? (1 << max_n) : 512;
   const int threads = T < 32 ? 32 : T;
+  // The shared-memory opt-in is set once per size (never while a stream is
+  // being captured after the first eager launch).
+  static size_t configured[2] = {0, 0};
   if (precision == 0) {
     const size_t sm = resident_smem<float>(max_n);
-    cudaError_t e = cudaFuncSetAttribute(resident_kernel<float>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
+    if (sm > configured[0]) {
+      cudaError_t e = cudaFuncSetAttribute(resident_kernel<float>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+      configured[0] = sm;
+    }
     resident_kernel<float><<<count, threads, sm, stream>>>(a);
   } else {
     const size_t sm = resident_smem<double>(max_n);
-    cudaError_t e = cudaFuncSetAttribute(resident_kernel<double>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
+    if (sm > configured[1]) {
+      cudaError_t e = cudaFuncSetAttribute(resident_kernel<double>,
+                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      if (e != cudaSuccess) return e;
+      configured[1] = sm;
+    }
     resident_kernel<double><<<count, threads, sm, stream>>>(a);
   }
   return cudaGetLastError();
 }
 
-PassGeomHost pass_geom(int precision, int n) {
+PassGeomHost pass_geom(int precision, int n, int lmax) {
   // Tile: 2^L amplitudes of b_{r+1} and 2^L of b_r in shared memory
   // (64 KB at L = 12 in FP32, 3 CTAs per SM). Rows of 2^a = 16 amplitudes
   // (128 bytes in FP32) keep T2 loads coalesced. L is chosen so the two
@@ -478,7 +581,10 @@ PassGeomHost pass_geom(int precision, int n) {
     env = e ? atoi(e) : -1;
   }
   int Lmax = precision == 0 ? 12 : 11;
-  if (env >= 2 && env <= 13) Lmax = env;
+  if (env >= 6 && env <= 13) Lmax = env;
+  if (lmax >= 6 && lmax <= 13) Lmax = lmax;
+  const int cap = precision == 0 ? 12 : 11;  // compiled tile sizes
+  if (Lmax > cap) Lmax = cap;
   // Threads own pairs along the top tile axes, lanes cover tile axes 1..5,
   // so a tile has at least 6 axes (n >= 6 on the grid path).
   PassGeomHost g;
@@ -494,50 +600,34 @@ PassGeomHost pass_geom(int precision, int n) {
 }
 
 namespace {
-template <typename R, int RP, int NU>
-cudaError_t launch_pass_k(const PassParams& p, dim3 grid, int threads,
-                          size_t smem, cudaStream_t stream) {
+template <typename R, int LT>
+cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
+  using S = PassShape<LT>;
   static size_t configured = 0;
+  const size_t smem = (size_t)S::kPairs * (3 * 4 * sizeof(R) + sizeof(float2));
   if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, RP, NU>,
+    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, LT>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     configured = smem;
   }
-  pass_kernel<R, RP, NU><<<grid, threads, smem, stream>>>(p);
+  dim3 grid((unsigned)((size_t)1 << (p.n - LT)), p.count);
+  pass_kernel<R, LT><<<grid, S::kThreads, smem, stream>>>(p);
   return cudaGetLastError();
-}
-
-template <typename R, int RP>
-cudaError_t launch_pass_rp(const PassParams& p, dim3 grid, int threads,
-                           size_t smem, int nu, cudaStream_t stream) {
-  switch (nu) {
-#define MQW_NU(k) \
-  case k:         \
-    return launch_pass_k<R, RP, k>(p, grid, threads, smem, stream);
-    MQW_NU(0) MQW_NU(1) MQW_NU(2) MQW_NU(3) MQW_NU(4) MQW_NU(5) MQW_NU(6)
-    MQW_NU(7) MQW_NU(8) MQW_NU(9) MQW_NU(10) MQW_NU(11) MQW_NU(12) MQW_NU(13)
-    MQW_NU(14)
-#undef MQW_NU
-    default:
-      return cudaErrorInvalidValue;
-  }
 }
 
 template <typename R>
 cudaError_t launch_pass_t(const PassParams& p, cudaStream_t stream) {
-  const int nu = p.n - (2 * p.L - p.a) > 0 ? p.n - (2 * p.L - p.a) : 0;
-  dim3 grid((unsigned)((size_t)1 << (p.n - p.L)), p.count);
-  const int npairs = 1 << (p.L - 1);
-  // 512 threads when the tile has enough pairs; never fewer than one warp
-  // (L >= 6 guarantees >= 32 pairs).
-  const int threads = npairs < kPassThreads ? npairs : kPassThreads;
-  const int rp = npairs / threads;
-  const size_t smem = (size_t)npairs * (3 * 4 * sizeof(R) + sizeof(float2));
-  switch (rp) {
-    case 1: return launch_pass_rp<R, 1>(p, grid, threads, smem, nu, stream);
-    case 2: return launch_pass_rp<R, 2>(p, grid, threads, smem, nu, stream);
-    case 4: return launch_pass_rp<R, 4>(p, grid, threads, smem, nu, stream);
+  switch (p.L) {
+    case 6: return launch_pass_lt<R, 6>(p, stream);
+    case 7: return launch_pass_lt<R, 7>(p, stream);
+    case 8: return launch_pass_lt<R, 8>(p, stream);
+    case 9: return launch_pass_lt<R, 9>(p, stream);
+    case 10: return launch_pass_lt<R, 10>(p, stream);
+    case 11: return launch_pass_lt<R, 11>(p, stream);
+    case 12:
+      if constexpr (sizeof(R) == 4) return launch_pass_lt<R, 12>(p, stream);
+      return cudaErrorInvalidValue;  // FP64 tiles stop at 2^11
     default: return cudaErrorInvalidValue;
   }
 }
@@ -545,7 +635,7 @@ cudaError_t launch_pass_t(const PassParams& p, cudaStream_t stream) {
 
 cudaError_t launch_pass(int precision, const PassParams& p,
                         cudaStream_t stream) {
-  if (p.n < 6 || p.L < 6 || p.L > p.n || p.a < 1 || p.a >= p.L ||
+  if (p.n < 6 || p.n > kMaxN || p.L < 6 || p.L > p.n || p.a != 4 ||
       (p.tiling != 1 && p.tiling != 2) || p.count < 1 || p.count > kMaxGroup)
     return cudaErrorInvalidValue;
   return precision == 0 ? launch_pass_t<float>(p, stream)
