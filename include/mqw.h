@@ -163,6 +163,31 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
                         const float* coeffs, const float* hp, float gamma,
                         float scale, const void* psi, void* out);
 
+/* ---- propagation without allocation ---------------------------------- */
+
+/* Largest n accepted by mqw_clenshaw_noalloc (its fixed working space). */
+#define MQW_NOALLOC_MAX_N 16
+
+/* No counterpart in the reference (which has no library API). The same
+ * propagation as mqw_clenshaw, for callers that cannot allocate device
+ * memory — for example code running during CUDA graph capture, code that must
+ * not synchronise the device, or hosts whose own allocator owns all device
+ * memory. All pointers are DEVICE pointers owned by the caller: d_coeffs[K],
+ * d_hp[2^n], d_psi[2^n] and d_out[2^n] complex (float for MQW_FP32, double
+ * for MQW_FP64); d_out must not alias d_psi and receives the result. Work is
+ * queued on `stream` (a cudaStream_t, NULL = the legacy default stream) of the
+ * current device; the call returns without waiting for it.
+ * Working space is a fixed device array of about 1 MiB inside the library
+ * (held by every GPU that loads it until exit); n > MQW_NOALLOC_MAX_N returns
+ * MQW_ERR_UNSUPPORTED and 6 <= n is required. The first call on each device
+ * looks up that array's device address and must precede any stream capture.
+ * Calls that overlap on the GPU share the array and race: order them on one
+ * stream. Calls no cudaMalloc, cudaFree or other allocating routine. */
+mqw_status mqw_clenshaw_noalloc(int precision, int n, int K,
+                                const float* d_coeffs, const float* d_hp,
+                                float gamma, float scale, const void* d_psi,
+                                void* d_out, void* stream);
+
 /* ---- the whole path -------------------------------------------------- */
 
 /* For `count` instances of n spins and m stages in the reference's layout

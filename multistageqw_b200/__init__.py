@@ -114,6 +114,7 @@ def _bind(L):
         "mqw_plan_stats": (i, [_vp, _P(RunStats)]),
         "mqw_plan_destroy": (None, [_vp]),
         "mqw_multiqw": (i, [_vp, i, i, ctypes.c_char_p, ll, ll, ctypes.c_char_p, i]),
+        "mqw_clenshaw_noalloc": (i, [i, i, i, _vp, _vp, f, f, _vp, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -299,6 +300,24 @@ class Context:
                 out_dir: str | None = None, print_: bool = True):
         _check(self.h, lib().mqw_multiqw(self.h, n, m, filename.encode(), start, problems,
                                          out_dir.encode() if out_dir else None, int(print_)))
+
+
+NOALLOC_MAX_N = 16
+
+
+def clenshaw_noalloc(precision: int, n: int, K: int, d_coeffs: int, d_hp: int, gamma: float,
+                     scale: float, d_psi: int, d_out: int, stream: int | None = None) -> None:
+    """Propagation without any device allocation (device pointers in and out).
+
+    For callers that cannot allocate device memory (e.g. while a CUDA graph is
+    captured, or when their own allocator owns the device): the library keeps
+    its working space in a fixed ~1 MiB device array, so n is limited to
+    NOALLOC_MAX_N, and calls that overlap on the GPU race on that array.
+    The first call on a device must come before any stream capture."""
+    st = lib().mqw_clenshaw_noalloc(precision, n, K, _vp(d_coeffs), _vp(d_hp), gamma, scale,
+                                    _vp(d_psi), _vp(d_out), _vp(stream) if stream else None)
+    if st != 0:
+        raise MQWError(st, f"clenshaw_noalloc(n={n})")
 
 
 class Plan:
