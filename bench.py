@@ -9,11 +9,16 @@ of a 2^20-amplitude state, reduced to the mean ground-state probability.
 A step is one batch of `--batch` seeded synthetic Sherrington–Kirkpatrick
 instances (J_ij, h_i ~ N(0,1), the reference's file layout; the reference's
 datasets are not used). `value` times the device path with the batch already
-resident in device memory (mqw_plan_execute); `e2e` times the public C ABI
-call from host buffers (mqw_run_problems: upload, schedule, run, read-back).
-L2 is flushed (256 MB write) between timed steps.
+resident in device memory (mqw_plan_execute; after the first execution this
+replays a CUDA graph of the whole device pipeline); `e2e` times the public C
+ABI from host buffers (plan create: upload and host schedule; execute;
+read-back). L2 is flushed (256 MB write) between timed steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Other workloads (--workload): mixed (a seeded subset of the mixed n=12..20,
+m=2..5 batch), n28 (one n=28, m=3 instance, a few samples per step) and
+precision (the n=24 near-degenerate FP32/FP64/CPU study; one JSON report).
 
 With --impl reference the line times the reference's own CPU hot loop
 (Clenshaw_step, compiled from the reference source into oracle/_ref) driven
@@ -30,6 +35,8 @@ import subprocess
 import sys
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -37,6 +44,11 @@ METRIC = ("instances/s at n=20,m=4 (|ΔP|≤1e-5 vs FP64); "
           "mean P_gs learned vs heuristic")
 BYTES_PER_TERM_AMP = {"fp32": 36, "fp64": 72}  # algorithmic, see DESIGN.md
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+# DRAM bytes per term·amp of pass_kernel from one ncu capture of this
+# workload (profiles/pass_kernel_sk_n20_m4.md); absent until captured.
+DRAM_BYTES_PER_TERM_AMP = {}
+# Host memory the CPU legs may use at once (all worker processes together).
+CPU_MEM_BUDGET = 24 << 30
 
 
 def parse():
@@ -45,6 +57,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mqw", choices=["mqw", "reference"])
+    ap.add_argument("--workload", default="sk_n20_m4",
+                    choices=["sk_n20_m4", "mixed", "n28", "precision"])
     ap.add_argument("--n", type=int, default=20)
     ap.add_argument("--m", type=int, default=4)
     ap.add_argument("--batch", type=int, default=2, help="instances per step per GPU")
@@ -54,7 +68,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=20)
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 |dP| check")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--cpu-samples", type=int, default=2, help="samples per CPU worker")
+    ap.add_argument("--cpu-samples", type=int, default=1, help="samples per CPU worker")
+    ap.add_argument("--cpu-walks", type=int, default=4, help="precision: CPU-checked instances")
     return ap.parse_args()
 
 
@@ -121,7 +136,7 @@ def gpu_selector(torch, dev):
         return vis.split(",")[dev] if vis else str(dev)
 
 
-# ---- CPU baseline (reference hot loop, one process per core) ------------------
+# ---- CPU baselines (reference hot loop, one process per core) ------------------
 
 def _cpu_worker(args):
     n, m, seed, samples = args
@@ -134,13 +149,14 @@ def _cpu_worker(args):
     return time.perf_counter() - t0, use_ref
 
 
-def cpu_baseline(n, m, seed, samples_per_worker, workers=None):
+def cpu_baseline(n, m, seed, samples_per_worker):
+    """Whole samples of the reference pipeline (n <= 22): every process runs
+    `samples_per_worker` samples of its own instance."""
     cores = len(os.sched_getaffinity(0))
-    workers = workers or cores
-    ctx = mp.get_context("spawn")
+    workers = max(1, min(cores, CPU_MEM_BUDGET // (44 << n)))
     jobs = [(n, m, seed + i, samples_per_worker) for i in range(workers)]
     t0 = time.perf_counter()
-    with ctx.Pool(workers) as pool:
+    with mp.get_context("spawn").Pool(workers) as pool:
         res = pool.map(_cpu_worker, jobs)
     wall = time.perf_counter() - t0
     busy = max(r[0] for r in res)
@@ -156,39 +172,177 @@ def cpu_baseline(n, m, seed, samples_per_worker, workers=None):
     }
 
 
-# ---- main ---------------------------------------------------------------------
+def _cpu_term_worker(args):
+    """Seconds per Clenshaw term (both real halves) of the reference's own
+    Clenshaw_step at size n, on seeded vectors."""
+    n, reps, seed = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    N = 1 << n
+    rng = np.random.default_rng(seed)
+    b1 = rng.standard_normal(N).astype(np.float32)
+    b2 = rng.standard_normal(N).astype(np.float32)
+    hp = rng.standard_normal(N).astype(np.float32)
+    psi = rng.standard_normal(N).astype(np.float32)
+    use_ref = O.ref_lib() is not None
+    step = O.ref_clenshaw_step if use_ref else O.clenshaw_step_f32
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        step(b1, b2, hp, psi, n, 40.0, 1.5, 0.1)  # real half
+        step(b1, b2, hp, psi, n, 40.0, 1.5, 0.1)  # imaginary half
+    return (time.perf_counter() - t0) / reps, use_ref
+
+
+def cpu_baseline_per_term(n, terms_per_instance, reps=2):
+    """Bounded CPU baseline for large n (a whole n = 28 sample is ~20 min per
+    core): every worker times `reps` terms of the reference's step;
+    instances/s = workers / (terms per instance x s/term). Workers are capped
+    so that their vectors fit CPU_MEM_BUDGET."""
+    cores = len(os.sched_getaffinity(0))
+    workers = max(1, min(cores, CPU_MEM_BUDGET // (16 << n)))
+    with mp.get_context("spawn").Pool(workers) as pool:
+        res = pool.map(_cpu_term_worker, [(n, reps, 11 + i) for i in range(workers)])
+    sec = max(r[0] for r in res)
+    kind = "reference" if all(r[1] for r in res) else "port"
+    return {"value": workers / (terms_per_instance * sec), "unit": "instances/s",
+            "cores": workers, "kind": kind,
+            "sample": (f"{workers} processes x {reps} Clenshaw terms (both halves) at n={n} of the "
+                       + ("reference's Clenshaw_step, MultiQW.cpp:88-173, AVX-512 build" if kind == "reference"
+                          else "oracle restatement")
+                       + f"; {sec:.3f} s/term scaled by {terms_per_instance} terms per instance"),
+            "seconds_per_term": sec}
+
+
+def _cpu_one_sample(args):
+    n, m, raw = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    use_ref = O.ref_lib() is not None
+    t0 = time.perf_counter()
+    r = O.run_problems(n, m, raw, 1, 1, "f32", use_ref_step=use_ref)
+    return float(r["p"][0]), time.perf_counter() - t0, use_ref
+
+
+def cpu_precision_check(raws, n, m):
+    """Sample 0 of each instance on the CPU with the reference's own FP32
+    Clenshaw_step (partial build) against the GPU's FP32 and FP64 paths."""
+    import multistageqw_b200 as M
+    ctx = M.Context(0)
+    g32 = ctx.run_problems(n, m, raws, samples=1, precision="fp32")["p"]
+    g64 = ctx.run_problems(n, m, raws, samples=1, precision="fp64")["p"]
+    ctx.close()
+    workers = max(1, min(len(raws), CPU_MEM_BUDGET // (44 << n)))
+    with mp.get_context("spawn").Pool(workers) as pool:
+        res = pool.map(_cpu_one_sample, [(n, m, r) for r in raws])
+    cpu = np.array([r[0] for r in res])
+    return {"instances": len(raws), "samples": 1, "processes": workers,
+            "kind": "reference" if all(r[2] for r in res) else "port",
+            "p_cpu": cpu.tolist(), "p_gpu_fp32": g32.tolist(), "p_gpu_fp64": g64.tolist(),
+            "max_abs_dP_cpu_vs_gpu_fp64": float(np.abs(cpu - g64).max()),
+            "max_abs_dP_gpu_fp32_vs_fp64": float(np.abs(g32 - g64).max()),
+            "cpu_seconds_per_sample": float(np.mean([r[1] for r in res]))}
+
+
+# ---- replicas (one process per GPU, no exchange) ------------------------------
+
+def replica_seed(seed: int, rank: int) -> int:
+    """Each rank runs its own seeded batch (independent problems, like the
+    reference's run.sh process split)."""
+    return seed + 7919 * rank
+
+
+def max_over_ranks(x: float, world: int, dist=None, device=None) -> float:
+    """Max of a per-rank time over all ranks (the job ends when the slowest
+    rank ends); identity on one rank."""
+    if world <= 1:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---- workloads -----------------------------------------------------------------
+
+def make_batch(M, a, rank):
+    """(n list, m list, raw concatenated, description) for the workload."""
+    seed = replica_seed(a.seed, rank)
+    if a.workload == "mixed":
+        # The mixed batch: n uniform in {12, 14, 16, 18, 20}, m in {2..5}.
+        rng = np.random.default_rng(seed)
+        ns = rng.choice([12, 14, 16, 18, 20], a.batch).tolist()
+        ms = rng.integers(2, 6, a.batch).tolist()
+        raws = [M.sk_instances(n, 1, int(rng.integers(1 << 31)))[0] for n in ns]
+        desc = {"workload": "sk_mixed_n12-20_m2-5", "n": "12..20 (even)", "m": "2..5",
+                "note": f"{a.batch}-instance seeded subset of the 4096-instance mixed batch"}
+        return ns, ms, np.concatenate(raws), desc
+    if a.workload == "n28":
+        raw = M.sk_instances(28, 1, 7)
+        desc = {"workload": "sk_n28_m3_seed7", "n": 28, "m": 3,
+                "note": f"one instance, {a.samples} of its 100 samples per step; "
+                        "instances/s counts samples/100"}
+        return [28], [3], raw.ravel(), desc
+    raw = M.sk_instances(a.n, a.batch, seed)
+    desc = {"workload": f"sk_n{a.n}_m{a.m}", "n": a.n, "m": a.m}
+    return [a.n] * a.batch, [a.m] * a.batch, raw.ravel(), desc
+
+
+def instance_units(a, count: int) -> float:
+    """Instances completed per step (n28 runs a fraction of one instance)."""
+    return count * (a.samples / 100.0 if a.workload == "n28" else 1.0)
+
+
+def reference_arm(a):
+    n, m = (28, 3) if a.workload == "n28" else (a.n, a.m)
+    times, base = [], None
+    for step in range(a.warmup + a.steps):
+        if n > 22:
+            # ~1 s per term per core at n = 28: time terms, scale by the
+            # instance's term count (3 stages x ~190 terms x 100 samples).
+            b = cpu_baseline_per_term(n, 57000, reps=1)
+        else:
+            b = cpu_baseline(n, m, a.seed + 1000 * step, 1)
+        if step >= a.warmup:
+            times.append(b)
+        base = b
+    val = sum(t["value"] for t in times) / len(times)
+    return {
+        "metric": METRIC, "value": val, "unit": "instances/s", "n_gpus": a.gpus,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 / val,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic seeded SK instances (J,h ~ N(0,1))",
+        "impl": "reference",
+        "config": {"workload": f"sk_n{n}_m{m}", "n": n, "m": m, "samples": 100},
+        "cpu_baseline": {k: base[k] for k in ("kind", "cores", "sample")} | {"value": val, "unit": "instances/s"},
+        "e2e": {"value": val, "unit": "instances/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
 
 def main():
     a = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.workload == "n28" and a.samples == 100:
+        a.samples = 4
 
     if a.impl == "reference":
-        if rank != 0:
-            return
-        times = []
-        base = None
-        for step in range(a.warmup + a.steps):
-            b = cpu_baseline(a.n, a.m, a.seed + 1000 * step, 1)
-            if step >= a.warmup:
-                times.append(b)
-            base = b
-        val = sum(t["value"] for t in times) / len(times)
-        line = {
-            "metric": METRIC, "value": val, "unit": "instances/s", "n_gpus": a.gpus,
-            "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 / val,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic seeded SK instances (J,h ~ N(0,1))",
-            "impl": "reference",
-            "config": {"workload": f"sk_n{a.n}_m{a.m}", "n": a.n, "m": a.m, "samples": 100},
-            "cpu_baseline": {k: base[k] for k in ("kind", "cores", "sample")} | {"value": val, "unit": "instances/s"},
-            "e2e": {"value": val, "unit": "instances/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        }
-        print(json.dumps(line))
+        if rank == 0:
+            print(json.dumps(reference_arm(a)), flush=True)
         return
 
-    import numpy as np
+    if a.workload == "precision":
+        if rank == 0:
+            from multistageqw_b200 import studies
+            rep = studies.precision_study()
+            raws = rep.pop("raws")
+            rep.pop("p_fp32")
+            rep.pop("p_fp64")
+            if not a.no_cpu:
+                rep["cpu_reference"] = cpu_precision_check(raws[:a.cpu_walks], 24, 4)
+            print(json.dumps(rep), flush=True)
+        return
+
     import torch
     import torch.distributed as dist
 
@@ -199,9 +353,15 @@ def main():
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     ctx = M.Context(local)
-    stream = torch.cuda.current_stream(dev)
-    raw = M.sk_instances(a.n, a.batch, a.seed + 7919 * rank)
-    plan = M.Plan(ctx, a.n, a.m, raw, samples=a.samples, precision=a.precision, group=a.group)
+    # A dedicated stream: the library launches (or replays its graph) on the
+    # stream it is given, and the CUDA events below are recorded on the same
+    # one. (torch's default stream has handle 0, which the ABI reads as "the
+    # context's own stream".)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    ns, ms, raw, desc = make_batch(M, a, rank)
+    count = len(ns)
+    plan = M.Plan(ctx, ns, ms, raw, samples=a.samples, precision=a.precision, group=a.group)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def barrier():
@@ -213,11 +373,9 @@ def main():
         plan.execute(stream.cuda_stream)
     barrier()
     clocks = ClockSampler(gpu_selector(torch, local))
-    step_ms = []
-    kern_ms = []
+    step_ms, kern_ms = [], []
     term_amps = 0.0
-    launches = 0
-    term_launches = 0
+    launches = term_launches = terms = 0
     for _ in range(a.steps):
         flush.zero_()
         torch.cuda.synchronize(dev)
@@ -233,74 +391,84 @@ def main():
         term_amps += st["term_amps"]
         launches += st["launches"]
         term_launches += st["term_launches"]
+        terms = st["terms"]
     barrier()
     clk = clocks.stop()
-    total_ms = sum(step_ms)
-    if world > 1:
-        t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-    value = world * a.batch * a.steps / (total_ms / 1000.0)
+    total_ms = max_over_ranks(sum(step_ms), world, dist, dev)
+    value = world * instance_units(a, count) * a.steps / (total_ms / 1000.0)
 
     # End to end through the public API from pinned host buffers.
     raw_pinned = torch.from_numpy(np.ascontiguousarray(raw)).pin_memory().numpy()
     e2e_ms = []
     h2d = d2h = 0.0
-    for i in range(max(1, min(a.steps, 2))):
+    for _ in range(max(1, min(a.steps, 2))):
         flush.zero_()
         barrier()
         t0 = time.perf_counter()
-        r = ctx.run_problems(a.n, a.m, raw_pinned, samples=a.samples, precision=a.precision, group=a.group)
+        p2 = M.Plan(ctx, ns, ms, raw_pinned, samples=a.samples, precision=a.precision,
+                    group=a.group, graph=0)
+        p2.execute()
+        r = p2.results()
         torch.cuda.synchronize(dev)
         e2e_ms.append((time.perf_counter() - t0) * 1000.0)
-        h2d, d2h = r["stats"]["h2d_bytes"], r["stats"]["d2h_bytes"]
-    e2e_total = sum(e2e_ms)
-    if world > 1:
-        t = torch.tensor([e2e_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_val = world * a.batch * len(e2e_ms) / (e2e_total / 1000.0)
+        st2 = p2.stats()
+        h2d, d2h = st2["h2d_bytes"], st2["d2h_bytes"]
+        p2.close()
+    e2e_total = max_over_ranks(sum(e2e_ms), world, dist, dev)
+    e2e_val = world * instance_units(a, count) * len(e2e_ms) / (e2e_total / 1000.0)
 
     # |dP| of the timed FP32 results against the FP64 path (first instance).
     check = None
     res = plan.results()
     if not a.no_check and a.precision == "fp32":
-        r64 = ctx.run_problems(a.n, a.m, raw[:1], samples=a.samples, precision="fp64", group=a.group)
-        check = {"max_abs_dP_vs_fp64": float(abs(res["p"][0] - r64["p"][0])),
-                 "instances_checked": 1, "p_fp32": float(res["p"][0]), "p_fp64": float(r64["p"][0])}
+        n0, m0 = ns[0], ms[0]
+        per0 = n0 * (n0 + 1) // 2
+        r64 = M.Plan(ctx, [n0], [m0], raw[:per0], samples=a.samples, precision="fp64", graph=0)
+        r64.execute()
+        p64 = r64.results()["p"][0]
+        r64.close()
+        check = {"max_abs_dP_vs_fp64": float(abs(res["p"][0] - p64)),
+                 "instances_checked": 1, "p_fp32": float(res["p"][0]), "p_fp64": float(p64)}
 
     pk, pk_kind = peaks()
     kms = sum(kern_ms)
     achieved = BYTES_PER_TERM_AMP[a.precision] * term_amps / (kms / 1000.0) / 1e9 if kms > 0 else None
     peak = pk["hbm_gbs"]
+    per_launch_amps = term_amps / max(1, term_launches)
+    dram = DRAM_BYTES_PER_TERM_AMP.get(a.workload)
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-        "frac": achieved / peak if achieved else None, "traffic": None,
+        "frac": achieved / peak if achieved else None,
+        "traffic": dram * per_launch_amps if dram else None,
         "peak_source": f"hbm_gbs of {pk_kind}",
-        "kernel": "term_kernel (grid-path Clenshaw term)",
-        "bytes_per_launch": BYTES_PER_TERM_AMP[a.precision] * term_amps / max(1, term_launches),
+        "kernel": "pass_kernel (grid-path fused Clenshaw pass)",
+        "bytes_per_launch": BYTES_PER_TERM_AMP[a.precision] * per_launch_amps,
         "avg_launch_us": 1000.0 * kms / max(1, term_launches),
     }
 
-    line = None
     if rank == 0:
         cpu = None
-        if world == 1 and not a.no_cpu:
+        if world == 1 and not a.no_cpu and a.workload != "mixed":
             try:
-                cpu = cpu_baseline(a.n, a.m, 4242, a.cpu_samples)
+                if a.workload == "n28":
+                    cpu = cpu_baseline_per_term(28, int(terms * 100.0 / a.samples))
+                else:
+                    cpu = cpu_baseline(a.n, a.m, 4242, a.cpu_samples)
             except Exception as ex:  # the baseline is reported, not required
                 cpu = {"value": None, "error": str(ex)}
+        config = dict(desc)
+        config.update({"instances_per_step": count * world, "samples": a.samples,
+                       "precision": a.precision, "group": a.group or "autotuned",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": "flushed between timed steps (256 MB write)",
+                       "graph": "CUDA graph replay of the whole device pipeline"})
         line = {
             "metric": METRIC, "value": value, "unit": "instances/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if a.precision == "fp32" else "f64",
             "data": "synthetic seeded SK instances (J,h ~ N(0,1)); reference datasets not used",
-            "config": {"workload": f"sk_n{a.n}_m{a.m}", "n": a.n, "m": a.m,
-                       "instances_per_step": a.batch * world, "samples": a.samples,
-                       "precision": a.precision, "group": a.group or "auto",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                       "l2": "flushed between timed steps (256 MB write)"},
+            "config": config,
             "e2e": {"value": e2e_val, "unit": "instances/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches // max(1, a.steps),

@@ -581,8 +581,12 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
   P.executed = true;
   // Capture the whole device pipeline for later executes. The capture runs
   // on the context's private stream (nothing executes while capturing); the
-  // graph is later launched on whatever stream the caller passes.
-  if (P.opt.graph) {
+  // graph is later launched on whatever stream the caller passes. Very large
+  // pipelines (over kMaxGraphLaunches kernels) stay eager: their launch
+  // overhead is already negligible and a graph of millions of nodes costs
+  // host memory and instantiation time.
+  constexpr long long kMaxGraphLaunches = 200000;
+  if (P.opt.graph && P.stats.launches <= kMaxGraphLaunches) {
     CK(cudaStreamSynchronize(stream));
     cudaStream_t cs = ctx->stream;
     P.counting = false;
