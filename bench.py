@@ -334,7 +334,17 @@ def main():
     if a.workload == "precision":
         if rank == 0:
             from multistageqw_b200 import studies
-            rep = studies.precision_study()
+            # The post-selected draws (screened once on the CPU with the
+            # reference's energy arithmetic, tests/golden/make_precision_set.py);
+            # the study re-checks every gap on the GPU.
+            fx = os.path.join(ROOT, "tests", "golden", "precision_n24_m4.json")
+            draws = eloc = None
+            if os.path.exists(fx):
+                with open(fx) as f:
+                    sel = json.load(f)["instances"]
+                draws = [s["draw"] for s in sel]
+                eloc = [s["e_loc"] for s in sel]
+            rep = studies.precision_study(draws=draws, expect_e_loc=eloc)
             raws = rep.pop("raws")
             rep.pop("p_fp32")
             rep.pop("p_fp64")

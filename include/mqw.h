@@ -217,6 +217,36 @@ mqw_status mqw_plan_results(mqw_plan* plan, double* p_out, float* total_t,
 mqw_status mqw_plan_stats(const mqw_plan* plan, mqw_run_stats* stats);
 void mqw_plan_destroy(mqw_plan* plan);
 
+/* ---- learned stage schedule (no counterpart in the reference) ---------- */
+/* Building blocks of the MLP that proposes per-stage (gamma, t) multipliers
+ * (multistageqw_b200/learned.py): BF16 weights, FP32 activations and
+ * accumulation. All pointers are DEVICE pointers; work is queued on `stream`
+ * (a cudaStream_t, NULL = legacy default stream) of the current device.
+ * W_bf16 is row-major [out][in] (bfloat16 bit patterns); X [batch][in];
+ * Y, dY [batch][out]. */
+
+/* Y = X W^T + b, then ReLU when relu != 0. b may be NULL. */
+mqw_status mqw_mlp_linear_forward(int batch, int in, int out,
+                                  const uint16_t* W_bf16, const float* b,
+                                  const float* X, float* Y, int relu,
+                                  void* stream);
+/* With dZ = dY (masked by Y > 0 when relu != 0): dW = dZ^T X [out][in],
+ * db = column sums of dZ [out], and dX = dZ W [batch][in] when dX != NULL.
+ * Y is the layer's forward output (needed only when relu != 0). */
+mqw_status mqw_mlp_linear_backward(int batch, int in, int out,
+                                   const uint16_t* W_bf16, const float* X,
+                                   const float* Y, const float* dY, float* dX,
+                                   float* dW, float* db, int relu,
+                                   void* stream);
+/* One Adam step on FP32 master weights w with moments m, v (step >= 1), then
+ * w_bf16 = bf16(w) when w_bf16 != NULL. */
+mqw_status mqw_mlp_adam(int count, float* w, uint16_t* w_bf16, const float* g,
+                        float* m, float* v, float lr, float beta1, float beta2,
+                        float eps, float weight_decay, int step, void* stream);
+/* w_bf16 = bf16(w), round to nearest even. */
+mqw_status mqw_mlp_to_bf16(int count, const float* w, uint16_t* w_bf16,
+                           void* stream);
+
 /* ---- the reference command -------------------------------------------- */
 
 /* Equivalent of `MultiQW n m filename [start problems]` (MultiQW.cpp:241-458):

@@ -115,6 +115,10 @@ def _bind(L):
         "mqw_plan_destroy": (None, [_vp]),
         "mqw_multiqw": (i, [_vp, i, i, ctypes.c_char_p, ll, ll, ctypes.c_char_p, i]),
         "mqw_clenshaw_noalloc": (i, [i, i, i, _vp, _vp, f, f, _vp, _vp, _vp]),
+        "mqw_mlp_linear_forward": (i, [i, i, i, _vp, _vp, _vp, _vp, i, _vp]),
+        "mqw_mlp_linear_backward": (i, [i, i, i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, i, _vp]),
+        "mqw_mlp_adam": (i, [i, _vp, _vp, _vp, _vp, _vp, f, f, f, f, f, i, _vp]),
+        "mqw_mlp_to_bf16": (i, [i, _vp, _vp, _vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -1,11 +1,13 @@
 """Precision study on near-degenerate instances (n = 24, m = 4).
 
-Seeded SK instances (J, h ~ N(0,1)) are drawn until `count` of them have a
-gap E_(1) - E_(0) < gap_max between their two lowest energies (the energies
-of the reference's arithmetic, the ones that define E_loc). On those:
+The instances are seeded SK draws (J, h ~ N(0,1)) whose two lowest energies
+E_(1) - E_(0) differ by less than `gap_max` (energies in the reference's
+arithmetic, the ones that define E_loc). The kept draws either come as a
+list (a precomputed screen; every gap is re-checked here on the GPU) or are
+screened here on the GPU. On them:
 
 * the whole path in FP32 and in FP64 on the GPU (`samples` samples each):
-  per-instance |dP|;
+  per-instance |dP| and the ground-state index of both paths;
 * for `state_walks` walks, the state after every stage in FP32 and FP64
   (stage by stage through mqw_clenshaw): relative L2 error per stage;
 * the Chebyshev degree per stage (mean over samples);
@@ -19,23 +21,41 @@ import time
 
 import numpy as np
 
-from . import Context, cheb_coeffs_host, schedule, sk_instances
+from . import Context, cheb_coeffs_host, schedule
+
+DRAW_SEED = 24 * 1_000_003  # draw d is default_rng(DRAW_SEED + d)
 
 
-def screen(ctx: Context, n: int, count: int, seed: int, gap_max: float, max_draws: int):
+def draw_raw(n: int, d: int) -> np.ndarray:
+    """Draw d of the study: n(n+1)/2 standard normals (J pairs, then h)."""
+    return np.random.default_rng(DRAW_SEED + d).standard_normal(n * (n + 1) // 2)
+
+
+def two_lowest_gap(ctx: Context, n: int, raw):
+    """(E_(1) - E_(0), E_loc, E_abs) from the GPU diagonal."""
+    _, E, info = ctx.build_diag(n, raw, energies=True)
+    i = int(E.argmin())
+    e0 = E[i]
+    E[i] = np.inf
+    return float(E.min() - e0), int(info.e_loc), float(info.e_abs)
+
+
+def screen(ctx: Context, n: int, count: int, gap_max: float, max_draws: int, draws=None):
     kept = []
-    draws = 0
     t0 = time.time()
-    while len(kept) < count and draws < max_draws:
-        raw = sk_instances(n, 1, seed * 1_000_003 + draws)[0]
-        _, E, info = ctx.build_diag(n, raw, energies=True)
-        two = np.partition(E, 1)[:2]
-        gap = float(two[1] - two[0])
+    cand = range(max_draws) if draws is None else draws
+    seen = 0
+    for d in cand:
+        if len(kept) >= count:
+            break
+        raw = draw_raw(n, int(d))
+        gap, e_loc, e_abs = two_lowest_gap(ctx, n, raw)
+        seen += 1
         if gap < gap_max:
-            kept.append({"raw": raw, "gap": gap, "e_loc": int(info.e_loc), "e_abs": float(info.e_abs),
-                         "draw": draws})
-        draws += 1
-    return kept, draws, time.time() - t0
+            kept.append({"raw": raw, "gap": gap, "e_loc": e_loc, "e_abs": e_abs, "draw": int(d)})
+        elif draws is not None:
+            raise ValueError(f"draw {d}: gap {gap} is not below {gap_max}")
+    return kept, seen, time.time() - t0
 
 
 def stage_states(ctx: Context, n: int, m: int, raw, sample: int, precision: str):
@@ -57,11 +77,13 @@ def stage_states(ctx: Context, n: int, m: int, raw, sample: int, precision: str)
     return out, degrees, int(info.e_loc)
 
 
-def precision_study(n: int = 24, m: int = 4, count: int = 32, seed: int = 24,
-                    gap_max: float = 1e-2, samples: int = 4, max_draws: int = 4000,
-                    state_walks: int = 2) -> dict:
+def precision_study(n: int = 24, m: int = 4, count: int = 32, gap_max: float = 1e-2,
+                    samples: int = 4, max_draws: int = 20000, state_walks: int = 2,
+                    draws=None, expect_e_loc=None) -> dict:
+    """Runs the study; `draws` (optional) lists the kept draw indices of a
+    precomputed screen and `expect_e_loc` their ground-state indices."""
     ctx = Context(0)
-    kept, draws, t_screen = screen(ctx, n, count, seed, gap_max, max_draws)
+    kept, seen, t_screen = screen(ctx, n, count, gap_max, max_draws, draws)
     raws = np.stack([k["raw"] for k in kept])
     t0 = time.time()
     r32 = ctx.run_problems(n, m, raws, samples=samples, precision="fp32")
@@ -89,9 +111,11 @@ def precision_study(n: int = 24, m: int = 4, count: int = 32, seed: int = 24,
             "dP_sample0": float(abs(abs(s32[-1][eloc]) ** 2 - abs(s64[-1][eloc]) ** 2)),
         })
     ctx.close()
-    return {
+    e_loc = [k["e_loc"] for k in kept]
+    rep = {
         "metric": "precision study: FP32 vs FP64 on near-degenerate SK instances",
-        "n": n, "m": m, "instances": len(kept), "draws_screened": draws, "gap_max": gap_max,
+        "n": n, "m": m, "instances": len(kept), "draws_screened": seen, "gap_max": gap_max,
+        "screen": "precomputed list, gaps re-checked on the GPU" if draws is not None else "GPU screen",
         "screen_seconds": t_screen, "samples": samples,
         "gaps": [k["gap"] for k in kept],
         "gaps_below_1e-4": int(sum(k["gap"] < 1e-4 for k in kept)),
@@ -104,3 +128,6 @@ def precision_study(n: int = 24, m: int = 4, count: int = 32, seed: int = 24,
         "raws": raws,  # for the caller's CPU comparison; dropped before printing
         "p_fp32": r32["p"], "p_fp64": r64["p"],
     }
+    if expect_e_loc is not None:
+        rep["e_loc_equals_screen"] = bool(list(expect_e_loc)[:len(e_loc)] == e_loc)
+    return rep
