@@ -166,3 +166,16 @@ def test_cli_drop_in(ctx, orc, mqw, tmp_path):
     # a short file is an error, not a silent repeat
     r = subprocess.run([mqw.CLI_PATH, "10", "2", str(f), "10", "5"], cwd=tmp_path, capture_output=True)
     assert r.returncode == 1
+
+
+def test_near_degenerate_n24_ground_state_index(ctx):
+    """The 32 post-selected n = 24 instances (two lowest energies < 1e-2
+    apart, two of them < 1e-4): the GPU diagonal gives the same ground-state
+    index and the same gap as the oracle's reference-arithmetic screen."""
+    from multistageqw_b200 import studies
+    sel = load_golden("precision_n24_m4.json")
+    for s in sel["instances"]:
+        raw = studies.draw_raw(24, s["draw"])
+        gap, e_loc, _ = studies.two_lowest_gap(ctx, 24, raw)
+        assert e_loc == s["e_loc"], s
+        assert gap == s["gap"], s

@@ -189,3 +189,22 @@ def test_oracle_golden_small(orc):
         r = orc.run_problems(c["n"], c["m"], raw, c["count"], c["samples"], "f64")
         assert np.allclose(r["p"], c["p_f64"], rtol=0, atol=1e-14), c
         assert np.abs(np.array(c["p_f32"]) - np.array(c["p_f64"])).max() < 1e-5, c
+
+
+def test_precision_screen_fixture(orc):
+    """Spot-checks the committed n = 24 near-degenerate screen: the first
+    kept draw and the two draws with gaps below 1e-4 give the recorded gap
+    and ground-state index again, and the draws follow the study's seed
+    rule."""
+    from multistageqw_b200 import studies
+    from tests.golden import make_precision_set as MP
+    sel = load_golden("precision_n24_m4.json")
+    inst = sel["instances"]
+    assert len(inst) == 32 and sel["gap_max"] == 1e-2
+    assert all(i["gap"] < 1e-2 for i in inst)
+    tiny = [i for i in inst if i["gap"] < 1e-4]
+    assert len(tiny) >= 1
+    for s in [inst[0]] + tiny:
+        assert np.array_equal(MP.draw_raw(s["draw"]), studies.draw_raw(24, s["draw"]))
+        d, gap, e_loc, e0 = MP.gap_of(s["draw"])
+        assert (gap, e_loc, e0) == (s["gap"], s["e_loc"], s["e0"])
