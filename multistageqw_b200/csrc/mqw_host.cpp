@@ -217,6 +217,7 @@ mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
     PassParams pp{};
     pp.n = n;
     pp.L = geo.L;
+    pp.C = geo.C;
     pp.a = geo.a;
     pp.tiling = (r & 1) ? 2 : 1;
     pp.count = G;
@@ -340,6 +341,7 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
       PassParams pp{};
       pp.n = n;
       pp.L = geo.L;
+      pp.C = geo.C;
       pp.a = geo.a;
       pp.tiling = (r & 1) ? 2 : 1;
       pp.count = G;
@@ -991,6 +993,7 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
     PassParams pp{};
     pp.n = n;
     pp.L = geo.L;
+    pp.C = geo.C;
     pp.a = geo.a;
     pp.tiling = (r & 1) ? 2 : 1;
     pp.count = 1;

@@ -107,7 +107,10 @@ cudaError_t launch_resident(int precision, const ResidentWalk* walks,
 //   T2: 2^(L-a) rows of 2^a consecutive amplitudes, one row per value of the
 //       top L-a axes (axes [0, a) and [n-L+a, n)).
 // Axes in neither tiling ([L, n-L+a), when n > 2L-a) are read from global
-// memory during the finish.
+// memory during the finish. With C > 0 a tiling's tile of 2^(L+C)
+// amplitudes is spread over a cluster of 2^C CTAs (each holds 2^L, the CTA's
+// cluster rank supplies the top C tile bits) and L above stands for L + C;
+// partners along the rank bits are read from the other CTAs' shared memory.
 struct PassWalk {
   const void* bin;     // b_{r+1}; may equal bout only when no axis is read
                        // from global memory (nu == 0)
@@ -128,12 +131,14 @@ struct PassWalk {
 };
 struct PassParams {
   int n, L, a;
+  int C;               // cluster log: a tile spans 2^C CTAs (0 = one CTA)
   int tiling;          // 1 or 2
   int count;
   PassWalk walk[kMaxGroup];
 };
 struct PassGeomHost {
-  int L, a, nu;        // tile log, row log, axes read from global memory
+  int L, a, nu;        // CTA tile log, row log, axes read from global memory
+  int C;               // cluster log (tile of 2^(L+C) amplitudes over 2^C CTAs)
 };
 // Geometry for n; lmax > 0 caps the tile (log2 amplitudes), else the
 // precision's default cap (or MQW_PASS_TILE_LOG) applies.

@@ -92,6 +92,7 @@ extern "C" mqw_status mqw_clenshaw_noalloc(int precision, int n, int K,
     PassParams pp{};
     pp.n = n;
     pp.L = geo.L;
+    pp.C = geo.C;
     pp.a = geo.a;
     pp.tiling = (r & 1) ? 2 : 1;
     pp.count = 1;

@@ -318,6 +318,38 @@ __device__ __forceinline__ Pair<double> from4(const V4<double>& v) {
   return {make_double2(v.x, v.y), make_double2(v.z, v.w)};
 }
 
+// Distributed shared memory (thread-block clusters): the shared-window
+// address of the same variable in the CTA of cluster rank `rank`, loads from
+// it, and the cluster-wide barrier (release/acquire: orders this CTA's shared
+// memory writes before the other CTAs' reads after the barrier).
+__device__ __forceinline__ unsigned cluster_addr(const void* smem, unsigned rank) {
+  const unsigned local = (unsigned)__cvta_generic_to_shared(smem);
+  unsigned r;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+  return r;
+}
+__device__ __forceinline__ Pair<float> pld_cluster(const float*, unsigned addr) {
+  unsigned long long a, b;
+  asm volatile("ld.shared::cluster.v2.u64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "r"(addr) : "memory");
+  return {a, b};
+}
+__device__ __forceinline__ Pair<double> pld_cluster(const double*, unsigned addr) {
+  double x, y, z, w;
+  asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(x), "=d"(y) : "r"(addr) : "memory");
+  asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(z), "=d"(w) : "r"(addr + 16) : "memory");
+  return {make_double2(x, y), make_double2(z, w)};
+}
+__device__ __forceinline__ void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n"
+               "barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
+}
+// The block barrier, or the cluster barrier when the tile spans a cluster.
+template <int CL>
+__device__ __forceinline__ void tile_barrier() {
+  if constexpr (CL > 0) cluster_barrier();
+  else __syncthreads();
+}
+
 // Sum over tile axes q in [q0, q1) of the partners of register pair j. The
 // pair index of register j is pp = tid | (j << LOGT): tile bit 0 is inside
 // the pair, bits 1..5 are lane bits (shuffles), bits 6..LOGT are warp bits
@@ -354,11 +386,17 @@ template <int LT> struct PassShape {
 
 // Two CTAs per SM in FP32 (64 registers); FP64 pairs need twice the
 // registers, so FP64 allows one CTA per SM at up to 128 registers.
-template <typename R, int LT>
+// CL > 0: the tiling's tile spans a cluster of 2^CL CTAs (tile bits
+// [LT, LT + CL) are the CTA's cluster rank); partners along those bits are
+// read from the other CTAs' exchange tiles, and every barrier that guards the
+// exchange tile is a cluster barrier. All CTAs of a cluster belong to the
+// same walk and term, so they take the same path through every barrier.
+template <typename R, int LT, int CL>
 __global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 1)
     pass_kernel(PassParams p) {
   using S = PassShape<LT>;
   constexpr int RP = S::kRP, LOGT = S::kLogT, T = S::kThreads;
+  constexpr int LL = LT + CL;  // tile bits of the tiling
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[32];
   const PassWalk& W = p.walk[blockIdx.y];
@@ -370,17 +408,23 @@ __global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 
   R* ss = sp + 4 * S::kPairs;              // staged psi
   float2* sd = reinterpret_cast<float2*>(ss + 4 * S::kPairs);  // staged D
   // Global amplitude index of register pair j: g0 + j * gstride (32-bit: n <= 30).
-  const unsigned tile = blockIdx.x;
-  const unsigned pos0 = 2u * tid;
+  // For a 1-D cluster the cluster rank is blockIdx.x mod 2^CL.
+  const unsigned rank = CL > 0 ? (blockIdx.x & ((1u << CL) - 1u)) : 0u;
+  const unsigned tile = blockIdx.x >> CL;
+  const unsigned pos0 = (rank << LT) | (2u * tid);  // tile position of pair 0
   unsigned g0, gstride;
   if (p.tiling == 1) {
-    g0 = (tile << LT) | pos0;
+    g0 = (tile << LL) | pos0;
     gstride = 1u << (LOGT + 1);
   } else {
     const unsigned amask = (1u << a) - 1u;
-    g0 = (pos0 & amask) | (tile << a) | ((pos0 >> a) << (n - LT + a));
-    gstride = 1u << (LOGT + 1 + n - LT);
+    g0 = (pos0 & amask) | (tile << a) | ((pos0 >> a) << (n - LL + a));
+    gstride = 1u << (LOGT + 1 + n - LL);
   }
+  // Exchange tiles of the cluster's other CTAs, one per rank bit.
+  unsigned peer_sx[CL > 0 ? CL : 1];
+#pragma unroll
+  for (int k = 0; k < CL; k++) peer_sx[k] = cluster_addr(sx, rank ^ (1u << k));
   const R* bin = reinterpret_cast<const R*>(W.bin);  // may alias bout (nu == 0)
   R* bout = reinterpret_cast<R*>(W.bout);
   R* __restrict__ part = reinterpret_cast<R*>(W.part);
@@ -389,11 +433,19 @@ __global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 
   const int r = W.r, K = W.K;
   const bool first = r == K - 1;
   const bool uni = W.psi_uniform;
-  const int nu = n - (2 * LT - a) > 0 ? n - (2 * LT - a) : 0;
-  // Finish axes (tile bits): T1 -> [a, min(L, n-L+a)), T2 -> [max(2L-n, a), L);
-  // axes [L, L+nu) are in neither tiling and come from global memory.
-  const int fb0 = p.tiling == 1 ? a : max(2 * LT - n, a);
-  const int fb1 = p.tiling == 1 ? min(LT, n - LT + a) : LT;
+  const int nu = n - (2 * LL - a) > 0 ? n - (2 * LL - a) : 0;
+  // Finish axes (tile bits): T1 -> [a, min(L, n-L+a)), T2 -> [max(2L-n, a), L)
+  // with L = LL; axes [LL, LL+nu) are in neither tiling and come from global
+  // memory.
+  const int fb0 = p.tiling == 1 ? a : max(2 * LL - n, a);
+  const int fb1 = p.tiling == 1 ? min(LL, n - LL + a) : LL;
+  // Partners along the rank bits [LT, LL) that lie in [q0, q1), summed into acc.
+  auto cluster_sum = [&](Pair<R>& acc, int j, int q0, int q1) {
+    const unsigned off = (unsigned)(4 * sizeof(R)) * (unsigned)(tid | (j << LOGT));
+#pragma unroll
+    for (int k = 0; k < CL; k++)
+      if (LT + k >= q0 && LT + k < q1) padd(acc, pld_cluster((const R*)nullptr, peer_sx[k] + off));
+  };
 
   // Stage P_r, psi and D for this thread's own pairs.
 #pragma unroll
@@ -426,17 +478,18 @@ __global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 
     const R ag = (r == 0 ? a_fin : a_mid) * gamma;
 #pragma unroll
     for (int j = 0; j < RP; j++) pst(sx + 4 * (tid | (j << LOGT)), va[j]);
-    __syncthreads();
+    tile_barrier<CL>();
     cp_async_wait_all();
 #pragma unroll
     for (int j = 0; j < RP; j++) {
       Pair<R> accp = axis_sum<R, LT, LOGT, RP>(va, j, sx, fb0, fb1, tid);
+      cluster_sum(accp, j, fb0, fb1);
       const unsigned gi = g0 + j * gstride;
       for (int u0 = 0; u0 < nu; u0 += 4) {
         Pair<R> gv[4];
 #pragma unroll
         for (int u = 0; u < 4; u++)
-          if (u0 + u < nu) gv[u] = pld(bin + 2 * (size_t)(gi ^ (1u << (LT + u0 + u))));
+          if (u0 + u < nu) gv[u] = pld(bin + 2 * (size_t)(gi ^ (1u << (LL + u0 + u))));
 #pragma unroll
         for (int u = 0; u < 4; u++)
           if (u0 + u < nu) padd(accp, gv[u]);
@@ -458,19 +511,22 @@ __global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 
     }
     const double sum = block_sum<R>(nrm, s_red);
     if (tid == 0) W.norm_part[blockIdx.x] = sum;
+    if constexpr (CL > 0) cluster_barrier();  // peers may still read sx
     return;
   }
   // Start P_{r-1} = c psi + a (D b_r - gamma X_Z b_r) - b_{r+1} over all tile axes.
-  __syncthreads();
+  tile_barrier<CL>();  // every reader of sx (this CTA and its peers) is done
 #pragma unroll
   for (int j = 0; j < RP; j++) pst(sx + 4 * (tid | (j << LOGT)), vb[j]);
-  __syncthreads();
+  tile_barrier<CL>();
   const int rm = r - 1;
   const R am = rm == 0 ? a_fin : a_mid;
   const R cm = (R)((double)W.coef[rm] * kap);
 #pragma unroll
   for (int j = 0; j < RP; j++) {
-    const V4<R> acc = to4(axis_sum<R, LT, LOGT, RP>(vb, j, sx, 0, LT, tid));
+    Pair<R> accp = axis_sum<R, LT, LOGT, RP>(vb, j, sx, 0, LT, tid);
+    cluster_sum(accp, j, 0, LL);
+    const V4<R> acc = to4(accp);
     const int o = j * T + tid;
     const V4<R> pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * o);
     const float2 d = sd[o];
@@ -484,6 +540,8 @@ __global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 
     out.w = fma(am, fma(d1, b.w, -gamma * acc.w), out.w - b1.w);
     st4<R>(part + 2 * (size_t)(g0 + j * gstride), out);
   }
+  // A CTA's shared memory must outlive its peers' reads of it.
+  if constexpr (CL > 0) cluster_barrier();
 }
 
 template <typename R>
@@ -570,11 +628,60 @@ cudaError_t launch_resident(int precision, const ResidentWalk* walks,
   return cudaGetLastError();
 }
 
+namespace {
+// Largest cluster log (<= 4) whose pass kernel can be resident on this
+// device, for the precision's widest tile; 0 when clusters are unavailable.
+template <typename R, int LT, int CL>
+int cluster_fits() {
+  using S = PassShape<LT>;
+  const size_t smem = (size_t)S::kPairs * (3 * 4 * sizeof(R) + sizeof(float2));
+  if (cudaFuncSetAttribute(pass_kernel<R, LT, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)smem) != cudaSuccess)
+    return 0;
+  if (CL > 3 && cudaFuncSetAttribute(pass_kernel<R, LT, CL>,
+                                     cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+    return 0;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(1u << CL, 1, 1);
+  cfg.blockDim = dim3(S::kThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = 1u << CL;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, pass_kernel<R, LT, CL>, &cfg) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  return clusters > 0;
+}
+
+template <typename R, int LT>
+int max_cluster_log() {
+  static int cached = -1;  // per precision; one device type per process
+  if (cached < 0) {
+    int c = 0;
+    if (cluster_fits<R, LT, 1>()) c = 1;
+    if (c == 1 && cluster_fits<R, LT, 2>()) c = 2;
+    if (c == 2 && cluster_fits<R, LT, 3>()) c = 3;
+    if (c == 3 && cluster_fits<R, LT, 4>()) c = 4;
+    cached = c;
+  }
+  return cached;
+}
+}  // namespace
+
 PassGeomHost pass_geom(int precision, int n, int lmax) {
   // Tile: 2^L amplitudes of b_{r+1} and 2^L of b_r in shared memory
   // (64 KB at L = 12 in FP32, 3 CTAs per SM). Rows of 2^a = 16 amplitudes
   // (128 bytes in FP32) keep T2 loads coalesced. L is chosen so the two
-  // tilings cover every axis when possible (2L - a >= n).
+  // tilings cover every axis when possible (2L - a >= n); above that, at the
+  // widest compiled tile, a tiling's tile spans a cluster of 2^C CTAs
+  // (2(L+C) - a >= n up to C = 4) before any axis is left to global memory.
   static int env = -2;
   if (env == -2) {
     const char* e = getenv("MQW_PASS_TILE_LOG");
@@ -589,44 +696,89 @@ PassGeomHost pass_geom(int precision, int n, int lmax) {
   // so a tile has at least 6 axes (n >= 6 on the grid path).
   PassGeomHost g;
   g.a = 4;
+  g.C = 0;
   int L = (n + g.a + 1) / 2;
   if (L < 6) L = 6;
   if (L > Lmax) L = Lmax;
   if (L > n) L = n;
   g.L = L;
   g.nu = n - (2 * L - g.a);
+  if (g.nu > 0 && L == cap) {
+    const int cmax = precision == 0 ? max_cluster_log<float, 12>() : max_cluster_log<double, 11>();
+    g.C = (g.nu + 1) / 2;
+    if (g.C > cmax) g.C = cmax;
+    g.nu = n - (2 * (L + g.C) - g.a);
+  }
   if (g.nu < 0) g.nu = 0;
   return g;
 }
 
 namespace {
-template <typename R, int LT>
+template <typename R, int LT, int CL>
 cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
   using S = PassShape<LT>;
   static size_t configured = 0;
   const size_t smem = (size_t)S::kPairs * (3 * 4 * sizeof(R) + sizeof(float2));
   if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, LT>,
+    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, LT, CL>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
+    if (CL > 3) {
+      e = cudaFuncSetAttribute(pass_kernel<R, LT, CL>,
+                               cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+      if (e != cudaSuccess) return e;
+    }
     configured = smem;
   }
-  dim3 grid((unsigned)((size_t)1 << (p.n - LT)), p.count);
-  pass_kernel<R, LT><<<grid, S::kThreads, smem, stream>>>(p);
-  return cudaGetLastError();
+  const dim3 grid((unsigned)((size_t)1 << (p.n - LT)), p.count);
+  if constexpr (CL == 0) {
+    pass_kernel<R, LT, 0><<<grid, S::kThreads, smem, stream>>>(p);
+    return cudaGetLastError();
+  } else {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(S::kThreads, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1u << CL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, pass_kernel<R, LT, CL>, p);
+  }
+}
+
+// The widest tile with a cluster of 2^C CTAs.
+template <typename R, int LT>
+cudaError_t launch_pass_cluster(const PassParams& p, cudaStream_t stream) {
+  switch (p.C) {
+    case 0: return launch_pass_lt<R, LT, 0>(p, stream);
+    case 1: return launch_pass_lt<R, LT, 1>(p, stream);
+    case 2: return launch_pass_lt<R, LT, 2>(p, stream);
+    case 3: return launch_pass_lt<R, LT, 3>(p, stream);
+    case 4: return launch_pass_lt<R, LT, 4>(p, stream);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 template <typename R>
 cudaError_t launch_pass_t(const PassParams& p, cudaStream_t stream) {
+  constexpr int cap = sizeof(R) == 4 ? 12 : 11;
+  if (p.C != 0 && p.L != cap) return cudaErrorInvalidValue;
   switch (p.L) {
-    case 6: return launch_pass_lt<R, 6>(p, stream);
-    case 7: return launch_pass_lt<R, 7>(p, stream);
-    case 8: return launch_pass_lt<R, 8>(p, stream);
-    case 9: return launch_pass_lt<R, 9>(p, stream);
-    case 10: return launch_pass_lt<R, 10>(p, stream);
-    case 11: return launch_pass_lt<R, 11>(p, stream);
+    case 6: return launch_pass_lt<R, 6, 0>(p, stream);
+    case 7: return launch_pass_lt<R, 7, 0>(p, stream);
+    case 8: return launch_pass_lt<R, 8, 0>(p, stream);
+    case 9: return launch_pass_lt<R, 9, 0>(p, stream);
+    case 10: return launch_pass_lt<R, 10, 0>(p, stream);
+    case 11:
+      if constexpr (sizeof(R) == 8) return launch_pass_cluster<R, 11>(p, stream);
+      return launch_pass_lt<R, 11, 0>(p, stream);
     case 12:
-      if constexpr (sizeof(R) == 4) return launch_pass_lt<R, 12>(p, stream);
+      if constexpr (sizeof(R) == 4) return launch_pass_cluster<R, 12>(p, stream);
       return cudaErrorInvalidValue;  // FP64 tiles stop at 2^11
     default: return cudaErrorInvalidValue;
   }
@@ -635,8 +787,9 @@ cudaError_t launch_pass_t(const PassParams& p, cudaStream_t stream) {
 
 cudaError_t launch_pass(int precision, const PassParams& p,
                         cudaStream_t stream) {
-  if (p.n < 6 || p.n > kMaxN || p.L < 6 || p.L > p.n || p.a != 4 ||
-      (p.tiling != 1 && p.tiling != 2) || p.count < 1 || p.count > kMaxGroup)
+  if (p.n < 6 || p.n > kMaxN || p.L < 6 || p.L > p.n || p.a != 4 || p.C < 0 || p.C > 4 ||
+      p.n - p.L < p.C || (p.tiling != 1 && p.tiling != 2) || p.count < 1 ||
+      p.count > kMaxGroup)
     return cudaErrorInvalidValue;
   return precision == 0 ? launch_pass_t<float>(p, stream)
                         : launch_pass_t<double>(p, stream);

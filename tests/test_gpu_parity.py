@@ -58,8 +58,10 @@ def _planar_to_complex(x):
     return x[:N] + 1j * x[N:]
 
 
-@pytest.mark.parametrize("n", [6, 9, 11, 12, 15, 17])
+@pytest.mark.parametrize("n", [6, 9, 11, 12, 15, 17, 19, 21])
 def test_clenshaw_single_propagation(ctx, orc, n):
+    # n = 19: FP64 tiles span 2-CTA clusters; n = 21: FP32 2-CTA and FP64
+    # 4-CTA clusters.
     N = 1 << n
     raw = orc.sk_instances(n, 1, 40 + n)[0]
     _, hp, info = orc.energies_ref(n, raw)
@@ -179,3 +181,20 @@ def test_near_degenerate_n24_ground_state_index(ctx):
         gap, e_loc, _ = studies.two_lowest_gap(ctx, 24, raw)
         assert e_loc == s["e_loc"], s
         assert gap == s["gap"], s
+
+
+@pytest.mark.parametrize("n", [23, 25, 27])
+def test_cluster_tiles_match_global_partner_path(ctx, orc, n):
+    """Above n = 20 (FP32) the tiles span clusters of 4, 8 and 16 CTAs at
+    n = 23, 25, 27. Capping the tile at 2^11 (tile_log = 11) instead runs the
+    single-CTA path with the remaining axes read from global memory: both
+    must agree with each other and with FP64 to the FP32 target."""
+    raw = orc.sk_instances(n, 1, 500 + n)
+    kw = dict(samples=1, graph=0, group=1)
+    r_cl = ctx.run_problems(n, 2, raw, precision="fp32", **kw)
+    r_gl = ctx.run_problems(n, 2, raw, precision="fp32", tile_log=11, **kw)
+    r_64 = ctx.run_problems(n, 2, raw, precision="fp64", **kw)
+    assert r_cl["stats"]["terms"] == r_gl["stats"]["terms"] == r_64["stats"]["terms"]
+    assert abs(r_cl["p"][0] - r_gl["p"][0]) <= 1e-6
+    assert abs(r_cl["p"][0] - r_64["p"][0]) <= 1e-5
+    assert 0.0 < r_cl["p"][0] < 1.0
