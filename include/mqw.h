@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define MQW_ABI_VERSION 1
+#define MQW_ABI_VERSION 2
 #define MQW_SAMPLES 100  /* time samples per stage, MultiQW.cpp:257 */
 #define MQW_MAX_N 30     /* 2^30 amplitudes; the reference overflows at n >= 31 (MultiQW.cpp:246) */
 #define MQW_MAX_M 64     /* stages per walk */
@@ -69,6 +69,8 @@ typedef struct mqw_options {
   int graph;       /* 1 (default): a plan's second and later executions
                       replay a CUDA graph of its whole device pipeline;
                       0: launch kernels one by one every time */
+  int lanes;       /* grid-path walk groups in flight at once, each on its
+                      own stream (1..4), 0 = autotuned */
 } mqw_options;
 
 typedef struct mqw_diag_info {

@@ -55,6 +55,7 @@ class Options(ctypes.Structure):
         ("stage_scale", ctypes.POINTER(ctypes.c_float)),
         ("tile_log", ctypes.c_int),
         ("graph", ctypes.c_int),
+        ("lanes", ctypes.c_int),
     ]
 
 
@@ -155,7 +156,7 @@ def _ptr(a, ct):
 
 
 def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_max_n=0,
-          stage_scale=None, tile_log=0, graph=1):
+          stage_scale=None, tile_log=0, graph=1, lanes=0):
     o = Options()
     lib().mqw_default_options(ctypes.byref(o))
     o.precision = {"fp32": FP32, "fp64": FP64, FP32: FP32, FP64: FP64}[precision]
@@ -165,6 +166,7 @@ def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_ma
     o.resident_max_n = int(resident_max_n)
     o.tile_log = int(tile_log)
     o.graph = int(graph)
+    o.lanes = int(lanes)
     keep = None
     if stage_scale is not None:
         keep = np.ascontiguousarray(stage_scale, dtype=np.float32)

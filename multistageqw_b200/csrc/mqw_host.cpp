@@ -63,6 +63,13 @@ struct DevMem {
 // diagonal's chunk partials. Plans of one context are executed one at a time
 // (the ABI's threading rule), so sharing is safe and repeated calls do not
 // pay for allocation.
+// Grid-path shape for one (precision, n): tile cap, walks per launch, and
+// concurrent launch lanes.
+struct GridShape {
+  int lmax = 0, group = 1, lanes = 1;
+};
+constexpr int kMaxLanes = 4;
+
 struct mqw_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -72,8 +79,49 @@ struct mqw_ctx {
   // Bumped whenever a shared scratch buffer is reallocated: a plan's captured
   // graph holds the old addresses and is re-captured when this changes.
   unsigned long long scratch_gen = 1;
-  // Autotuned grid-path geometry per (precision, n): tile cap and group size.
-  std::map<std::pair<int, int>, std::pair<int, int>> tuned;
+  // Autotuned grid-path geometry per (precision, n).
+  std::map<std::pair<int, int>, GridShape> tuned;
+  // Concurrent walk-group lanes of the grid path: lane 0 runs on the
+  // launching stream, lanes 1.. on these private streams, forked from and
+  // joined back into the launching stream with events (which a CUDA graph
+  // capture follows, so a captured pipeline keeps its lanes concurrent).
+  cudaStream_t lane_stream[kMaxLanes] = {};
+  cudaEvent_t fork_ev = nullptr;
+  cudaEvent_t join_ev[kMaxLanes] = {};
+  cudaError_t ensure_lanes(int lanes) {
+    if (!fork_ev) {
+      cudaError_t e = cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming);
+      if (e != cudaSuccess) return e;
+    }
+    for (int k = 1; k < lanes && k < kMaxLanes; k++) {
+      if (!lane_stream[k]) {
+        cudaError_t e = cudaStreamCreateWithFlags(&lane_stream[k], cudaStreamNonBlocking);
+        if (e != cudaSuccess) return e;
+      }
+      if (!join_ev[k]) {
+        cudaError_t e = cudaEventCreateWithFlags(&join_ev[k], cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+      }
+    }
+    return cudaSuccess;
+  }
+  // Makes lanes 1..lanes-1 wait for the work queued so far on `stream`.
+  cudaError_t fork(cudaStream_t stream, int lanes) {
+    if (lanes <= 1) return cudaSuccess;
+    cudaError_t e = cudaEventRecord(fork_ev, stream);
+    for (int k = 1; k < lanes && e == cudaSuccess; k++)
+      e = cudaStreamWaitEvent(lane_stream[k], fork_ev, 0);
+    return e;
+  }
+  // Makes `stream` wait for everything queued on lanes 1..lanes-1.
+  cudaError_t join(cudaStream_t stream, int lanes) {
+    cudaError_t e = cudaSuccess;
+    for (int k = 1; k < lanes && e == cudaSuccess; k++) {
+      e = cudaEventRecord(join_ev[k], lane_stream[k]);
+      if (e == cudaSuccess) e = cudaStreamWaitEvent(stream, join_ev[k], 0);
+    }
+    return e;
+  }
   cudaError_t grow(DevMem& m, size_t bytes) {
     if (bytes <= m.bytes && m.p) return cudaSuccess;
     scratch_gen++;
@@ -116,6 +164,7 @@ void default_opts(mqw_options* o) {
   o->stage_scale = nullptr;
   o->tile_log = 0;
   o->graph = 1;
+  o->lanes = 0;
 }
 
 }  // namespace
@@ -143,8 +192,8 @@ struct mqw_plan {
   size_t diag_scratch_bytes = 0;
   // Coefficient pool and launch tables (plan-owned: a captured graph reads them).
   DevMem d_coef, d_coef_off, d_stages, d_walks;
-  // Grid-path geometry chosen for each n of the plan: (tile cap, group).
-  std::map<int, std::pair<int, int>> grid_geo;
+  // Grid-path shape chosen for each n of the plan.
+  std::map<int, GridShape> grid_geo;
   // CUDA graph of the whole device pipeline, replayed by later executes.
   cudaGraphExec_t gexec = nullptr;
   unsigned long long graph_gen = 0;
@@ -198,22 +247,25 @@ int default_group(int precision, const PassGeomHost& geo, int n) {
 }
 
 // Times one configuration of the grid path: `reps` full passes (both
-// tilings) over G zero-filled walks. Returns microseconds per walk-pass.
+// tilings) over G zero-filled walks on each of `lanes` concurrent streams.
+// Returns microseconds per walk-pass.
 mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
-                            int G, double* us_per_walk) {
+                            int G, int lanes, double* us_per_walk) {
   const PassGeomHost geo = pass_geom(precision, n, lmax);
   const size_t N = (size_t)1 << n;
   const size_t amp = precision == 0 ? 8 : 16;
   const int slots = walk_slots(geo);
-  CK(ctx->grow(ctx->state, (size_t)G * slots * N * amp + N * sizeof(float)));
-  CK(ctx->grow(ctx->norm_part, (size_t)G * (N >> geo.L) * sizeof(double)));
+  const int W = G * lanes;
+  CK(ctx->ensure_lanes(lanes));
+  CK(ctx->grow(ctx->state, (size_t)W * slots * N * amp + N * sizeof(float)));
+  CK(ctx->grow(ctx->norm_part, (size_t)W * (N >> geo.L) * sizeof(double)));
   CK(ctx->tune_coef.ensure(64 * sizeof(float)));
   cudaStream_t st = ctx->stream;
-  CK(cudaMemsetAsync(ctx->state.p, 0, (size_t)G * slots * N * amp + N * sizeof(float), st));
+  CK(cudaMemsetAsync(ctx->state.p, 0, (size_t)W * slots * N * amp + N * sizeof(float), st));
   CK(cudaMemsetAsync(ctx->tune_coef.p, 0, 64 * sizeof(float), st));
   char* base = ctx->state.as<char>();
-  const float* hp = reinterpret_cast<const float*>(base + (size_t)G * slots * N * amp);
-  auto issue = [&](int r) -> cudaError_t {
+  const float* hp = reinterpret_cast<const float*>(base + (size_t)W * slots * N * amp);
+  auto issue = [&](int r, int lane) -> cudaError_t {
     PassParams pp{};
     pp.n = n;
     pp.L = geo.L;
@@ -222,51 +274,58 @@ mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
     pp.tiling = (r & 1) ? 2 : 1;
     pp.count = G;
     for (int g = 0; g < G; g++) {
-      PassWalk& W = pp.walk[g];
-      char* w = base + (size_t)g * slots * N * amp;
-      W.active = 1;
-      W.bin = w + N * amp;
-      W.bout = w + (slots == 4 ? 3 : 1) * N * amp;
-      W.part = w + 2 * N * amp;
-      W.psi = w;
-      W.hp = hp;
-      W.coef = ctx->tune_coef.as<float>();
-      W.kappa = nullptr;
-      W.norm_part = ctx->norm_part.as<double>() + (size_t)g * (N >> geo.L);
-      W.gamma = 1.0f;
-      W.scale = 64.0f;
-      W.r = r;
-      W.K = 40;
-      W.psi_uniform = 0;
-      W.psi0 = 0.0f;
+      PassWalk& Wk = pp.walk[g];
+      const int wi = lane * G + g;
+      char* w = base + (size_t)wi * slots * N * amp;
+      Wk.active = 1;
+      Wk.bin = w + N * amp;
+      Wk.bout = w + (slots == 4 ? 3 : 1) * N * amp;
+      Wk.part = w + 2 * N * amp;
+      Wk.psi = w;
+      Wk.hp = hp;
+      Wk.coef = ctx->tune_coef.as<float>();
+      Wk.kappa = nullptr;
+      Wk.norm_part = ctx->norm_part.as<double>() + (size_t)wi * (N >> geo.L);
+      Wk.gamma = 1.0f;
+      Wk.scale = 64.0f;
+      Wk.r = r;
+      Wk.K = 40;
+      Wk.psi_uniform = 0;
+      Wk.psi0 = 0.0f;
     }
-    return launch_pass(precision, pp, st);
+    return launch_pass(precision, pp, lane == 0 ? st : ctx->lane_stream[lane]);
   };
-  for (int r = 4; r >= 1; r--) CK(issue(r));
+  CK(ctx->fork(st, lanes));
+  for (int r = 4; r >= 1; r--)
+    for (int l = 0; l < lanes; l++) CK(issue(r, l));
+  CK(ctx->join(st, lanes));
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
   const int reps = 12;
   CK(cudaEventRecord(e0, st));
-  for (int r = reps; r >= 1; r--) CK(issue(r));
+  CK(ctx->fork(st, lanes));
+  for (int r = reps; r >= 1; r--)
+    for (int l = 0; l < lanes; l++) CK(issue(r, l));
+  CK(ctx->join(st, lanes));
   CK(cudaEventRecord(e1, st));
   CK(cudaEventSynchronize(e1));
   float ms = 0.0f;
   CK(cudaEventElapsedTime(&ms, e0, e1));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  *us_per_walk = 1000.0 * ms / (reps * G);
+  *us_per_walk = 1000.0 * ms / (reps * W);
   return MQW_OK;
 }
 
-// Autotuner: picks the grid-path tile cap and group size for (precision, n)
-// by timing the candidates once per context; the result is cached.
-mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, int* lmax, int* G) {
+// Autotuner: picks the grid-path tile cap, group size and lane count for
+// (precision, n) by timing the candidates once per context; the result is
+// cached. Fixed choices in `want` (non-zero fields) are kept.
+mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridShape* out) {
   const auto key = std::make_pair(precision, n);
   auto it = ctx->tuned.find(key);
-  if (it != ctx->tuned.end()) {
-    *lmax = it->second.first;
-    *G = it->second.second;
+  if (it != ctx->tuned.end() && !want.lmax && !want.group && !want.lanes) {
+    *out = it->second;
     return MQW_OK;
   }
   const int def_l = precision == 0 ? 12 : 11;
@@ -274,25 +333,35 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, int* lmax, int* G) {
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)8 << 30;
   const size_t budget = std::min(free_b / 4, (size_t)16 << 30);
   double best = 1e300;
-  int best_l = def_l, best_g = 1;
+  GridShape b;
+  b.lmax = want.lmax ? want.lmax : def_l;
+  b.group = want.group ? want.group : 1;
+  b.lanes = want.lanes ? want.lanes : 1;
   for (int l = def_l; l >= def_l - 1; l--) {
+    if (want.lmax && l != want.lmax) continue;
     const PassGeomHost geo = pass_geom(precision, n, l);
     const int g0 = default_group(precision, geo, n);
     for (int g : {1, 2, 3, 4, g0}) {
-      if (g > kMaxGroup || (size_t)g * walk_bytes(precision, geo, n) > budget) continue;
-      double us = 0.0;
-      mqw_status s = time_grid_config(ctx, precision, n, l, g, &us);
-      if (s != MQW_OK) return s;
-      if (us < best * 0.98) {  // prefer the earlier (larger tile, smaller group) on ties
-        best = us;
-        best_l = l;
-        best_g = g;
+      if (want.group && g != want.group) continue;
+      for (int lanes : {1, 2}) {
+        if (want.lanes && lanes != want.lanes) continue;
+        if (g > kMaxGroup || (size_t)g * lanes * walk_bytes(precision, geo, n) > budget) continue;
+        double us = 0.0;
+        mqw_status s = time_grid_config(ctx, precision, n, l, g, lanes, &us);
+        if (s != MQW_OK) return s;
+        // Prefer the earlier candidate (larger tile, fewer walks in flight)
+        // unless a later one is clearly faster.
+        if (us < best * 0.98) {
+          best = us;
+          b.lmax = l;
+          b.group = g;
+          b.lanes = lanes;
+        }
       }
     }
   }
-  ctx->tuned[key] = std::make_pair(best_l, best_g);
-  *lmax = best_l;
-  *G = best_g;
+  if (!want.lmax && !want.group && !want.lanes) ctx->tuned[key] = b;
+  *out = b;
   return MQW_OK;
 }
 
@@ -302,8 +371,11 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, int* lmax, int* G) {
 // even r and y for odd r), otherwise it is updated in place, which keeps a
 // walk at 3 vectors so that two walks of n = 20 stay resident in L2. Pass r
 // uses tiling 1 for even r and tiling 2 for odd r.
+// `lane` selects the lane's own slice of the shared scratch (state, norm
+// partials, kappa), sized for groups of `gmax` walks.
 mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
-                          const PassGeomHost& geo, cudaStream_t stream) {
+                          const PassGeomHost& geo, int lane, int gmax,
+                          cudaStream_t stream) {
   mqw_ctx* ctx = P.ctx;
   const int n = P.walks[widx[0]].n;
   const size_t N = (size_t)1 << n;
@@ -311,7 +383,7 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
   const int G = (int)widx.size();
   const size_t amp = P.precision == 0 ? 8 : 16;
   const int slots = walk_slots(geo);
-  char* base = P.ctx->state.as<char>();
+  char* base = P.ctx->state.as<char>() + (size_t)lane * gmax * slots * N * amp;
   auto buf = [&](int g, int k) -> void* {
     return base + ((size_t)g * slots + k) * N * amp;
   };
@@ -322,8 +394,8 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
     pi[g] = 0;
     xs[g] = 1;
   }
-  double* norm_part = P.ctx->norm_part.as<double>();
-  double* kappa = P.ctx->kappa.as<double>();
+  double* norm_part = P.ctx->norm_part.as<double>() + (size_t)lane * gmax * tiles;
+  double* kappa = P.ctx->kappa.as<double>() + (size_t)lane * kMaxGroup;
   double* p_sample = P.d_p_sample.as<double>();
   const float* coef = P.d_coef.as<float>();
   const float* hp = P.d_hp.as<float>();
@@ -454,15 +526,23 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
   }
   for (auto& kv : grid_by_n) {
     const int n = kv.first;
-    const std::pair<int, int> lg = P.grid_geo.at(n);
-    const PassGeomHost geo = pass_geom(P.precision, n, lg.first);
-    const int G = lg.second;
+    const GridShape gs = P.grid_geo.at(n);
+    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax);
+    const int G = gs.group;
     const std::vector<int>& ws = kv.second;
-    for (size_t i = 0; i < ws.size(); i += G) {
-      std::vector<int> grp(ws.begin() + i, ws.begin() + std::min(ws.size(), i + G));
-      mqw_status s = run_grid_group(P, grp, geo, stream);
+    // Groups are dealt round-robin to the lanes, which run concurrently.
+    const int ngroups = (int)((ws.size() + G - 1) / G);
+    const int lanes = std::min(gs.lanes, ngroups);
+    CK(ctx->fork(stream, lanes));
+    for (int i = 0; i < ngroups; i++) {
+      const size_t a = (size_t)i * G;
+      std::vector<int> grp(ws.begin() + a, ws.begin() + std::min(ws.size(), a + G));
+      const int lane = i % lanes;
+      mqw_status s = run_grid_group(P, grp, geo, lane, G,
+                                    lane == 0 ? stream : ctx->lane_stream[lane]);
       if (s != MQW_OK) return s;
     }
+    CK(ctx->join(stream, lanes));
   }
   if (P.counting) CK(cudaEventRecord(P.ev1, stream));
   CK(launch_mean(P.d_p_sample.as<double>(), P.d_p_off.as<int>(),
@@ -496,28 +576,36 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
   for (size_t w = 0; w < P.walks.size(); w++)
     if (P.walk_is_grid[w]) grid_count[P.walks[w].n]++;
   size_t state_b = 0, norm_b = 0;
+  int lanes_max = 1;
   for (auto& kv : grid_count) {
     const int n = kv.first;
-    int lmax = P.opt.tile_log, G = P.opt.group;
-    if (lmax <= 0 || G <= 0) {
-      int tl = 0, tg = 0;
-      mqw_status s = tune_grid(ctx, P.precision, n, &tl, &tg);
+    GridShape gs;
+    gs.lmax = std::max(0, P.opt.tile_log);
+    gs.group = std::max(0, P.opt.group);
+    gs.lanes = std::min(std::max(0, P.opt.lanes), kMaxLanes);
+    if (!gs.lmax || !gs.group || !gs.lanes) {
+      GridShape t;
+      mqw_status s = tune_grid(ctx, P.precision, n, gs, &t);
       if (s != MQW_OK) return s;
-      if (lmax <= 0) lmax = tl;
-      if (G <= 0) G = tg;
+      gs = t;
     }
-    G = std::min(std::min(G, kMaxGroup), kv.second);
-    const PassGeomHost geo = pass_geom(P.precision, n, lmax);
-    P.grid_geo[n] = std::make_pair(lmax, G);
+    gs.group = std::min(std::min(gs.group, kMaxGroup), kv.second);
+    const int ngroups = (kv.second + gs.group - 1) / gs.group;
+    gs.lanes = std::max(1, std::min(gs.lanes, ngroups));
+    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax);
+    P.grid_geo[n] = gs;
+    lanes_max = std::max(lanes_max, gs.lanes);
     const size_t N = (size_t)1 << n;
     const size_t amp = P.precision == 0 ? 8 : 16;
-    state_b = std::max(state_b, (size_t)G * walk_slots(geo) * N * amp);
-    norm_b = std::max(norm_b, (size_t)G * (N >> geo.L) * sizeof(double));
+    const size_t walks = (size_t)gs.lanes * gs.group;
+    state_b = std::max(state_b, walks * walk_slots(geo) * N * amp);
+    norm_b = std::max(norm_b, walks * (N >> geo.L) * sizeof(double));
   }
+  CK(ctx->ensure_lanes(lanes_max));
   CK(ctx->grow(ctx->diag_scratch, P.diag_scratch_bytes));
   if (state_b) CK(ctx->grow(ctx->state, state_b));
   if (norm_b) CK(ctx->grow(ctx->norm_part, norm_b));
-  CK(ctx->grow(ctx->kappa, kMaxGroup * sizeof(double)));
+  CK(ctx->grow(ctx->kappa, kMaxLanes * kMaxGroup * sizeof(double)));
 
   // 1-2. Diagonals and degrees; degrees and onenorms are read back to lay
   // out the coefficient pool and the launch schedule.
@@ -658,6 +746,11 @@ void mqw_destroy(mqw_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  for (int k = 1; k < kMaxLanes; k++) {
+    if (ctx->lane_stream[k]) cudaStreamDestroy(ctx->lane_stream[k]);
+    if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
+  }
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   delete ctx;
 }
 

@@ -198,3 +198,17 @@ def test_cluster_tiles_match_global_partner_path(ctx, orc, n):
     assert abs(r_cl["p"][0] - r_gl["p"][0]) <= 1e-6
     assert abs(r_cl["p"][0] - r_64["p"][0]) <= 1e-5
     assert 0.0 < r_cl["p"][0] < 1.0
+
+
+def test_lanes_give_identical_results(ctx, orc, mqw):
+    """Walk groups run on 1, 2 or 3 concurrent lanes (streams, and branches
+    of the captured graph) produce bit-identical per-sample results."""
+    raw = orc.sk_instances(16, 3, 77)
+    out = []
+    for lanes in (1, 2, 3):
+        plan = mqw.Plan(ctx, 16, 3, raw, samples=7, group=2, lanes=lanes)
+        plan.execute()
+        plan.execute()  # graph replay
+        out.append(plan.results(per_sample=True)["p_sample"])
+        plan.close()
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
