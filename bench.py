@@ -384,7 +384,7 @@ def main():
     barrier()
     clocks = ClockSampler(gpu_selector(torch, local))
     step_ms, kern_ms = [], []
-    term_amps = 0.0
+    term_amps = pass_amps = 0.0
     launches = term_launches = terms = 0
     for _ in range(a.steps):
         flush.zero_()
@@ -399,6 +399,7 @@ def main():
         st = plan.stats()
         kern_ms.append(st["kernel_ms"])
         term_amps += st["term_amps"]
+        pass_amps += st["pass_amps"]
         launches += st["launches"]
         term_launches += st["term_launches"]
         terms = st["terms"]
@@ -442,9 +443,12 @@ def main():
 
     pk, pk_kind = peaks()
     kms = sum(kern_ms)
-    achieved = BYTES_PER_TERM_AMP[a.precision] * term_amps / (kms / 1000.0) / 1e9 if kms > 0 else None
+    # Bytes of the Clenshaw passes actually executed (the stage-1 basis
+    # replaces most first-stage passes; term_amps counts the reference's
+    # work) over the device time of the whole propagation phase.
+    achieved = BYTES_PER_TERM_AMP[a.precision] * pass_amps / (kms / 1000.0) / 1e9 if kms > 0 else None
     peak = pk["hbm_gbs"]
-    per_launch_amps = term_amps / max(1, term_launches)
+    per_launch_amps = pass_amps / max(1, term_launches)
     dram = DRAM_BYTES_PER_TERM_AMP.get(a.workload)
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -467,6 +471,9 @@ def main():
             except Exception as ex:  # the baseline is reported, not required
                 cpu = {"value": None, "error": str(ex)}
         config = dict(desc)
+        config["grid_shape"] = ctx.grid_shape(max(ns), a.precision)
+        config["reference_term_amps_per_step"] = term_amps / a.steps
+        config["pass_term_amps_per_step"] = pass_amps / a.steps
         config.update({"instances_per_step": count * world, "samples": a.samples,
                        "precision": a.precision, "group": a.group or "autotuned",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",

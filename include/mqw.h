@@ -62,15 +62,20 @@ typedef struct mqw_options {
   int group;       /* trajectories per grid-path launch, 0 = autotuned */
   int resident_max_n; /* largest n run with a whole state in one CTA's shared
                          memory, 0 = default (13 for FP32, 12 for FP64) */
-  const float* stage_scale; /* optional [count][m][2] multipliers applied to
-                               (gamma_i, t_i) of each stage (a learned
-                               schedule); NULL = the paper heuristic */
+  const float* stage_scale; /* optional (gamma_i, t_i) multipliers, two
+                               floats per stage, instance after instance
+                               (m_0 + m_1 + ... pairs, caller order): a
+                               learned schedule; NULL = the paper heuristic */
   int tile_log;    /* grid-path tile (log2 amplitudes), 0 = autotuned */
   int graph;       /* 1 (default): a plan's second and later executions
                       replay a CUDA graph of its whole device pipeline;
                       0: launch kernels one by one every time */
   int lanes;       /* grid-path walk groups in flight at once, each on its
                       own stream (1..4), 0 = autotuned */
+  int stage1_basis; /* 1 (default): FP32 walks of an instance share one
+                       Chebyshev basis for their first stage (built once,
+                       recombined per walk); 0: every walk runs its own
+                       first-stage recurrence */
 } mqw_options;
 
 typedef struct mqw_diag_info {
@@ -92,6 +97,10 @@ typedef struct mqw_run_stats {
                                events on the launching stream) */
   double h2d_bytes;         /* host-to-device bytes copied by the plan */
   double d2h_bytes;         /* device-to-host bytes copied by the plan */
+  double pass_amps;         /* term x amplitudes the grid-path Clenshaw passes
+                               actually executed (stage-1 recombination
+                               replaces the per-walk first stage, so this can
+                               be below term_amps) */
 } mqw_run_stats;
 
 typedef struct mqw_ctx mqw_ctx;
@@ -218,6 +227,18 @@ mqw_status mqw_plan_results(mqw_plan* plan, double* p_out, float* total_t,
                             uint32_t* e_loc, double* p_sample);
 mqw_status mqw_plan_stats(const mqw_plan* plan, mqw_run_stats* stats);
 void mqw_plan_destroy(mqw_plan* plan);
+
+/* The grid-path shape the autotuner picks for n-spin walks in `precision`
+ * on this context (tuning now if it has not yet): tile of 2^tile_log
+ * amplitudes per CTA, spread over 2^cluster_log CTAs; global_axes axes whose
+ * partners are read from global memory; group walks per launch; lanes
+ * launches in flight; us_per_walk_pass the timed cost of one walk-term. */
+typedef struct mqw_grid_shape {
+  int tile_log, cluster_log, global_axes, group, lanes;
+  double us_per_walk_pass;
+} mqw_grid_shape;
+mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,
+                              mqw_grid_shape* out);
 
 /* ---- learned stage schedule (no counterpart in the reference) ---------- */
 /* Building blocks of the MLP that proposes per-stage (gamma, t) multipliers

@@ -56,6 +56,7 @@ class Options(ctypes.Structure):
         ("tile_log", ctypes.c_int),
         ("graph", ctypes.c_int),
         ("lanes", ctypes.c_int),
+        ("stage1_basis", ctypes.c_int),
     ]
 
 
@@ -69,6 +70,20 @@ class DiagInfo(ctypes.Structure):
     ]
 
 
+class GridShape(ctypes.Structure):
+    _fields_ = [
+        ("tile_log", ctypes.c_int),
+        ("cluster_log", ctypes.c_int),
+        ("global_axes", ctypes.c_int),
+        ("group", ctypes.c_int),
+        ("lanes", ctypes.c_int),
+        ("us_per_walk_pass", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class RunStats(ctypes.Structure):
     _fields_ = [
         ("instances", ctypes.c_longlong),
@@ -80,6 +95,7 @@ class RunStats(ctypes.Structure):
         ("kernel_ms", ctypes.c_double),
         ("h2d_bytes", ctypes.c_double),
         ("d2h_bytes", ctypes.c_double),
+        ("pass_amps", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:
@@ -116,6 +132,7 @@ def _bind(L):
         "mqw_plan_destroy": (None, [_vp]),
         "mqw_multiqw": (i, [_vp, i, i, ctypes.c_char_p, ll, ll, ctypes.c_char_p, i]),
         "mqw_clenshaw_noalloc": (i, [i, i, i, _vp, _vp, f, f, _vp, _vp, _vp]),
+        "mqw_grid_shape_for": (i, [_vp, i, i, _P(GridShape)]),
         "mqw_mlp_linear_forward": (i, [i, i, i, _vp, _vp, _vp, _vp, i, _vp]),
         "mqw_mlp_linear_backward": (i, [i, i, i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, i, _vp]),
         "mqw_mlp_adam": (i, [i, _vp, _vp, _vp, _vp, _vp, f, f, f, f, f, i, _vp]),
@@ -156,7 +173,7 @@ def _ptr(a, ct):
 
 
 def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_max_n=0,
-          stage_scale=None, tile_log=0, graph=1, lanes=0):
+          stage_scale=None, tile_log=0, graph=1, lanes=0, stage1_basis=1):
     o = Options()
     lib().mqw_default_options(ctypes.byref(o))
     o.precision = {"fp32": FP32, "fp64": FP64, FP32: FP32, FP64: FP64}[precision]
@@ -167,6 +184,7 @@ def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_ma
     o.tile_log = int(tile_log)
     o.graph = int(graph)
     o.lanes = int(lanes)
+    o.stage1_basis = int(stage1_basis)
     keep = None
     if stage_scale is not None:
         keep = np.ascontiguousarray(stage_scale, dtype=np.float32)
@@ -301,6 +319,13 @@ class Context:
                                               _ptr(el, ctypes.c_uint32), ctypes.byref(stats)))
         del keep
         return {"p": p, "total_t": tt, "e_loc": el, "stats": stats.as_dict()}
+
+    def grid_shape(self, n: int, precision="fp32") -> dict:
+        """The autotuned grid-path shape for n-spin walks (tunes on first use)."""
+        g = GridShape()
+        prec = FP32 if precision == "fp32" else FP64
+        _check(self.h, lib().mqw_grid_shape_for(self.h, prec, n, ctypes.byref(g)))
+        return g.as_dict()
 
     def multiqw(self, n: int, m: int, filename: str, start: int = 0, problems: int = 2000,
                 out_dir: str | None = None, print_: bool = True):

@@ -20,6 +20,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -67,6 +68,7 @@ struct DevMem {
 // concurrent launch lanes.
 struct GridShape {
   int lmax = 0, group = 1, lanes = 1;
+  double us = 0.0;  // timed microseconds per walk-pass (0: not timed)
 };
 constexpr int kMaxLanes = 4;
 
@@ -76,6 +78,7 @@ struct mqw_ctx {
   std::string err;
   int sm_count = 0;
   DevMem state, norm_part, kappa, diag_scratch, tune_coef;
+  DevMem basis;  // stage-1 basis of the instance in flight (+ its partial P)
   // Bumped whenever a shared scratch buffer is reallocated: a plan's captured
   // graph holds the old addresses and is re-captured when this changes.
   unsigned long long scratch_gen = 1;
@@ -165,6 +168,7 @@ void default_opts(mqw_options* o) {
   o->tile_log = 0;
   o->graph = 1;
   o->lanes = 0;
+  o->stage1_basis = 1;
 }
 
 }  // namespace
@@ -194,6 +198,11 @@ struct mqw_plan {
   DevMem d_coef, d_coef_off, d_stages, d_walks;
   // Grid-path shape chosen for each n of the plan.
   std::map<int, GridShape> grid_geo;
+  // Stage-1 basis: vectors per instance (0 = not used for that n) and the
+  // unit coefficient list the basis passes read ([0, ..., 0, 1]).
+  std::map<int, int> basis_kb;
+  DevMem d_unit;
+  int unit_len = 0;
   // CUDA graph of the whole device pipeline, replayed by later executes.
   cudaGraphExec_t gexec = nullptr;
   unsigned long long graph_gen = 0;
@@ -351,11 +360,15 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
         if (s != MQW_OK) return s;
         // Prefer the earlier candidate (larger tile, fewer walks in flight)
         // unless a later one is clearly faster.
+        if (getenv("MQW_TUNE_LOG"))
+          fprintf(stderr, "mqw tune: precision %d n %d tile %d cluster %d global %d group %d lanes %d: %.3f us/walk-pass\n",
+                  precision, n, geo.L, geo.C, geo.nu, g, lanes, us);
         if (us < best * 0.98) {
           best = us;
           b.lmax = l;
           b.group = g;
           b.lanes = lanes;
+          b.us = us;
         }
       }
     }
@@ -373,9 +386,11 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
 // uses tiling 1 for even r and tiling 2 for odd r.
 // `lane` selects the lane's own slice of the shared scratch (state, norm
 // partials, kappa), sized for groups of `gmax` walks.
+// With `basis` set (the instance's stage-1 basis of Kb vectors), the first
+// stage is recombined from it instead of run as a recurrence per walk.
 mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
                           const PassGeomHost& geo, int lane, int gmax,
-                          cudaStream_t stream) {
+                          const void* basis, int Kb, cudaStream_t stream) {
   mqw_ctx* ctx = P.ctx;
   const int n = P.walks[widx[0]].n;
   const size_t N = (size_t)1 << n;
@@ -409,6 +424,25 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
       K[g] = st < w.stages ? P.degree[w.stage_desc_off + st] : 0;
       Kmax = std::max(Kmax, K[g]);
     }
+    if (st == 0 && basis) {
+      CombineParams cp{};
+      cp.basis = basis;
+      cp.n = n;
+      cp.L = geo.L;
+      cp.Kb = Kb;
+      cp.count = G;
+      for (int g = 0; g < G; g++) {
+        const int job = P.walks[widx[g]].stage_desc_off;
+        CombineWalk& C = cp.walk[g];
+        C.coef = coef + P.coef_off[job];
+        C.K = K[g];
+        C.out = buf(g, xs[g]);
+        C.norm_part = norm_part + (size_t)g * tiles;
+      }
+      CK(launch_combine(P.precision, cp, stream));
+      if (P.counting) P.stats.launches++;
+      Kmax = 0;  // no recurrence passes for this stage
+    }
     for (int r = Kmax - 1; r >= 0; r--) {
       PassParams pp{};
       pp.n = n;
@@ -441,7 +475,7 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
         W.K = K[g];
         W.psi_uniform = st == 0;  // every walk starts from the uniform state
         W.psi0 = (float)(1.0 / std::sqrt((double)N));
-        if (P.counting) P.stats.term_amps += (double)N;
+        if (P.counting) P.stats.pass_amps += (double)N;
       }
       CK(launch_pass(P.precision, pp, stream));
       if (P.counting) {
@@ -470,6 +504,56 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
     for (int g = 0; g < G; g++) {
       if (st >= P.walks[widx[g]].stages) continue;
       std::swap(pi[g], xs[g]);  // the output (slot x) becomes psi
+    }
+  }
+  return MQW_OK;
+}
+
+// Builds the stage-1 basis w_0 .. w_{Kb-1} of the instance of walk w0 into
+// ctx->basis (slot 0 holds the passes' partial P, slot 1 + j holds w_j):
+// Kb single-walk passes with c = [0, .., 0, 1] at an even top index R >= Kb,
+// so that b_R = psi0 and every later pass is b_r = 2 H~ b_{r+1} - b_{r+2};
+// the passes stop at r = R - Kb + 1 >= 1 (the r = 0 form is never used).
+mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int Kb,
+                       const PassGeomHost& geo, cudaStream_t stream) {
+  mqw_ctx* ctx = P.ctx;
+  const int n = w0.n;
+  const size_t N = (size_t)1 << n;
+  const size_t amp = P.precision == 0 ? 8 : 16;
+  char* base = ctx->basis.as<char>();
+  auto slot = [&](int k) -> void* { return base + (size_t)k * N * amp; };
+  const int R = Kb + (Kb & 1);
+  const int job = w0.stage_desc_off;
+  const float* unit = P.d_unit.as<float>() + (P.unit_len - 1 - R);
+  for (int j = 0; j < Kb; j++) {
+    PassParams pp{};
+    pp.n = n;
+    pp.L = geo.L;
+    pp.C = geo.C;
+    pp.a = geo.a;
+    pp.tiling = ((R - j) & 1) ? 2 : 1;
+    pp.count = 1;
+    PassWalk& W = pp.walk[0];
+    W.active = 1;
+    W.bin = slot(j == 0 ? 1 : j);  // not read by the first pass
+    W.bout = slot(1 + j);
+    W.part = slot(0);
+    W.psi = slot(1);  // not read: the uniform state
+    W.hp = P.d_hp.as<float>() + w0.hp_off;
+    W.coef = unit;
+    W.kappa = nullptr;
+    W.norm_part = ctx->norm_part.as<double>();  // not written (r >= 1)
+    W.gamma = P.jobs[job].gamma;
+    W.scale = P.onenorm[job];
+    W.r = R - j;
+    W.K = R + 1;
+    W.psi_uniform = 1;
+    W.psi0 = (float)(1.0 / std::sqrt((double)N));
+    CK(launch_pass(P.precision, pp, stream));
+    if (P.counting) {
+      P.stats.launches++;
+      P.stats.term_launches++;
+      P.stats.pass_amps += (double)N;
     }
   }
   return MQW_OK;
@@ -530,19 +614,44 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
     const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax);
     const int G = gs.group;
     const std::vector<int>& ws = kv.second;
-    // Groups are dealt round-robin to the lanes, which run concurrently.
-    const int ngroups = (int)((ws.size() + G - 1) / G);
-    const int lanes = std::min(gs.lanes, ngroups);
-    CK(ctx->fork(stream, lanes));
-    for (int i = 0; i < ngroups; i++) {
-      const size_t a = (size_t)i * G;
-      std::vector<int> grp(ws.begin() + a, ws.begin() + std::min(ws.size(), a + G));
-      const int lane = i % lanes;
-      mqw_status s = run_grid_group(P, grp, geo, lane, G,
-                                    lane == 0 ? stream : ctx->lane_stream[lane]);
-      if (s != MQW_OK) return s;
+    const int kb_cap = P.basis_kb.count(n) ? P.basis_kb.at(n) : 0;
+    // Blocks of walks: one block per instance when the stage-1 basis is used
+    // (the basis is built before, and read during, the block), else all.
+    size_t b0 = 0;
+    while (b0 < ws.size()) {
+      size_t b1 = ws.size();
+      const void* basis = nullptr;
+      int Kb = 0;
+      if (kb_cap > 0) {
+        b1 = b0;
+        while (b1 < ws.size() && P.walks[ws[b1]].inst == P.walks[ws[b0]].inst) b1++;
+        const ResidentWalk& w0 = P.walks[ws[b0]];
+        if (!w0.record_each && w0.stages >= 2) {
+          for (size_t k = b0; k < b1; k++)
+            Kb = std::max(Kb, P.degree[P.walks[ws[k]].stage_desc_off]);
+          if (Kb <= kb_cap) {
+            mqw_status s = issue_basis(P, w0, Kb, geo, stream);
+            if (s != MQW_OK) return s;
+            basis = ctx->basis.as<char>() + ((size_t)1 << n) * (P.precision == 0 ? 8 : 16);
+          }
+        }
+      }
+      // Groups are dealt round-robin to the lanes, which run concurrently.
+      const int nw = (int)(b1 - b0);
+      const int ngroups = (nw + G - 1) / G;
+      const int lanes = std::min(gs.lanes, ngroups);
+      CK(ctx->fork(stream, lanes));
+      for (int i = 0; i < ngroups; i++) {
+        const size_t a = b0 + (size_t)i * G;
+        std::vector<int> grp(ws.begin() + a, ws.begin() + std::min(b1, a + G));
+        const int lane = i % lanes;
+        mqw_status s = run_grid_group(P, grp, geo, lane, G, basis, basis ? Kb : 0,
+                                      lane == 0 ? stream : ctx->lane_stream[lane]);
+        if (s != MQW_OK) return s;
+      }
+      CK(ctx->join(stream, lanes));
+      b0 = b1;
     }
-    CK(ctx->join(stream, lanes));
   }
   if (P.counting) CK(cudaEventRecord(P.ev1, stream));
   CK(launch_mean(P.d_p_sample.as<double>(), P.d_p_off.as<int>(),
@@ -569,6 +678,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
   }
   P.counting = true;
   P.stats.launches = P.stats.term_launches = 0;
+  P.stats.pass_amps = 0;
   P.stats.h2d_bytes = P.stats.d2h_bytes = 0;
   // Geometry and shared scratch for every n of the plan, sized up front so
   // that nothing is allocated while the pipeline is issued or captured.
@@ -639,11 +749,47 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
   std::vector<ResidentWalk> res;
   P.stats.term_amps = 0;
   for (size_t w = 0; w < P.walks.size(); w++) {
-    if (P.walk_is_grid[w]) continue;
-    res.push_back(P.walks[w]);
     for (int st = 0; st < P.walks[w].stages; st++)
       P.stats.term_amps += (double)P.degree[P.walks[w].stage_desc_off + st] *
                            (double)(1u << P.walks[w].n);
+    if (!P.walk_is_grid[w]) res.push_back(P.walks[w]);
+  }
+  // Stage-1 basis: the largest first-stage degree per n decides the buffer;
+  // an n whose basis would not fit the budget runs without it.
+  P.basis_kb.clear();
+  if (P.opt.stage1_basis && P.precision == 0) {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)8 << 30;
+    const size_t budget = std::min(free_b / 4, (size_t)8 << 30);
+    std::map<int, int> kb;
+    for (size_t w = 0; w < P.walks.size(); w++) {
+      const ResidentWalk& wk = P.walks[w];
+      if (!P.walk_is_grid[w] || wk.record_each || wk.stages < 2) continue;
+      int& k = kb[wk.n];
+      k = std::max(k, P.degree[wk.stage_desc_off]);
+    }
+    size_t basis_b = 0;
+    int rmax = 0;
+    for (auto& e : kb) {
+      const size_t bytes = (size_t)(e.second + 1) * ((size_t)1 << e.first) * 8;
+      if (e.second > kMaxBasis || bytes > budget) continue;
+      P.basis_kb[e.first] = e.second;
+      basis_b = std::max(basis_b, bytes);
+      rmax = std::max(rmax, e.second + (e.second & 1));
+    }
+    if (basis_b) {
+      CK(ctx->grow(ctx->basis, basis_b));
+      if (P.unit_len < rmax + 1) {
+        std::vector<float> unit(rmax + 1, 0.0f);
+        unit[rmax] = 1.0f;
+        CK(P.d_unit.ensure(unit.size() * sizeof(float)));
+        CK(cudaMemcpyAsync(P.d_unit.p, unit.data(), unit.size() * sizeof(float),
+                           cudaMemcpyHostToDevice, stream));
+        CK(cudaStreamSynchronize(stream));  // `unit` is a local buffer
+        P.unit_len = rmax + 1;
+        P.stats.h2d_bytes += (double)unit.size() * sizeof(float);
+      }
+    }
   }
   // A re-layout drops any captured graph (its addresses may change).
   if (P.gexec) {
@@ -808,8 +954,11 @@ mqw_status mqw_plan_create(mqw_ctx* ctx, int count, const int* n, const int* m,
   P->n.assign(n, n + count);
   P->m.assign(m, m + count);
   P->total_t.assign(count, 0.0f);
-  std::vector<long long> caller_off(count + 1, 0);
-  for (int i = 0; i < count; i++) caller_off[i + 1] = caller_off[i] + params_per(n[i]);
+  std::vector<long long> caller_off(count + 1, 0), stage_off(count + 1, 0);
+  for (int i = 0; i < count; i++) {
+    caller_off[i + 1] = caller_off[i] + params_per(n[i]);
+    stage_off[i + 1] = stage_off[i] + m[i];
+  }
   P->order.resize(count);
   std::iota(P->order.begin(), P->order.end(), 0);
   std::stable_sort(P->order.begin(), P->order.end(),
@@ -840,8 +989,8 @@ mqw_status mqw_plan_create(mqw_ctx* ctx, int count, const int* n, const int* m,
     P->total_t[i] = tot;
     if (opt.stage_scale) {
       for (int s2 = 0; s2 < mi; s2++) {
-        const float fg = opt.stage_scale[((size_t)i * mi + s2) * 2 + 0];
-        const float ft = opt.stage_scale[((size_t)i * mi + s2) * 2 + 1];
+        const float fg = opt.stage_scale[(size_t)(stage_off[i] + s2) * 2 + 0];
+        const float ft = opt.stage_scale[(size_t)(stage_off[i] + s2) * 2 + 1];
         if (!(fg > 0.0f) || !(ft > 0.0f) || !std::isfinite(fg) || !std::isfinite(ft))
           return fail(ctx, MQW_ERR_INVALID, "stage_scale must be positive and finite");
         gam[s2] *= fg;
@@ -957,6 +1106,25 @@ mqw_status mqw_plan_results(mqw_plan* plan, double* p_out, float* total_t,
   }
   if (total_t)
     for (int i = 0; i < count; i++) total_t[i] = plan->total_t[i];
+  return MQW_OK;
+}
+
+mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,
+                              mqw_grid_shape* out) {
+  mqw_status st = check_ctx(ctx);
+  if (st != MQW_OK) return st;
+  if (!out || (precision != MQW_FP32 && precision != MQW_FP64) || n < 6 || n > kMaxN)
+    return fail(ctx, MQW_ERR_INVALID, "mqw_grid_shape_for: bad arguments");
+  GridShape gs;
+  st = tune_grid(ctx, precision, n, GridShape{0, 0, 0, 0.0}, &gs);
+  if (st != MQW_OK) return st;
+  const PassGeomHost geo = pass_geom(precision, n, gs.lmax);
+  out->tile_log = geo.L;
+  out->cluster_log = geo.C;
+  out->global_axes = geo.nu;
+  out->group = gs.group;
+  out->lanes = gs.lanes;
+  out->us_per_walk_pass = gs.us;
   return MQW_OK;
 }
 

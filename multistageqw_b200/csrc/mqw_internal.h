@@ -146,6 +146,32 @@ PassGeomHost pass_geom(int precision, int n, int lmax = 0);
 cudaError_t launch_pass(int precision, const PassParams& p,
                         cudaStream_t stream);
 
+// Stage-1 shared basis. Every walk of an instance starts from the uniform
+// state psi0 and its first stage applies the same operator H~ (one gamma and
+// onenorm per instance stage), only with its own time, i.e. its own
+// coefficients. The basis w_j = U_j(H~) psi0 (Chebyshev polynomials of the
+// second kind: w_0 = psi0, w_1 = 2 H~ psi0, w_{j+1} = 2 H~ w_j - w_{j-1},
+// real vectors stored as interleaved complex with zero imaginary part) is
+// built once per instance by pass_kernel launches with one unit coefficient,
+// and each walk's stage output sum_k c_k T_k(H~) psi0 is recombined from it:
+// with T_0 = U_0, T_1 = U_1 / 2, T_k = (U_k - U_{k-2}) / 2,
+//   sum_k c_k T_k = sum_j d_j U_j,  d_0 = c_0 - c_2/2,  d_j = (c_j - c_{j+2})/2,
+// d_j real for even j and imaginary for odd j, like c_j.
+struct CombineWalk {
+  const float* coef;   // the walk's stage-1 coefficients c_0 .. c_{K-1}
+  int K;
+  void* out;           // stage output (interleaved complex, 2^n amplitudes)
+  double* norm_part;   // per-block |out|^2 partials (2^(n-L) blocks)
+};
+struct CombineParams {
+  const void* basis;   // Kb vectors of 2^n interleaved complex amplitudes
+  int n, L, Kb, count;
+  CombineWalk walk[kMaxGroup];
+};
+constexpr int kMaxBasis = 1024;  // basis vectors (stage-1 degree bound)
+cudaError_t launch_combine(int precision, const CombineParams& p,
+                           cudaStream_t stream);
+
 // Finalisation after a stage: kappa[g] = 1/sqrt(sum of partials); when
 // record != 0 also p_out[g] = |out[e_loc]|^2 * kappa^2.
 struct FinalTraj {

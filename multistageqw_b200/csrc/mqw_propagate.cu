@@ -544,6 +544,69 @@ __global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 
   if constexpr (CL > 0) cluster_barrier();
 }
 
+// Stage-1 recombination: block b covers amplitudes [b 2^L, (b+1) 2^L) of
+// every walk of the group, reads each basis vector once for all walks, and
+// leaves the block's |out|^2 in norm_part[b] (fixed order: deterministic).
+template <typename R>
+__global__ void __launch_bounds__(256) combine_kernel(CombineParams p) {
+  __shared__ float sd[kMaxGroup][kMaxBasis];
+  __shared__ double s_red[32];
+  const int Kb = p.Kb, G = p.count;
+  for (int e = threadIdx.x; e < G * Kb; e += blockDim.x) {
+    const int g = e / Kb, j = e % Kb;
+    const CombineWalk& W = p.walk[g];
+    const float cj = j < W.K ? W.coef[j] : 0.0f;
+    const float cj2 = j + 2 < W.K ? W.coef[j + 2] : 0.0f;
+    sd[g][j] = j == 0 ? cj - 0.5f * cj2 : 0.5f * (cj - cj2);
+  }
+  __syncthreads();
+  const size_t N = (size_t)1 << p.n;
+  const size_t chunk = (size_t)1 << p.L;
+  const size_t base = (size_t)blockIdx.x * chunk;
+  const R* basis = reinterpret_cast<const R*>(p.basis);
+  double nrm[kMaxGroup];
+#pragma unroll
+  for (int g = 0; g < kMaxGroup; g++) nrm[g] = 0.0;
+  // Two amplitudes per thread and step: one 16-byte (FP32) load per vector.
+  for (size_t i = base + 2 * threadIdx.x; i < base + chunk; i += 2 * blockDim.x) {
+    R re0[kMaxGroup], im0[kMaxGroup], re1[kMaxGroup], im1[kMaxGroup];
+#pragma unroll
+    for (int g = 0; g < kMaxGroup; g++) re0[g] = im0[g] = re1[g] = im1[g] = (R)0;
+    for (int j = 0; j < Kb; j++) {
+      const V4<R> w = ld4<R>(basis + 2 * ((size_t)j * N + i));  // (w[i], 0, w[i+1], 0)
+      if (j & 1) {
+#pragma unroll
+        for (int g = 0; g < kMaxGroup; g++)
+          if (g < G) {
+            im0[g] = fma((R)sd[g][j], w.x, im0[g]);
+            im1[g] = fma((R)sd[g][j], w.z, im1[g]);
+          }
+      } else {
+#pragma unroll
+        for (int g = 0; g < kMaxGroup; g++)
+          if (g < G) {
+            re0[g] = fma((R)sd[g][j], w.x, re0[g]);
+            re1[g] = fma((R)sd[g][j], w.z, re1[g]);
+          }
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < kMaxGroup; g++)
+      if (g < G) {
+        st4<R>(reinterpret_cast<R*>(p.walk[g].out) + 2 * i, V4<R>{re0[g], im0[g], re1[g], im1[g]});
+        nrm[g] += (double)re0[g] * re0[g] + (double)im0[g] * im0[g] +
+                  (double)re1[g] * re1[g] + (double)im1[g] * im1[g];
+      }
+  }
+#pragma unroll
+  for (int g = 0; g < kMaxGroup; g++)
+    if (g < G) {  // uniform over the block
+      const double sum = block_sum<R>(nrm[g], s_red);
+      if (threadIdx.x == 0) p.walk[g].norm_part[blockIdx.x] = sum;
+      __syncthreads();  // s_red is reused by the next walk's sum
+    }
+}
+
 template <typename R>
 __global__ void finalize_kernel(FinalParams p) {
   using C2 = typename Cplx<R>::T;
@@ -793,6 +856,23 @@ cudaError_t launch_pass(int precision, const PassParams& p,
     return cudaErrorInvalidValue;
   return precision == 0 ? launch_pass_t<float>(p, stream)
                         : launch_pass_t<double>(p, stream);
+}
+
+cudaError_t launch_combine(int precision, const CombineParams& p,
+                           cudaStream_t stream) {
+  if (p.n < 6 || p.n > kMaxN || p.L < 6 || p.L > p.n || p.Kb < 1 || p.Kb > kMaxBasis ||
+      p.count < 1 || p.count > kMaxGroup || !p.basis)
+    return cudaErrorInvalidValue;
+  for (int g = 0; g < p.count; g++)
+    if (p.walk[g].K < 1 || p.walk[g].K > p.Kb || !p.walk[g].coef || !p.walk[g].out ||
+        !p.walk[g].norm_part)
+      return cudaErrorInvalidValue;
+  const unsigned blocks = (unsigned)((size_t)1 << (p.n - p.L));
+  if (precision == 0)
+    combine_kernel<float><<<blocks, 256, 0, stream>>>(p);
+  else
+    combine_kernel<double><<<blocks, 256, 0, stream>>>(p);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_finalize(int precision, const FinalParams& p,

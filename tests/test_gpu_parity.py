@@ -212,3 +212,20 @@ def test_lanes_give_identical_results(ctx, orc, mqw):
         out.append(plan.results(per_sample=True)["p_sample"])
         plan.close()
     assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
+
+
+@pytest.mark.parametrize("n,m", [(14, 2), (17, 3), (20, 4)])
+def test_stage1_basis_matches_per_walk_recurrence(ctx, orc, n, m):
+    """The shared stage-1 basis (built once per instance, recombined per
+    walk) against every walk running its own first-stage recurrence and
+    against FP64: same ground-state probabilities to FP32 accuracy, with less
+    pass work."""
+    raw = orc.sk_instances(n, 2, 900 + n)
+    kw = dict(samples=12, graph=0)
+    on = ctx.run_problems(n, m, raw, precision="fp32", **kw)
+    off = ctx.run_problems(n, m, raw, precision="fp32", stage1_basis=0, **kw)
+    r64 = ctx.run_problems(n, m, raw, precision="fp64", **kw)
+    assert np.abs(on["p"] - off["p"]).max() <= 1e-6
+    assert np.abs(on["p"] - r64["p"]).max() <= 1e-5
+    assert on["stats"]["term_amps"] == off["stats"]["term_amps"]
+    assert on["stats"]["pass_amps"] < 0.95 * off["stats"]["pass_amps"]
