@@ -64,7 +64,9 @@ def parse():
     ap.add_argument("--batch", type=int, default=2, help="instances per step per GPU")
     ap.add_argument("--samples", type=int, default=100)
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
-    ap.add_argument("--group", type=int, default=0)
+    ap.add_argument("--group", type=int, default=0, help="walks per launch (0: autotuned)")
+    ap.add_argument("--tile-log", type=int, default=0, help="grid-path tile cap (0: autotuned)")
+    ap.add_argument("--lanes", type=int, default=0, help="concurrent launch lanes (0: autotuned)")
     ap.add_argument("--seed", type=int, default=20)
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 |dP| check")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -371,7 +373,8 @@ def main():
     torch.cuda.set_stream(stream)
     ns, ms, raw, desc = make_batch(M, a, rank)
     count = len(ns)
-    plan = M.Plan(ctx, ns, ms, raw, samples=a.samples, precision=a.precision, group=a.group)
+    shape = dict(group=a.group, tile_log=a.tile_log, lanes=a.lanes)
+    plan = M.Plan(ctx, ns, ms, raw, samples=a.samples, precision=a.precision, **shape)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
     def barrier():
@@ -417,7 +420,7 @@ def main():
         barrier()
         t0 = time.perf_counter()
         p2 = M.Plan(ctx, ns, ms, raw_pinned, samples=a.samples, precision=a.precision,
-                    group=a.group, graph=0)
+                    graph=0, **shape)
         p2.execute()
         r = p2.results()
         torch.cuda.synchronize(dev)
@@ -471,7 +474,8 @@ def main():
             except Exception as ex:  # the baseline is reported, not required
                 cpu = {"value": None, "error": str(ex)}
         config = dict(desc)
-        config["grid_shape"] = ctx.grid_shape(max(ns), a.precision)
+        if not (a.group or a.tile_log or a.lanes):
+            config["grid_shape"] = ctx.grid_shape(max(ns), a.precision)
         config["reference_term_amps_per_step"] = term_amps / a.steps
         config["pass_term_amps_per_step"] = pass_amps / a.steps
         config.update({"instances_per_step": count * world, "samples": a.samples,

@@ -72,6 +72,8 @@ typedef struct mqw_options {
                       0: launch kernels one by one every time */
   int lanes;       /* grid-path walk groups in flight at once, each on its
                       own stream (1..4), 0 = autotuned */
+  int threads;     /* CTA threads of the grid path at its widest tile: 512
+                      or 256 (twice the amplitudes per thread), 0 = autotuned */
   int stage1_basis; /* 1 (default): FP32 walks of an instance share one
                        Chebyshev basis for their first stage (built once,
                        recombined per walk); 0: every walk runs its own
@@ -235,6 +237,7 @@ void mqw_plan_destroy(mqw_plan* plan);
  * launches in flight; us_per_walk_pass the timed cost of one walk-term. */
 typedef struct mqw_grid_shape {
   int tile_log, cluster_log, global_axes, group, lanes;
+  int threads;     /* threads per CTA */
   double us_per_walk_pass;
 } mqw_grid_shape;
 mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,

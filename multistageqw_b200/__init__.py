@@ -56,6 +56,7 @@ class Options(ctypes.Structure):
         ("tile_log", ctypes.c_int),
         ("graph", ctypes.c_int),
         ("lanes", ctypes.c_int),
+        ("threads", ctypes.c_int),
         ("stage1_basis", ctypes.c_int),
     ]
 
@@ -77,6 +78,7 @@ class GridShape(ctypes.Structure):
         ("global_axes", ctypes.c_int),
         ("group", ctypes.c_int),
         ("lanes", ctypes.c_int),
+        ("threads", ctypes.c_int),
         ("us_per_walk_pass", ctypes.c_double),
     ]
 
@@ -173,7 +175,7 @@ def _ptr(a, ct):
 
 
 def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_max_n=0,
-          stage_scale=None, tile_log=0, graph=1, lanes=0, stage1_basis=1):
+          stage_scale=None, tile_log=0, graph=1, lanes=0, threads=0, stage1_basis=1):
     o = Options()
     lib().mqw_default_options(ctypes.byref(o))
     o.precision = {"fp32": FP32, "fp64": FP64, FP32: FP32, FP64: FP64}[precision]
@@ -184,6 +186,7 @@ def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_ma
     o.tile_log = int(tile_log)
     o.graph = int(graph)
     o.lanes = int(lanes)
+    o.threads = int(threads)
     o.stage1_basis = int(stage1_basis)
     keep = None
     if stage_scale is not None:

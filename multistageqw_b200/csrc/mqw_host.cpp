@@ -68,6 +68,7 @@ struct DevMem {
 // concurrent launch lanes.
 struct GridShape {
   int lmax = 0, group = 1, lanes = 1;
+  int threads = 0;  // CTA threads at the widest tile (0: 512)
   double us = 0.0;  // timed microseconds per walk-pass (0: not timed)
 };
 constexpr int kMaxLanes = 4;
@@ -168,6 +169,7 @@ void default_opts(mqw_options* o) {
   o->tile_log = 0;
   o->graph = 1;
   o->lanes = 0;
+  o->threads = 0;
   o->stage1_basis = 1;
 }
 
@@ -259,8 +261,8 @@ int default_group(int precision, const PassGeomHost& geo, int n) {
 // tilings) over G zero-filled walks on each of `lanes` concurrent streams.
 // Returns microseconds per walk-pass.
 mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
-                            int G, int lanes, double* us_per_walk) {
-  const PassGeomHost geo = pass_geom(precision, n, lmax);
+                            int G, int lanes, int threads, double* us_per_walk) {
+  const PassGeomHost geo = pass_geom(precision, n, lmax, threads);
   const size_t N = (size_t)1 << n;
   const size_t amp = precision == 0 ? 8 : 16;
   const int slots = walk_slots(geo);
@@ -279,6 +281,7 @@ mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
     pp.n = n;
     pp.L = geo.L;
     pp.C = geo.C;
+    pp.threads = geo.threads;
     pp.a = geo.a;
     pp.tiling = (r & 1) ? 2 : 1;
     pp.count = G;
@@ -333,7 +336,8 @@ mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
 mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridShape* out) {
   const auto key = std::make_pair(precision, n);
   auto it = ctx->tuned.find(key);
-  if (it != ctx->tuned.end() && !want.lmax && !want.group && !want.lanes) {
+  const bool fixed_none = !want.lmax && !want.group && !want.lanes && !want.threads;
+  if (it != ctx->tuned.end() && fixed_none) {
     *out = it->second;
     return MQW_OK;
   }
@@ -348,32 +352,37 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
   b.lanes = want.lanes ? want.lanes : 1;
   for (int l = def_l; l >= def_l - 1; l--) {
     if (want.lmax && l != want.lmax) continue;
-    const PassGeomHost geo = pass_geom(precision, n, l);
-    const int g0 = default_group(precision, geo, n);
-    for (int g : {1, 2, 3, 4, g0}) {
-      if (want.group && g != want.group) continue;
-      for (int lanes : {1, 2}) {
-        if (want.lanes && lanes != want.lanes) continue;
-        if (g > kMaxGroup || (size_t)g * lanes * walk_bytes(precision, geo, n) > budget) continue;
-        double us = 0.0;
-        mqw_status s = time_grid_config(ctx, precision, n, l, g, lanes, &us);
-        if (s != MQW_OK) return s;
-        // Prefer the earlier candidate (larger tile, fewer walks in flight)
-        // unless a later one is clearly faster.
-        if (getenv("MQW_TUNE_LOG"))
-          fprintf(stderr, "mqw tune: precision %d n %d tile %d cluster %d global %d group %d lanes %d: %.3f us/walk-pass\n",
-                  precision, n, geo.L, geo.C, geo.nu, g, lanes, us);
-        if (us < best * 0.98) {
-          best = us;
-          b.lmax = l;
-          b.group = g;
-          b.lanes = lanes;
-          b.us = us;
+    for (int threads : {0, 256}) {
+      if (want.threads && (want.threads == 256) != (threads == 256)) continue;
+      const PassGeomHost geo = pass_geom(precision, n, l, threads);
+      if (geo.threads != threads) continue;  // no 256-thread shape here
+      const int g0 = default_group(precision, geo, n);
+      for (int g : {1, 2, 3, 4, g0}) {
+        if (want.group && g != want.group) continue;
+        for (int lanes : {1, 2}) {
+          if (want.lanes && lanes != want.lanes) continue;
+          if (g > kMaxGroup || (size_t)g * lanes * walk_bytes(precision, geo, n) > budget) continue;
+          double us = 0.0;
+          mqw_status s = time_grid_config(ctx, precision, n, l, g, lanes, threads, &us);
+          if (s != MQW_OK) return s;
+          if (getenv("MQW_TUNE_LOG"))
+            fprintf(stderr, "mqw tune: precision %d n %d tile %d cluster %d global %d threads %d group %d lanes %d: %.3f us/walk-pass\n",
+                    precision, n, geo.L, geo.C, geo.nu, threads ? threads : 512, g, lanes, us);
+          // Prefer the earlier candidate (larger tile, fewer walks in flight)
+          // unless a later one is clearly faster.
+          if (us < best * 0.98) {
+            best = us;
+            b.lmax = l;
+            b.group = g;
+            b.lanes = lanes;
+            b.threads = threads;
+            b.us = us;
+          }
         }
       }
     }
   }
-  if (!want.lmax && !want.group && !want.lanes) ctx->tuned[key] = b;
+  if (fixed_none) ctx->tuned[key] = b;
   *out = b;
   return MQW_OK;
 }
@@ -448,6 +457,7 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
       pp.n = n;
       pp.L = geo.L;
       pp.C = geo.C;
+      pp.threads = geo.threads;
       pp.a = geo.a;
       pp.tiling = (r & 1) ? 2 : 1;
       pp.count = G;
@@ -530,6 +540,7 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int Kb,
     pp.n = n;
     pp.L = geo.L;
     pp.C = geo.C;
+    pp.threads = geo.threads;
     pp.a = geo.a;
     pp.tiling = ((R - j) & 1) ? 2 : 1;
     pp.count = 1;
@@ -611,7 +622,7 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
   for (auto& kv : grid_by_n) {
     const int n = kv.first;
     const GridShape gs = P.grid_geo.at(n);
-    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax);
+    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads);
     const int G = gs.group;
     const std::vector<int>& ws = kv.second;
     const int kb_cap = P.basis_kb.count(n) ? P.basis_kb.at(n) : 0;
@@ -693,16 +704,19 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     gs.lmax = std::max(0, P.opt.tile_log);
     gs.group = std::max(0, P.opt.group);
     gs.lanes = std::min(std::max(0, P.opt.lanes), kMaxLanes);
-    if (!gs.lmax || !gs.group || !gs.lanes) {
+    gs.threads = P.opt.threads == 256 ? 256 : 0;
+    if (!gs.lmax || !gs.group || !gs.lanes || !P.opt.threads) {
+      GridShape want = gs;
+      want.threads = P.opt.threads;  // 0: tuned, else fixed
       GridShape t;
-      mqw_status s = tune_grid(ctx, P.precision, n, gs, &t);
+      mqw_status s = tune_grid(ctx, P.precision, n, want, &t);
       if (s != MQW_OK) return s;
       gs = t;
     }
     gs.group = std::min(std::min(gs.group, kMaxGroup), kv.second);
     const int ngroups = (kv.second + gs.group - 1) / gs.group;
     gs.lanes = std::max(1, std::min(gs.lanes, ngroups));
-    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax);
+    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads);
     P.grid_geo[n] = gs;
     lanes_max = std::max(lanes_max, gs.lanes);
     const size_t N = (size_t)1 << n;
@@ -1115,11 +1129,13 @@ mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,
   if (st != MQW_OK) return st;
   if (!out || (precision != MQW_FP32 && precision != MQW_FP64) || n < 6 || n > kMaxN)
     return fail(ctx, MQW_ERR_INVALID, "mqw_grid_shape_for: bad arguments");
-  GridShape gs;
-  st = tune_grid(ctx, precision, n, GridShape{0, 0, 0, 0.0}, &gs);
+  GridShape want, gs;
+  want.group = want.lanes = 0;  // nothing fixed
+  st = tune_grid(ctx, precision, n, want, &gs);
   if (st != MQW_OK) return st;
-  const PassGeomHost geo = pass_geom(precision, n, gs.lmax);
+  const PassGeomHost geo = pass_geom(precision, n, gs.lmax, gs.threads);
   out->tile_log = geo.L;
+  out->threads = geo.threads ? geo.threads : 512;
   out->cluster_log = geo.C;
   out->global_axes = geo.nu;
   out->group = gs.group;
@@ -1255,6 +1271,7 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
     pp.n = n;
     pp.L = geo.L;
     pp.C = geo.C;
+    pp.threads = geo.threads;
     pp.a = geo.a;
     pp.tiling = (r & 1) ? 2 : 1;
     pp.count = 1;

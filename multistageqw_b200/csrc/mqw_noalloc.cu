@@ -93,6 +93,7 @@ extern "C" mqw_status mqw_clenshaw_noalloc(int precision, int n, int K,
     pp.n = n;
     pp.L = geo.L;
     pp.C = geo.C;
+    pp.threads = geo.threads;
     pp.a = geo.a;
     pp.tiling = (r & 1) ? 2 : 1;
     pp.count = 1;

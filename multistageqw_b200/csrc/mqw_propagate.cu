@@ -377,11 +377,21 @@ __device__ __forceinline__ Pair<R> axis_sum(const Pair<R> (&v)[RP], int j,
   return acc;
 }
 
-template <int LT> struct PassShape {
+// CTA shape of a tile of 2^LT amplitudes with at most TB threads: each
+// thread owns RP pairs. Fewer threads own more pairs, so more tile axes are
+// register axes (free) and fewer go through shuffles or shared memory.
+template <int LT, int TB = kPassThreads> struct PassShape {
   static constexpr int kPairs = 1 << (LT - 1);
-  static constexpr int kThreads = kPairs < kPassThreads ? kPairs : kPassThreads;
+  static constexpr int kThreads = kPairs < TB ? kPairs : TB;
   static constexpr int kRP = kPairs / kThreads;
   static constexpr int kLogT = kThreads >= 512 ? 9 : kThreads >= 256 ? 8 : kThreads >= 128 ? 7 : kThreads >= 64 ? 6 : 5;
+  // With RP >= 8 a thread has the registers to keep P_r (the partial read by
+  // the finish) in registers; smaller RP stages it in shared memory.
+  static constexpr bool kStageP = kRP < 8;
+  template <typename R>
+  static constexpr size_t smem() {
+    return (size_t)kPairs * ((kStageP ? 3 : 2) * 4 * sizeof(R) + sizeof(float2));
+  }
 };
 
 // Two CTAs per SM in FP32 (64 registers); FP64 pairs need twice the
@@ -391,11 +401,12 @@ template <int LT> struct PassShape {
 // read from the other CTAs' exchange tiles, and every barrier that guards the
 // exchange tile is a cluster barrier. All CTAs of a cluster belong to the
 // same walk and term, so they take the same path through every barrier.
-template <typename R, int LT, int CL>
-__global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 1)
+template <typename R, int LT, int CL, int TB>
+__global__ void __launch_bounds__(PassShape<LT, TB>::kThreads, (sizeof(R) == 4 && CL == 0) ? 2 : 1)
     pass_kernel(PassParams p) {
-  using S = PassShape<LT>;
+  using S = PassShape<LT, TB>;
   constexpr int RP = S::kRP, LOGT = S::kLogT, T = S::kThreads;
+  constexpr bool kStageP = S::kStageP;
   constexpr int LL = LT + CL;  // tile bits of the tiling
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[32];
@@ -405,12 +416,22 @@ __global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 
   const int tid = threadIdx.x;
   R* sx = reinterpret_cast<R*>(smem_raw);  // exchange tile: 2^LT complex
   R* sp = sx + 4 * S::kPairs;              // staged P_r, [j][tid] pairs
-  R* ss = sp + 4 * S::kPairs;              // staged psi
+  R* ss = kStageP ? sp + 4 * S::kPairs : sp;  // staged psi
   float2* sd = reinterpret_cast<float2*>(ss + 4 * S::kPairs);  // staged D
   // Global amplitude index of register pair j: g0 + j * gstride (32-bit: n <= 30).
   // For a 1-D cluster the cluster rank is blockIdx.x mod 2^CL.
   const unsigned rank = CL > 0 ? (blockIdx.x & ((1u << CL) - 1u)) : 0u;
-  const unsigned tile = blockIdx.x >> CL;
+  const int nu = n - (2 * LL - a) > 0 ? n - (2 * LL - a) : 0;
+  // Launch order of the tiles: the tile bits of the nu axes read from global
+  // memory come first, so that the tiles whose amplitudes a tile reads are
+  // processed at about the same time and those reads hit L2. In T1 they are
+  // the lowest tile bits already; in T2 they are the top nu of the n - LL
+  // tile bits, rotated down here.
+  unsigned tile = blockIdx.x >> CL;
+  if (p.tiling == 2 && nu > 0) {
+    const int tb = n - LL;
+    tile = ((tile & ((1u << nu) - 1u)) << (tb - nu)) | (tile >> nu);
+  }
   const unsigned pos0 = (rank << LT) | (2u * tid);  // tile position of pair 0
   unsigned g0, gstride;
   if (p.tiling == 1) {
@@ -433,33 +454,48 @@ __global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 
   const int r = W.r, K = W.K;
   const bool first = r == K - 1;
   const bool uni = W.psi_uniform;
-  const int nu = n - (2 * LL - a) > 0 ? n - (2 * LL - a) : 0;
   // Finish axes (tile bits): T1 -> [a, min(L, n-L+a)), T2 -> [max(2L-n, a), L)
   // with L = LL; axes [LL, LL+nu) are in neither tiling and come from global
   // memory.
   const int fb0 = p.tiling == 1 ? a : max(2 * LL - n, a);
   const int fb1 = p.tiling == 1 ? min(LL, n - LL + a) : LL;
-  // Partners along the rank bits [LT, LL) that lie in [q0, q1), summed into acc.
-  auto cluster_sum = [&](Pair<R>& acc, int j, int q0, int q1) {
+  // Partners along the rank bits [LT, LL) that lie in [q0, q1): all of a
+  // pair's remote loads are issued together (before the local partner sums,
+  // which hide their latency) and added afterwards.
+  struct Remote {
+    Pair<R> v[CL > 0 ? CL : 1];
+  };
+  auto cluster_load = [&](int j, int q0, int q1) {
+    Remote rv;
     const unsigned off = (unsigned)(4 * sizeof(R)) * (unsigned)(tid | (j << LOGT));
 #pragma unroll
     for (int k = 0; k < CL; k++)
-      if (LT + k >= q0 && LT + k < q1) padd(acc, pld_cluster((const R*)nullptr, peer_sx[k] + off));
+      if (LT + k >= q0 && LT + k < q1) rv.v[k] = pld_cluster((const R*)nullptr, peer_sx[k] + off);
+    return rv;
+  };
+  auto cluster_add = [&](Pair<R>& acc, const Remote& rv, int q0, int q1) {
+#pragma unroll
+    for (int k = 0; k < CL; k++)
+      if (LT + k >= q0 && LT + k < q1) padd(acc, rv.v[k]);
   };
 
-  // Stage P_r, psi and D for this thread's own pairs.
+  // Stage P_r (unless it goes to registers), psi and D for this thread's
+  // own pairs.
 #pragma unroll
   for (int j = 0; j < RP; j++) {
     const unsigned gi = g0 + j * gstride;
     const int o = j * T + tid;
-    if (!first) cp_async_pair<R>(sp + 4 * o, part + 2 * (size_t)gi);
+    if (kStageP && !first) cp_async_pair<R>(sp + 4 * o, part + 2 * (size_t)gi);
     if (!uni) cp_async_pair<R>(ss + 4 * o, psi + 2 * (size_t)gi);
     cp_async8(sd + o, hp + gi);
   }
   Pair<R> va[RP];  // b_{r+1}
+  Pair<R> pv[kStageP ? 1 : RP];  // P_r when kept in registers
 #pragma unroll
-  for (int j = 0; j < RP; j++)
+  for (int j = 0; j < RP; j++) {
     va[j] = first ? pzero<R>() : pld(bin + 2 * (size_t)(g0 + j * gstride));
+    if constexpr (!kStageP) pv[j] = first ? pzero<R>() : pld(part + 2 * (size_t)(g0 + j * gstride));
+  }
   const double kap = W.kappa ? *W.kappa : 1.0;
   const R scale = (R)W.scale;
   const R gamma = (R)W.gamma;
@@ -482,8 +518,9 @@ __global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 
     cp_async_wait_all();
 #pragma unroll
     for (int j = 0; j < RP; j++) {
+      const Remote rv = cluster_load(j, fb0, fb1);
       Pair<R> accp = axis_sum<R, LT, LOGT, RP>(va, j, sx, fb0, fb1, tid);
-      cluster_sum(accp, j, fb0, fb1);
+      cluster_add(accp, rv, fb0, fb1);
       const unsigned gi = g0 + j * gstride;
       for (int u0 = 0; u0 < nu; u0 += 4) {
         Pair<R> gv[4];
@@ -495,7 +532,9 @@ __global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 
           if (u0 + u < nu) padd(accp, gv[u]);
       }
       const V4<R> acc = to4(accp);
-      const V4<R> pr = ld4<R>(sp + 4 * (j * T + tid));
+      V4<R> pr;
+      if constexpr (kStageP) pr = ld4<R>(sp + 4 * (j * T + tid));
+      else pr = to4(pv[kStageP ? 0 : j]);
       vb[j] = from4(V4<R>{fma(-ag, acc.x, pr.x), fma(-ag, acc.y, pr.y),
                           fma(-ag, acc.z, pr.z), fma(-ag, acc.w, pr.w)});
     }
@@ -524,8 +563,9 @@ __global__ void __launch_bounds__(PassShape<LT>::kThreads, sizeof(R) == 4 ? 2 : 
   const R cm = (R)((double)W.coef[rm] * kap);
 #pragma unroll
   for (int j = 0; j < RP; j++) {
+    const Remote rv = cluster_load(j, 0, LL);
     Pair<R> accp = axis_sum<R, LT, LOGT, RP>(vb, j, sx, 0, LT, tid);
-    cluster_sum(accp, j, 0, LL);
+    cluster_add(accp, rv, 0, LL);
     const V4<R> acc = to4(accp);
     const int o = j * T + tid;
     const V4<R> pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * o);
@@ -697,11 +737,11 @@ namespace {
 template <typename R, int LT, int CL>
 int cluster_fits() {
   using S = PassShape<LT>;
-  const size_t smem = (size_t)S::kPairs * (3 * 4 * sizeof(R) + sizeof(float2));
-  if (cudaFuncSetAttribute(pass_kernel<R, LT, CL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem) != cudaSuccess)
+  const size_t smem = S::template smem<R>();
+  if (cudaFuncSetAttribute(pass_kernel<R, LT, CL, kPassThreads>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return 0;
-  if (CL > 3 && cudaFuncSetAttribute(pass_kernel<R, LT, CL>,
+  if (CL > 3 && cudaFuncSetAttribute(pass_kernel<R, LT, CL, kPassThreads>,
                                      cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
     return 0;
   cudaLaunchConfig_t cfg = {};
@@ -716,7 +756,8 @@ int cluster_fits() {
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   int clusters = 0;
-  if (cudaOccupancyMaxActiveClusters(&clusters, pass_kernel<R, LT, CL>, &cfg) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveClusters(&clusters, pass_kernel<R, LT, CL, kPassThreads>, &cfg) !=
+      cudaSuccess) {
     (void)cudaGetLastError();
     return 0;
   }
@@ -738,7 +779,7 @@ int max_cluster_log() {
 }
 }  // namespace
 
-PassGeomHost pass_geom(int precision, int n, int lmax) {
+PassGeomHost pass_geom(int precision, int n, int lmax, int threads) {
   // Tile: 2^L amplitudes of b_{r+1} and 2^L of b_r in shared memory
   // (64 KB at L = 12 in FP32, 3 CTAs per SM). Rows of 2^a = 16 amplitudes
   // (128 bytes in FP32) keep T2 loads coalesced. L is chosen so the two
@@ -773,21 +814,23 @@ PassGeomHost pass_geom(int precision, int n, int lmax) {
     g.nu = n - (2 * (L + g.C) - g.a);
   }
   if (g.nu < 0) g.nu = 0;
+  // The 256-thread CTA exists for the widest single-CTA tile only.
+  g.threads = (threads == 256 && L == cap && g.C == 0) ? 256 : 0;
   return g;
 }
 
 namespace {
-template <typename R, int LT, int CL>
+template <typename R, int LT, int CL, int TB = kPassThreads>
 cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
-  using S = PassShape<LT>;
+  using S = PassShape<LT, TB>;
   static size_t configured = 0;
-  const size_t smem = (size_t)S::kPairs * (3 * 4 * sizeof(R) + sizeof(float2));
+  const size_t smem = S::template smem<R>();
   if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, LT, CL>,
+    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (CL > 3) {
-      e = cudaFuncSetAttribute(pass_kernel<R, LT, CL>,
+      e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB>,
                                cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
       if (e != cudaSuccess) return e;
     }
@@ -795,7 +838,7 @@ cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
   }
   const dim3 grid((unsigned)((size_t)1 << (p.n - LT)), p.count);
   if constexpr (CL == 0) {
-    pass_kernel<R, LT, 0><<<grid, S::kThreads, smem, stream>>>(p);
+    pass_kernel<R, LT, 0, TB><<<grid, S::kThreads, smem, stream>>>(p);
     return cudaGetLastError();
   } else {
     cudaLaunchConfig_t cfg = {};
@@ -810,7 +853,7 @@ cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, pass_kernel<R, LT, CL>, p);
+    return cudaLaunchKernelEx(&cfg, pass_kernel<R, LT, CL, TB>, p);
   }
 }
 
@@ -818,7 +861,9 @@ cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
 template <typename R, int LT>
 cudaError_t launch_pass_cluster(const PassParams& p, cudaStream_t stream) {
   switch (p.C) {
-    case 0: return launch_pass_lt<R, LT, 0>(p, stream);
+    case 0:
+      if (p.threads == 256) return launch_pass_lt<R, LT, 0, 256>(p, stream);
+      return launch_pass_lt<R, LT, 0>(p, stream);
     case 1: return launch_pass_lt<R, LT, 1>(p, stream);
     case 2: return launch_pass_lt<R, LT, 2>(p, stream);
     case 3: return launch_pass_lt<R, LT, 3>(p, stream);
@@ -852,7 +897,8 @@ cudaError_t launch_pass(int precision, const PassParams& p,
                         cudaStream_t stream) {
   if (p.n < 6 || p.n > kMaxN || p.L < 6 || p.L > p.n || p.a != 4 || p.C < 0 || p.C > 4 ||
       p.n - p.L < p.C || (p.tiling != 1 && p.tiling != 2) || p.count < 1 ||
-      p.count > kMaxGroup)
+      p.count > kMaxGroup || (p.threads != 0 && p.threads != 256 && p.threads != 512) ||
+      (p.threads == 256 && (p.C != 0 || p.L != (precision == 0 ? 12 : 11))))
     return cudaErrorInvalidValue;
   return precision == 0 ? launch_pass_t<float>(p, stream)
                         : launch_pass_t<double>(p, stream);

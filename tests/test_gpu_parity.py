@@ -229,3 +229,17 @@ def test_stage1_basis_matches_per_walk_recurrence(ctx, orc, n, m):
     assert np.abs(on["p"] - r64["p"]).max() <= 1e-5
     assert on["stats"]["term_amps"] == off["stats"]["term_amps"]
     assert on["stats"]["pass_amps"] < 0.95 * off["stats"]["pass_amps"]
+
+
+@pytest.mark.parametrize("n", [19, 20])
+def test_256_thread_tiles_match_512(ctx, orc, n):
+    """The widest FP32 tile with 256 threads (8 pairs per thread, P kept in
+    registers) against 512 threads (4 pairs, P staged in shared memory), and
+    both against FP64."""
+    raw = orc.sk_instances(n, 1, 1300 + n)
+    kw = dict(samples=6, graph=0, tile_log=12, group=2, lanes=1, resident_max_n=-1)
+    r256 = ctx.run_problems(n, 3, raw, precision="fp32", threads=256, **kw)
+    r512 = ctx.run_problems(n, 3, raw, precision="fp32", threads=512, **kw)
+    r64 = ctx.run_problems(n, 3, raw, precision="fp64", samples=6, graph=0)
+    assert abs(r256["p"][0] - r512["p"][0]) <= 1e-6
+    assert abs(r256["p"][0] - r64["p"][0]) <= 1e-5
