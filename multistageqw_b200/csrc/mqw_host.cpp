@@ -350,7 +350,11 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
   b.lmax = want.lmax ? want.lmax : def_l;
   b.group = want.group ? want.group : 1;
   b.lanes = want.lanes ? want.lanes : 1;
-  for (int l = def_l; l >= def_l - 1; l--) {
+  // Tile caps: the default widest tile, one narrower, and in FP32 the 2^13
+  // tile when the default leaves axes to global memory.
+  std::vector<int> caps = {def_l, def_l - 1};
+  if (precision == 0 && n > 2 * def_l - 4) caps.insert(caps.begin() + 1, def_l + 1);
+  for (int l : caps) {
     if (want.lmax && l != want.lmax) continue;
     for (int threads : {0, 256}) {
       if (want.threads && (want.threads == 256) != (threads == 256)) continue;
@@ -520,12 +524,14 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
 }
 
 // Builds the stage-1 basis w_0 .. w_{Kb-1} of the instance of walk w0 into
-// ctx->basis (slot 0 holds the passes' partial P, slot 1 + j holds w_j):
+// ctx->basis (slot 0 holds the passes' partial P, slot 1 + j holds w_j as a
+// complex vector; their real parts then go to the real basis that follows
+// the Kb_cap + 1 complex slots, where the recombination reads them):
 // Kb single-walk passes with c = [0, .., 0, 1] at an even top index R >= Kb,
 // so that b_R = psi0 and every later pass is b_r = 2 H~ b_{r+1} - b_{r+2};
 // the passes stop at r = R - Kb + 1 >= 1 (the r = 0 form is never used).
-mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int Kb,
-                       const PassGeomHost& geo, cudaStream_t stream) {
+mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int Kb, int kb_cap,
+                       const PassGeomHost& geo, void** real_out, cudaStream_t stream) {
   mqw_ctx* ctx = P.ctx;
   const int n = w0.n;
   const size_t N = (size_t)1 << n;
@@ -567,6 +573,10 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int Kb,
       P.stats.pass_amps += (double)N;
     }
   }
+  void* real = base + (size_t)(kb_cap + 1) * N * amp;
+  CK(launch_basis_real(slot(1), real, n, Kb, stream));
+  if (P.counting) P.stats.launches++;
+  *real_out = real;
   return MQW_OK;
 }
 
@@ -641,9 +651,10 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
           for (size_t k = b0; k < b1; k++)
             Kb = std::max(Kb, P.degree[P.walks[ws[k]].stage_desc_off]);
           if (Kb <= kb_cap) {
-            mqw_status s = issue_basis(P, w0, Kb, geo, stream);
+            void* real = nullptr;
+            mqw_status s = issue_basis(P, w0, Kb, kb_cap, geo, &real, stream);
             if (s != MQW_OK) return s;
-            basis = ctx->basis.as<char>() + ((size_t)1 << n) * (P.precision == 0 ? 8 : 16);
+            basis = real;
           }
         }
       }
@@ -785,7 +796,9 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     size_t basis_b = 0;
     int rmax = 0;
     for (auto& e : kb) {
-      const size_t bytes = (size_t)(e.second + 1) * ((size_t)1 << e.first) * 8;
+      // Kb + 1 complex slots (P and the basis) and the real basis.
+      const size_t bytes = (size_t)(e.second + 1) * ((size_t)1 << e.first) * 8 +
+                           (size_t)e.second * ((size_t)1 << e.first) * 4;
       if (e.second > kMaxBasis || bytes > budget) continue;
       P.basis_kb[e.first] = e.second;
       basis_b = std::max(basis_b, bytes);

@@ -167,11 +167,14 @@ struct CombineWalk {
   double* norm_part;   // per-block |out|^2 partials (2^(n-L) blocks)
 };
 struct CombineParams {
-  const void* basis;   // Kb vectors of 2^n interleaved complex amplitudes
+  const void* basis;   // Kb real FP32 vectors of 2^n amplitudes
   int n, L, Kb, count;
   CombineWalk walk[kMaxGroup];
 };
 constexpr int kMaxBasis = 1024;  // basis vectors (stage-1 degree bound)
+// Real parts of Kb contiguous complex FP32 vectors of 2^n amplitudes.
+cudaError_t launch_basis_real(const void* cplx, void* real, int n, int Kb,
+                              cudaStream_t stream);
 cudaError_t launch_combine(int precision, const CombineParams& p,
                            cudaStream_t stream);
 

@@ -401,8 +401,20 @@ template <int LT, int TB = kPassThreads> struct PassShape {
 // read from the other CTAs' exchange tiles, and every barrier that guards the
 // exchange tile is a cluster barrier. All CTAs of a cluster belong to the
 // same walk and term, so they take the same path through every barrier.
+// Register budget: 64 per thread when P is staged in shared memory (two
+// 512-thread CTAs per SM), 128 when it is kept in registers; FP64 and cluster
+// tiles take one CTA per SM.
+template <int LT, int TB, bool FP32, int CL>
+constexpr int pass_min_blocks() {
+  using S = PassShape<LT, TB>;
+  if (!FP32 || CL > 0) return 1;
+  const int per_cta = S::kThreads * (S::kStageP ? 64 : 128);
+  return 65536 / per_cta > 1 ? 65536 / per_cta : 1;
+}
+
 template <typename R, int LT, int CL, int TB>
-__global__ void __launch_bounds__(PassShape<LT, TB>::kThreads, (sizeof(R) == 4 && CL == 0) ? 2 : 1)
+__global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
+                                  pass_min_blocks<LT, TB, sizeof(R) == 4, CL>())
     pass_kernel(PassParams p) {
   using S = PassShape<LT, TB>;
   constexpr int RP = S::kRP, LOGT = S::kLogT, T = S::kThreads;
@@ -584,14 +596,27 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads, (sizeof(R) == 4 &
   if constexpr (CL > 0) cluster_barrier();
 }
 
-// Stage-1 recombination: block b covers amplitudes [b 2^L, (b+1) 2^L) of
-// every walk of the group, reads each basis vector once for all walks, and
-// leaves the block's |out|^2 in norm_part[b] (fixed order: deterministic).
-template <typename R>
+// The basis passes leave interleaved complex vectors with zero imaginary
+// parts; the recombination reads them as real vectors (half the bytes):
+// real[q] = amplitudes 4q .. 4q+3 of the contiguous complex basis.
+__global__ void basis_real_kernel(const float4* __restrict__ cplx, float4* __restrict__ real,
+                                  size_t quads) {
+  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < quads;
+       q += (size_t)gridDim.x * blockDim.x) {
+    const float4 a = cplx[2 * q], b = cplx[2 * q + 1];
+    real[q] = make_float4(a.x, a.z, b.x, b.z);
+  }
+}
+
+// Stage-1 recombination of G walks (FP32): block b covers amplitudes
+// [b 2^L, (b+1) 2^L), reads each real basis vector once for all G walks
+// (eight vectors in flight per thread), and leaves the block's |out|^2 in
+// norm_part[b] (fixed order: deterministic).
+template <int G>
 __global__ void __launch_bounds__(256) combine_kernel(CombineParams p) {
-  __shared__ float sd[kMaxGroup][kMaxBasis];
+  __shared__ float sd[G][kMaxBasis];
   __shared__ double s_red[32];
-  const int Kb = p.Kb, G = p.count;
+  const int Kb = p.Kb;
   for (int e = threadIdx.x; e < G * Kb; e += blockDim.x) {
     const int g = e / Kb, j = e % Kb;
     const CombineWalk& W = p.walk[g];
@@ -603,48 +628,54 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineParams p) {
   const size_t N = (size_t)1 << p.n;
   const size_t chunk = (size_t)1 << p.L;
   const size_t base = (size_t)blockIdx.x * chunk;
-  const R* basis = reinterpret_cast<const R*>(p.basis);
-  double nrm[kMaxGroup];
+  const float* __restrict__ basis = reinterpret_cast<const float*>(p.basis);
+  double nrm[G];
 #pragma unroll
-  for (int g = 0; g < kMaxGroup; g++) nrm[g] = 0.0;
-  // Two amplitudes per thread and step: one 16-byte (FP32) load per vector.
-  for (size_t i = base + 2 * threadIdx.x; i < base + chunk; i += 2 * blockDim.x) {
-    R re0[kMaxGroup], im0[kMaxGroup], re1[kMaxGroup], im1[kMaxGroup];
+  for (int g = 0; g < G; g++) nrm[g] = 0.0;
+  for (size_t i = base + 4 * threadIdx.x; i < base + chunk; i += 4 * blockDim.x) {
+    float re[G][4], im[G][4];
 #pragma unroll
-    for (int g = 0; g < kMaxGroup; g++) re0[g] = im0[g] = re1[g] = im1[g] = (R)0;
-    for (int j = 0; j < Kb; j++) {
-      const V4<R> w = ld4<R>(basis + 2 * ((size_t)j * N + i));  // (w[i], 0, w[i+1], 0)
-      if (j & 1) {
+    for (int g = 0; g < G; g++)
 #pragma unroll
-        for (int g = 0; g < kMaxGroup; g++)
-          if (g < G) {
-            im0[g] = fma((R)sd[g][j], w.x, im0[g]);
-            im1[g] = fma((R)sd[g][j], w.z, im1[g]);
-          }
-      } else {
+      for (int k = 0; k < 4; k++) re[g][k] = im[g][k] = 0.0f;
+    auto accumulate = [&](const float4& w, int j, bool odd) {
 #pragma unroll
-        for (int g = 0; g < kMaxGroup; g++)
-          if (g < G) {
-            re0[g] = fma((R)sd[g][j], w.x, re0[g]);
-            re1[g] = fma((R)sd[g][j], w.z, re1[g]);
-          }
+      for (int g = 0; g < G; g++) {
+        const float d = sd[g][j];
+        float* acc = odd ? im[g] : re[g];
+        acc[0] = fmaf(d, w.x, acc[0]);
+        acc[1] = fmaf(d, w.y, acc[1]);
+        acc[2] = fmaf(d, w.z, acc[2]);
+        acc[3] = fmaf(d, w.w, acc[3]);
       }
+    };
+    int j = 0;
+    for (; j + 8 <= Kb; j += 8) {
+      float4 w[8];
+#pragma unroll
+      for (int u = 0; u < 8; u++)
+        w[u] = __ldg(reinterpret_cast<const float4*>(basis + (size_t)(j + u) * N + i));
+#pragma unroll
+      for (int u = 0; u < 8; u++) accumulate(w[u], j + u, u & 1);  // j is even
     }
+    for (; j < Kb; j++)
+      accumulate(__ldg(reinterpret_cast<const float4*>(basis + (size_t)j * N + i)), j, j & 1);
 #pragma unroll
-    for (int g = 0; g < kMaxGroup; g++)
-      if (g < G) {
-        st4<R>(reinterpret_cast<R*>(p.walk[g].out) + 2 * i, V4<R>{re0[g], im0[g], re1[g], im1[g]});
-        nrm[g] += (double)re0[g] * re0[g] + (double)im0[g] * im0[g] +
-                  (double)re1[g] * re1[g] + (double)im1[g] * im1[g];
-      }
+    for (int g = 0; g < G; g++) {
+      float4* out = reinterpret_cast<float4*>(reinterpret_cast<float*>(p.walk[g].out) + 2 * i);
+      out[0] = make_float4(re[g][0], im[g][0], re[g][1], im[g][1]);
+      out[1] = make_float4(re[g][2], im[g][2], re[g][3], im[g][3]);
+#pragma unroll
+      for (int k = 0; k < 4; k++)
+        nrm[g] += (double)re[g][k] * re[g][k] + (double)im[g][k] * im[g][k];
+    }
   }
 #pragma unroll
-  for (int g = 0; g < kMaxGroup; g++)
-    if (g < G) {  // uniform over the block
-      const double sum = block_sum<R>(nrm[g], s_red);
-      if (threadIdx.x == 0) p.walk[g].norm_part[blockIdx.x] = sum;
-      __syncthreads();  // s_red is reused by the next walk's sum
-    }
+  for (int g = 0; g < G; g++) {
+    const double sum = block_sum<float>(nrm[g], s_red);
+    if (threadIdx.x == 0) p.walk[g].norm_part[blockIdx.x] = sum;
+    __syncthreads();  // s_red is reused by the next walk's sum
+  }
 }
 
 template <typename R>
@@ -794,8 +825,12 @@ PassGeomHost pass_geom(int precision, int n, int lmax, int threads) {
   int Lmax = precision == 0 ? 12 : 11;
   if (env >= 6 && env <= 13) Lmax = env;
   if (lmax >= 6 && lmax <= 13) Lmax = lmax;
-  const int cap = precision == 0 ? 12 : 11;  // compiled tile sizes
-  if (Lmax > cap) Lmax = cap;
+  // Compiled tile sizes: up to 2^13 in FP32 (the 2^13 tile is one 512-thread
+  // CTA per SM with 8 pairs per thread), 2^11 in FP64. Clusters and the
+  // 256-thread shape exist at the default widest tile `cap`.
+  const int top = precision == 0 ? 13 : 11;
+  const int cap = precision == 0 ? 12 : 11;
+  if (Lmax > top) Lmax = top;
   // Threads own pairs along the top tile axes, lanes cover tile axes 1..5,
   // so a tile has at least 6 axes (n >= 6 on the grid path).
   PassGeomHost g;
@@ -876,6 +911,7 @@ template <typename R>
 cudaError_t launch_pass_t(const PassParams& p, cudaStream_t stream) {
   constexpr int cap = sizeof(R) == 4 ? 12 : 11;
   if (p.C != 0 && p.L != cap) return cudaErrorInvalidValue;
+  if (p.threads == 256 && p.L != cap) return cudaErrorInvalidValue;
   switch (p.L) {
     case 6: return launch_pass_lt<R, 6, 0>(p, stream);
     case 7: return launch_pass_lt<R, 7, 0>(p, stream);
@@ -888,6 +924,12 @@ cudaError_t launch_pass_t(const PassParams& p, cudaStream_t stream) {
     case 12:
       if constexpr (sizeof(R) == 4) return launch_pass_cluster<R, 12>(p, stream);
       return cudaErrorInvalidValue;  // FP64 tiles stop at 2^11
+    case 13:
+      if constexpr (sizeof(R) == 4) {
+        if (p.C != 0 || p.threads == 256) return cudaErrorInvalidValue;
+        return launch_pass_lt<R, 13, 0>(p, stream);
+      }
+      return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;
   }
 }
@@ -904,20 +946,37 @@ cudaError_t launch_pass(int precision, const PassParams& p,
                         : launch_pass_t<double>(p, stream);
 }
 
+cudaError_t launch_basis_real(const void* cplx, void* real, int n, int Kb,
+                              cudaStream_t stream) {
+  if (n < 2 || n > kMaxN || Kb < 1 || Kb > kMaxBasis || !cplx || !real) return cudaErrorInvalidValue;
+  const size_t quads = ((size_t)Kb << n) / 4;
+  const size_t want = (quads + 255) / 256;
+  const unsigned blocks = (unsigned)(want < 8192 ? want : 8192);
+  basis_real_kernel<<<blocks, 256, 0, stream>>>(reinterpret_cast<const float4*>(cplx),
+                                               reinterpret_cast<float4*>(real), quads);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_combine(int precision, const CombineParams& p,
                            cudaStream_t stream) {
-  if (p.n < 6 || p.n > kMaxN || p.L < 6 || p.L > p.n || p.Kb < 1 || p.Kb > kMaxBasis ||
-      p.count < 1 || p.count > kMaxGroup || !p.basis)
+  if (precision != 0 || p.n < 6 || p.n > kMaxN || p.L < 6 || p.L > p.n || p.Kb < 1 ||
+      p.Kb > kMaxBasis || p.count < 1 || p.count > kMaxGroup || !p.basis)
     return cudaErrorInvalidValue;
   for (int g = 0; g < p.count; g++)
     if (p.walk[g].K < 1 || p.walk[g].K > p.Kb || !p.walk[g].coef || !p.walk[g].out ||
         !p.walk[g].norm_part)
       return cudaErrorInvalidValue;
   const unsigned blocks = (unsigned)((size_t)1 << (p.n - p.L));
-  if (precision == 0)
-    combine_kernel<float><<<blocks, 256, 0, stream>>>(p);
-  else
-    combine_kernel<double><<<blocks, 256, 0, stream>>>(p);
+  switch (p.count) {
+    case 1: combine_kernel<1><<<blocks, 256, 0, stream>>>(p); break;
+    case 2: combine_kernel<2><<<blocks, 256, 0, stream>>>(p); break;
+    case 3: combine_kernel<3><<<blocks, 256, 0, stream>>>(p); break;
+    case 4: combine_kernel<4><<<blocks, 256, 0, stream>>>(p); break;
+    case 5: combine_kernel<5><<<blocks, 256, 0, stream>>>(p); break;
+    case 6: combine_kernel<6><<<blocks, 256, 0, stream>>>(p); break;
+    case 7: combine_kernel<7><<<blocks, 256, 0, stream>>>(p); break;
+    default: combine_kernel<8><<<blocks, 256, 0, stream>>>(p); break;
+  }
   return cudaGetLastError();
 }
 

@@ -243,3 +243,16 @@ def test_256_thread_tiles_match_512(ctx, orc, n):
     r64 = ctx.run_problems(n, 3, raw, precision="fp64", samples=6, graph=0)
     assert abs(r256["p"][0] - r512["p"][0]) <= 1e-6
     assert abs(r256["p"][0] - r64["p"][0]) <= 1e-5
+
+
+@pytest.mark.parametrize("n", [21, 24])
+def test_wide_tile_2_13_matches(ctx, orc, n):
+    """The 2^13-amplitude FP32 tile (8 pairs per thread, one CTA per SM)
+    against the default tile and FP64."""
+    raw = orc.sk_instances(n, 1, 1700 + n)
+    kw = dict(samples=2, graph=0, group=1, lanes=1)
+    r13 = ctx.run_problems(n, 2, raw, precision="fp32", tile_log=13, **kw)
+    r12 = ctx.run_problems(n, 2, raw, precision="fp32", tile_log=12, **kw)
+    r64 = ctx.run_problems(n, 2, raw, precision="fp64", samples=2, graph=0)
+    assert abs(r13["p"][0] - r12["p"][0]) <= 1e-6
+    assert abs(r13["p"][0] - r64["p"][0]) <= 1e-5
