@@ -74,6 +74,8 @@ typedef struct mqw_options {
                       own stream (1..4), 0 = autotuned */
   int threads;     /* CTA threads of the grid path at its widest tile: 512
                       or 256 (twice the amplitudes per thread), 0 = autotuned */
+  int lane_smem;   /* grid-path partners along the warp-lane axes: 1 from
+                      shared memory, -1 by warp shuffles, 0 = autotuned */
   int stage1_basis; /* 1 (default): FP32 walks of an instance share one
                        Chebyshev basis for their first stage (built once,
                        recombined per walk); 0: every walk runs its own
@@ -238,6 +240,7 @@ void mqw_plan_destroy(mqw_plan* plan);
 typedef struct mqw_grid_shape {
   int tile_log, cluster_log, global_axes, group, lanes;
   int threads;     /* threads per CTA */
+  int lane_smem;   /* 1: lane-axis partners from shared memory */
   double us_per_walk_pass;
 } mqw_grid_shape;
 mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,

@@ -57,6 +57,7 @@ class Options(ctypes.Structure):
         ("graph", ctypes.c_int),
         ("lanes", ctypes.c_int),
         ("threads", ctypes.c_int),
+        ("lane_smem", ctypes.c_int),
         ("stage1_basis", ctypes.c_int),
     ]
 
@@ -79,6 +80,7 @@ class GridShape(ctypes.Structure):
         ("group", ctypes.c_int),
         ("lanes", ctypes.c_int),
         ("threads", ctypes.c_int),
+        ("lane_smem", ctypes.c_int),
         ("us_per_walk_pass", ctypes.c_double),
     ]
 
@@ -175,7 +177,8 @@ def _ptr(a, ct):
 
 
 def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_max_n=0,
-          stage_scale=None, tile_log=0, graph=1, lanes=0, threads=0, stage1_basis=1):
+          stage_scale=None, tile_log=0, graph=1, lanes=0, threads=0, lane_smem=0,
+          stage1_basis=1):
     o = Options()
     lib().mqw_default_options(ctypes.byref(o))
     o.precision = {"fp32": FP32, "fp64": FP64, FP32: FP32, FP64: FP64}[precision]
@@ -187,6 +190,7 @@ def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_ma
     o.graph = int(graph)
     o.lanes = int(lanes)
     o.threads = int(threads)
+    o.lane_smem = int(lane_smem)
     o.stage1_basis = int(stage1_basis)
     keep = None
     if stage_scale is not None:

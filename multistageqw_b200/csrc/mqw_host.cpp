@@ -69,6 +69,7 @@ struct DevMem {
 struct GridShape {
   int lmax = 0, group = 1, lanes = 1;
   int threads = 0;  // CTA threads at the widest tile (0: 512)
+  int lane_smem = 0;  // lane axes: 1 shared memory, -1 shuffles, 0 (want): any
   double us = 0.0;  // timed microseconds per walk-pass (0: not timed)
 };
 constexpr int kMaxLanes = 4;
@@ -170,6 +171,7 @@ void default_opts(mqw_options* o) {
   o->graph = 1;
   o->lanes = 0;
   o->threads = 0;
+  o->lane_smem = 0;
   o->stage1_basis = 1;
 }
 
@@ -261,8 +263,9 @@ int default_group(int precision, const PassGeomHost& geo, int n) {
 // tilings) over G zero-filled walks on each of `lanes` concurrent streams.
 // Returns microseconds per walk-pass.
 mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
-                            int G, int lanes, int threads, double* us_per_walk) {
-  const PassGeomHost geo = pass_geom(precision, n, lmax, threads);
+                            int G, int lanes, int threads, int lane_smem,
+                            double* us_per_walk) {
+  const PassGeomHost geo = pass_geom(precision, n, lmax, threads, lane_smem);
   const size_t N = (size_t)1 << n;
   const size_t amp = precision == 0 ? 8 : 16;
   const int slots = walk_slots(geo);
@@ -282,6 +285,7 @@ mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
     pp.L = geo.L;
     pp.C = geo.C;
     pp.threads = geo.threads;
+    pp.lane_smem = geo.lane_smem;
     pp.a = geo.a;
     pp.tiling = (r & 1) ? 2 : 1;
     pp.count = G;
@@ -336,7 +340,8 @@ mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
 mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridShape* out) {
   const auto key = std::make_pair(precision, n);
   auto it = ctx->tuned.find(key);
-  const bool fixed_none = !want.lmax && !want.group && !want.lanes && !want.threads;
+  const bool fixed_none =
+      !want.lmax && !want.group && !want.lanes && !want.threads && !want.lane_smem;
   if (it != ctx->tuned.end() && fixed_none) {
     *out = it->second;
     return MQW_OK;
@@ -356,22 +361,25 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
   if (precision == 0 && n > 2 * def_l - 4) caps.insert(caps.begin() + 1, def_l + 1);
   for (int l : caps) {
     if (want.lmax && l != want.lmax) continue;
-    for (int threads : {0, 256}) {
+    for (int threads : {0, 256})
+    for (int ls : {0, 1}) {
       if (want.threads && (want.threads == 256) != (threads == 256)) continue;
-      const PassGeomHost geo = pass_geom(precision, n, l, threads);
-      if (geo.threads != threads) continue;  // no 256-thread shape here
+      if (want.lane_smem && (want.lane_smem > 0) != (ls == 1)) continue;
+      const PassGeomHost geo = pass_geom(precision, n, l, threads, ls);
+      if (geo.threads != threads || geo.lane_smem != ls) continue;  // shape not built here
       const int g0 = default_group(precision, geo, n);
-      for (int g : {1, 2, 3, 4, g0}) {
+      for (int g : {1, 2, 4, g0}) {
         if (want.group && g != want.group) continue;
+        if (g == g0 && g0 <= 4 && g0 != 3) continue;  // already a candidate
         for (int lanes : {1, 2}) {
           if (want.lanes && lanes != want.lanes) continue;
           if (g > kMaxGroup || (size_t)g * lanes * walk_bytes(precision, geo, n) > budget) continue;
           double us = 0.0;
-          mqw_status s = time_grid_config(ctx, precision, n, l, g, lanes, threads, &us);
+          mqw_status s = time_grid_config(ctx, precision, n, l, g, lanes, threads, ls, &us);
           if (s != MQW_OK) return s;
           if (getenv("MQW_TUNE_LOG"))
-            fprintf(stderr, "mqw tune: precision %d n %d tile %d cluster %d global %d threads %d group %d lanes %d: %.3f us/walk-pass\n",
-                    precision, n, geo.L, geo.C, geo.nu, threads ? threads : 512, g, lanes, us);
+            fprintf(stderr, "mqw tune: precision %d n %d tile %d cluster %d global %d threads %d lane_smem %d group %d lanes %d: %.3f us/walk-pass\n",
+                    precision, n, geo.L, geo.C, geo.nu, threads ? threads : 512, ls, g, lanes, us);
           // Prefer the earlier candidate (larger tile, fewer walks in flight)
           // unless a later one is clearly faster.
           if (us < best * 0.98) {
@@ -380,6 +388,7 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
             b.group = g;
             b.lanes = lanes;
             b.threads = threads;
+            b.lane_smem = ls ? 1 : -1;
             b.us = us;
           }
         }
@@ -462,6 +471,7 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
       pp.L = geo.L;
       pp.C = geo.C;
       pp.threads = geo.threads;
+      pp.lane_smem = geo.lane_smem;
       pp.a = geo.a;
       pp.tiling = (r & 1) ? 2 : 1;
       pp.count = G;
@@ -547,6 +557,7 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int Kb, int kb_cap,
     pp.L = geo.L;
     pp.C = geo.C;
     pp.threads = geo.threads;
+    pp.lane_smem = geo.lane_smem;
     pp.a = geo.a;
     pp.tiling = ((R - j) & 1) ? 2 : 1;
     pp.count = 1;
@@ -632,7 +643,7 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
   for (auto& kv : grid_by_n) {
     const int n = kv.first;
     const GridShape gs = P.grid_geo.at(n);
-    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads);
+    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0);
     const int G = gs.group;
     const std::vector<int>& ws = kv.second;
     const int kb_cap = P.basis_kb.count(n) ? P.basis_kb.at(n) : 0;
@@ -716,7 +727,8 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     gs.group = std::max(0, P.opt.group);
     gs.lanes = std::min(std::max(0, P.opt.lanes), kMaxLanes);
     gs.threads = P.opt.threads == 256 ? 256 : 0;
-    if (!gs.lmax || !gs.group || !gs.lanes || !P.opt.threads) {
+    gs.lane_smem = P.opt.lane_smem;
+    if (!gs.lmax || !gs.group || !gs.lanes || !P.opt.threads || !P.opt.lane_smem) {
       GridShape want = gs;
       want.threads = P.opt.threads;  // 0: tuned, else fixed
       GridShape t;
@@ -727,7 +739,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     gs.group = std::min(std::min(gs.group, kMaxGroup), kv.second);
     const int ngroups = (kv.second + gs.group - 1) / gs.group;
     gs.lanes = std::max(1, std::min(gs.lanes, ngroups));
-    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads);
+    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0);
     P.grid_geo[n] = gs;
     lanes_max = std::max(lanes_max, gs.lanes);
     const size_t N = (size_t)1 << n;
@@ -1146,9 +1158,10 @@ mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,
   want.group = want.lanes = 0;  // nothing fixed
   st = tune_grid(ctx, precision, n, want, &gs);
   if (st != MQW_OK) return st;
-  const PassGeomHost geo = pass_geom(precision, n, gs.lmax, gs.threads);
+  const PassGeomHost geo = pass_geom(precision, n, gs.lmax, gs.threads, gs.lane_smem > 0);
   out->tile_log = geo.L;
   out->threads = geo.threads ? geo.threads : 512;
+  out->lane_smem = geo.lane_smem;
   out->cluster_log = geo.C;
   out->global_axes = geo.nu;
   out->group = gs.group;
@@ -1285,6 +1298,7 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
     pp.L = geo.L;
     pp.C = geo.C;
     pp.threads = geo.threads;
+    pp.lane_smem = geo.lane_smem;
     pp.a = geo.a;
     pp.tiling = (r & 1) ? 2 : 1;
     pp.count = 1;

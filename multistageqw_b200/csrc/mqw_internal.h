@@ -134,6 +134,8 @@ struct PassParams {
   int C;               // cluster log: a tile spans 2^C CTAs (0 = one CTA)
   int threads;         // CTA threads at the widest single-CTA tile: 512 (0)
                        // or 256 (more pairs per thread)
+  int lane_smem;       // 1: lane-axis partners from shared memory (FP32,
+                       // tiles of 2^12 and 2^13), 0: warp shuffles
   int tiling;          // 1 or 2
   int count;
   PassWalk walk[kMaxGroup];
@@ -142,10 +144,12 @@ struct PassGeomHost {
   int L, a, nu;        // CTA tile log, row log, axes read from global memory
   int C;               // cluster log (tile of 2^(L+C) amplitudes over 2^C CTAs)
   int threads;         // CTA threads (0: default 512)
+  int lane_smem;       // lane axes through shared memory instead of shuffles
 };
 // Geometry for n; lmax > 0 caps the tile (log2 amplitudes), else the
 // precision's default cap (or MQW_PASS_TILE_LOG) applies.
-PassGeomHost pass_geom(int precision, int n, int lmax = 0, int threads = 0);
+PassGeomHost pass_geom(int precision, int n, int lmax = 0, int threads = 0,
+                        int lane_smem = 0);
 cudaError_t launch_pass(int precision, const PassParams& p,
                         cudaStream_t stream);
 

@@ -356,16 +356,22 @@ __device__ __forceinline__ void tile_barrier() {
 // (exchange tile sx in shared memory), and bits above index the thread's own
 // registers v[]. Every loop is unrolled at compile time; [q0, q1) only
 // predicates whole axes.
-template <typename R, int LT, int LOGT, int RP>
+// LS: the lane axes are read from the exchange tile too (one 16-byte shared
+// load per partner pair instead of four 32-bit shuffles: the same bytes
+// through the shared-memory pipe, a quarter of the instructions).
+template <typename R, int LT, int LOGT, int RP, bool LS = false>
 __device__ __forceinline__ Pair<R> axis_sum(const Pair<R> (&v)[RP], int j,
                                            const R* sx, int q0, int q1,
                                            int tid) {
   Pair<R> acc = pzero<R>();
   if (q0 <= 0) padd(acc, pswap<R>(v[j]));
+  const int pp = tid | (j << LOGT);
 #pragma unroll
   for (int q = 1; q <= 5 && q < LT; q++)
-    if (q >= q0 && q < q1) padd(acc, pshfl(v[j], 1 << (q - 1)));
-  const int pp = tid | (j << LOGT);
+    if (q >= q0 && q < q1) {
+      if constexpr (LS) padd(acc, pld(sx + 4 * (pp ^ (1 << (q - 1)))));
+      else padd(acc, pshfl(v[j], 1 << (q - 1)));
+    }
 #pragma unroll
   for (int q = 6; q <= LOGT && q < LT; q++)
     if (q >= q0 && q < q1) padd(acc, pld(sx + 4 * (pp ^ (1 << (q - 1)))));
@@ -412,7 +418,7 @@ constexpr int pass_min_blocks() {
   return 65536 / per_cta > 1 ? 65536 / per_cta : 1;
 }
 
-template <typename R, int LT, int CL, int TB>
+template <typename R, int LT, int CL, int TB, bool LS = false>
 __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
                                   pass_min_blocks<LT, TB, sizeof(R) == 4, CL>())
     pass_kernel(PassParams p) {
@@ -531,7 +537,7 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
 #pragma unroll
     for (int j = 0; j < RP; j++) {
       const Remote rv = cluster_load(j, fb0, fb1);
-      Pair<R> accp = axis_sum<R, LT, LOGT, RP>(va, j, sx, fb0, fb1, tid);
+      Pair<R> accp = axis_sum<R, LT, LOGT, RP, LS>(va, j, sx, fb0, fb1, tid);
       cluster_add(accp, rv, fb0, fb1);
       const unsigned gi = g0 + j * gstride;
       for (int u0 = 0; u0 < nu; u0 += 4) {
@@ -576,7 +582,7 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
 #pragma unroll
   for (int j = 0; j < RP; j++) {
     const Remote rv = cluster_load(j, 0, LL);
-    Pair<R> accp = axis_sum<R, LT, LOGT, RP>(vb, j, sx, 0, LT, tid);
+    Pair<R> accp = axis_sum<R, LT, LOGT, RP, LS>(vb, j, sx, 0, LT, tid);
     cluster_add(accp, rv, 0, LL);
     const V4<R> acc = to4(accp);
     const int o = j * T + tid;
@@ -810,7 +816,7 @@ int max_cluster_log() {
 }
 }  // namespace
 
-PassGeomHost pass_geom(int precision, int n, int lmax, int threads) {
+PassGeomHost pass_geom(int precision, int n, int lmax, int threads, int lane_smem) {
   // Tile: 2^L amplitudes of b_{r+1} and 2^L of b_r in shared memory
   // (64 KB at L = 12 in FP32, 3 CTAs per SM). Rows of 2^a = 16 amplitudes
   // (128 bytes in FP32) keep T2 loads coalesced. L is chosen so the two
@@ -851,21 +857,23 @@ PassGeomHost pass_geom(int precision, int n, int lmax, int threads) {
   if (g.nu < 0) g.nu = 0;
   // The 256-thread CTA exists for the widest single-CTA tile only.
   g.threads = (threads == 256 && L == cap && g.C == 0) ? 256 : 0;
+  // Lane axes through shared memory: FP32 single-CTA tiles of 2^12 or 2^13.
+  g.lane_smem = (lane_smem && precision == 0 && g.C == 0 && L >= cap) ? 1 : 0;
   return g;
 }
 
 namespace {
-template <typename R, int LT, int CL, int TB = kPassThreads>
+template <typename R, int LT, int CL, int TB = kPassThreads, bool LS = false>
 cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
   using S = PassShape<LT, TB>;
   static size_t configured = 0;
   const size_t smem = S::template smem<R>();
   if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB>,
+    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB, LS>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (CL > 3) {
-      e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB>,
+      e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB, LS>,
                                cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
       if (e != cudaSuccess) return e;
     }
@@ -873,7 +881,7 @@ cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
   }
   const dim3 grid((unsigned)((size_t)1 << (p.n - LT)), p.count);
   if constexpr (CL == 0) {
-    pass_kernel<R, LT, 0, TB><<<grid, S::kThreads, smem, stream>>>(p);
+    pass_kernel<R, LT, 0, TB, LS><<<grid, S::kThreads, smem, stream>>>(p);
     return cudaGetLastError();
   } else {
     cudaLaunchConfig_t cfg = {};
@@ -888,7 +896,7 @@ cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, pass_kernel<R, LT, CL, TB>, p);
+    return cudaLaunchKernelEx(&cfg, pass_kernel<R, LT, CL, TB, LS>, p);
   }
 }
 
@@ -897,6 +905,12 @@ template <typename R, int LT>
 cudaError_t launch_pass_cluster(const PassParams& p, cudaStream_t stream) {
   switch (p.C) {
     case 0:
+      if constexpr (sizeof(R) == 4) {
+        if (p.lane_smem) {
+          if (p.threads == 256) return launch_pass_lt<R, LT, 0, 256, true>(p, stream);
+          return launch_pass_lt<R, LT, 0, kPassThreads, true>(p, stream);
+        }
+      }
       if (p.threads == 256) return launch_pass_lt<R, LT, 0, 256>(p, stream);
       return launch_pass_lt<R, LT, 0>(p, stream);
     case 1: return launch_pass_lt<R, LT, 1>(p, stream);
@@ -912,6 +926,7 @@ cudaError_t launch_pass_t(const PassParams& p, cudaStream_t stream) {
   constexpr int cap = sizeof(R) == 4 ? 12 : 11;
   if (p.C != 0 && p.L != cap) return cudaErrorInvalidValue;
   if (p.threads == 256 && p.L != cap) return cudaErrorInvalidValue;
+  if (p.lane_smem && (sizeof(R) != 4 || p.C != 0 || p.L < cap)) return cudaErrorInvalidValue;
   switch (p.L) {
     case 6: return launch_pass_lt<R, 6, 0>(p, stream);
     case 7: return launch_pass_lt<R, 7, 0>(p, stream);
@@ -927,6 +942,7 @@ cudaError_t launch_pass_t(const PassParams& p, cudaStream_t stream) {
     case 13:
       if constexpr (sizeof(R) == 4) {
         if (p.C != 0 || p.threads == 256) return cudaErrorInvalidValue;
+        if (p.lane_smem) return launch_pass_lt<R, 13, 0, kPassThreads, true>(p, stream);
         return launch_pass_lt<R, 13, 0>(p, stream);
       }
       return cudaErrorInvalidValue;

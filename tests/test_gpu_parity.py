@@ -232,12 +232,15 @@ def test_stage1_basis_matches_per_walk_recurrence(ctx, orc, n, m):
 
 
 @pytest.mark.parametrize("n", [19, 20])
-def test_256_thread_tiles_match_512(ctx, orc, n):
+@pytest.mark.parametrize("lane_smem", [-1, 1])
+def test_256_thread_tiles_match_512(ctx, orc, n, lane_smem):
     """The widest FP32 tile with 256 threads (8 pairs per thread, P kept in
-    registers) against 512 threads (4 pairs, P staged in shared memory), and
-    both against FP64."""
+    registers) against 512 threads (4 pairs, P staged in shared memory), with
+    the lane axes by shuffles (-1) or through shared memory (1), and all
+    against FP64."""
     raw = orc.sk_instances(n, 1, 1300 + n)
-    kw = dict(samples=6, graph=0, tile_log=12, group=2, lanes=1, resident_max_n=-1)
+    kw = dict(samples=6, graph=0, tile_log=12, group=2, lanes=1, resident_max_n=-1,
+              lane_smem=lane_smem)
     r256 = ctx.run_problems(n, 3, raw, precision="fp32", threads=256, **kw)
     r512 = ctx.run_problems(n, 3, raw, precision="fp32", threads=512, **kw)
     r64 = ctx.run_problems(n, 3, raw, precision="fp64", samples=6, graph=0)
@@ -252,6 +255,8 @@ def test_wide_tile_2_13_matches(ctx, orc, n):
     raw = orc.sk_instances(n, 1, 1700 + n)
     kw = dict(samples=2, graph=0, group=1, lanes=1)
     r13 = ctx.run_problems(n, 2, raw, precision="fp32", tile_log=13, **kw)
+    r13s = ctx.run_problems(n, 2, raw, precision="fp32", tile_log=13, lane_smem=1, **kw)
+    assert abs(r13s["p"][0] - r13["p"][0]) <= 1e-6
     r12 = ctx.run_problems(n, 2, raw, precision="fp32", tile_log=12, **kw)
     r64 = ctx.run_problems(n, 2, raw, precision="fp64", samples=2, graph=0)
     assert abs(r13["p"][0] - r12["p"][0]) <= 1e-6
