@@ -44,9 +44,12 @@ METRIC = ("instances/s at n=20,m=4 (|ΔP|≤1e-5 vs FP64); "
           "mean P_gs learned vs heuristic")
 BYTES_PER_TERM_AMP = {"fp32": 36, "fp64": 72}  # algorithmic, see DESIGN.md
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
-# DRAM bytes per term·amp of pass_kernel from one ncu capture of this
-# workload (profiles/pass_kernel_sk_n20_m4.md); absent until captured.
-DRAM_BYTES_PER_TERM_AMP = {}
+# DRAM bytes (read + write) per term·amp of one pass_kernel launch from an
+# ncu capture of the workload (cold caches: ncu flushes them between
+# replays), keyed by config.workload: profiles/pass_kernel_sk_n20_m4.md
+# (29.40 MB per 2^20-amplitude launch) and profiles/pass_kernel_sk_n24_global.md
+# (469.8 + 233.0 MB per 2^24-amplitude launch).
+DRAM_BYTES_PER_TERM_AMP = {"sk_n20_m4": 29.40e6 / 2**20, "sk_n24_m4": 702.8e6 / 2**24}
 # Host memory the CPU legs may use at once (all worker processes together).
 CPU_MEM_BUDGET = 24 << 30
 
@@ -452,7 +455,7 @@ def main():
     achieved = BYTES_PER_TERM_AMP[a.precision] * pass_amps / (kms / 1000.0) / 1e9 if kms > 0 else None
     peak = pk["hbm_gbs"]
     per_launch_amps = pass_amps / max(1, term_launches)
-    dram = DRAM_BYTES_PER_TERM_AMP.get(a.workload)
+    dram = DRAM_BYTES_PER_TERM_AMP.get(desc["workload"])
     roofline = {
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak if achieved else None,

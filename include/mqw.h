@@ -161,6 +161,14 @@ mqw_status mqw_cheb_coeffs_host(int count, const double* s, double tol,
 mqw_status mqw_build_diag(mqw_ctx* ctx, int n, const double* raw, float* hp,
                           double* energies, mqw_diag_info* info);
 
+/* Raw moments mean(H_P^k), k = 1..4, of the shifted float diagonal (the
+ * H_P of MultiQW.cpp:361), reduced on the GPU in FP64 in a fixed order; the
+ * skewness and kurtosis that the reference's comment at MultiQW.cpp:379-383
+ * considers for a higher-moment heuristic are M3/M2^1.5 and M4/M2^2. info
+ * (nullable) receives the diagonal's spectral data as in mqw_build_diag. */
+mqw_status mqw_diag_moments(mqw_ctx* ctx, int n, const double* raw,
+                            double* moments, mqw_diag_info* info);
+
 /* Chebyshev coefficients of exp(i s x) on [-1,1] computed on the GPU in FP64
  * (Jacobi–Anger, tail-sum truncation at `tol`), cast to float:
  * coeffs[count][max_k], degrees[count]. Replaces the call to

@@ -137,6 +137,7 @@ def _bind(L):
         "mqw_multiqw": (i, [_vp, i, i, ctypes.c_char_p, ll, ll, ctypes.c_char_p, i]),
         "mqw_clenshaw_noalloc": (i, [i, i, i, _vp, _vp, f, f, _vp, _vp, _vp]),
         "mqw_grid_shape_for": (i, [_vp, i, i, _P(GridShape)]),
+        "mqw_diag_moments": (i, [_vp, i, _P(d), _P(d), _P(DiagInfo)]),
         "mqw_mlp_linear_forward": (i, [i, i, i, _vp, _vp, _vp, _vp, i, _vp]),
         "mqw_mlp_linear_backward": (i, [i, i, i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, i, _vp]),
         "mqw_mlp_adam": (i, [i, _vp, _vp, _vp, _vp, _vp, f, f, f, f, f, i, _vp]),
@@ -289,6 +290,15 @@ class Context:
         _check(self.h, lib().mqw_build_diag(self.h, n, _ptr(raw, ctypes.c_double), _ptr(hp, ctypes.c_float),
                                             _ptr(E, ctypes.c_double), ctypes.byref(info)))
         return hp, E, info
+
+    def diag_moments(self, n: int, raw) -> np.ndarray:
+        """mean(H_P^k) for k = 1..4 of the shifted diagonal (FP64, on the GPU)."""
+        raw = np.ascontiguousarray(raw, dtype=np.float64)
+        m = np.zeros(4, np.float64)
+        info = DiagInfo()
+        _check(self.h, lib().mqw_diag_moments(self.h, n, _ptr(raw, ctypes.c_double),
+                                              _ptr(m, ctypes.c_double), ctypes.byref(info)))
+        return m
 
     def cheb_coeffs(self, s, tol: float = 1e-6, max_k: int = 4096):
         s = np.ascontiguousarray(np.atleast_1d(s), dtype=np.float64)

@@ -305,7 +305,59 @@ diag_write(int n, const double* raw_all, const double* chunk_excl,
   (void)total;
 }
 
+// Raw moments of the shifted diagonal, mean(H_P^k) for k = 1..4, in FP64:
+// a fixed grid with a grid-stride loop gives each block a fixed set of
+// amplitudes, and the block partials are summed in order by one block, so
+// the result is run-to-run identical.
+constexpr int kMomentBlocks = 1024;
+__global__ void moments_partial(const float* __restrict__ hp, size_t N, double* part) {
+  double s[4] = {0.0, 0.0, 0.0, 0.0};
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < N;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double x = hp[i], x2 = x * x;
+    s[0] += x;
+    s[1] += x2;
+    s[2] += x2 * x;
+    s[3] += x2 * x2;
+  }
+  __shared__ double red[4][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    double v = s[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[k][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[threadIdx.x][w];
+    part[(size_t)blockIdx.x * 4 + threadIdx.x] = v;
+  }
+}
+__global__ void moments_final(const double* part, int blocks, double inv_n, double* out) {
+  if (threadIdx.x < 4) {
+    double v = 0.0;
+    for (int b = 0; b < blocks; b++) v += part[(size_t)b * 4 + threadIdx.x];
+    out[threadIdx.x] = v * inv_n;
+  }
+}
+
 }  // namespace
+
+size_t moments_scratch_bytes() { return (size_t)(kMomentBlocks + 1) * 4 * sizeof(double); }
+
+cudaError_t launch_moments(int n, const float* hp, void* scratch, cudaStream_t stream) {
+  if (n < 1 || n > kMaxN || !hp || !scratch) return cudaErrorInvalidValue;
+  const size_t N = (size_t)1 << n;
+  const size_t want = (N + 255) / 256;
+  const int blocks = (int)(want < kMomentBlocks ? want : kMomentBlocks);
+  double* part = (double*)scratch;
+  double* out = part + (size_t)kMomentBlocks * 4;
+  moments_partial<<<blocks, 256, 0, stream>>>(hp, N, part);
+  moments_final<<<1, 32, 0, stream>>>(part, blocks, 1.0 / (double)N, out);
+  return cudaGetLastError();
+}
 
 size_t diag_scratch_bytes(int n, int count) {
   const DiagGeom g = diag_geom(n);

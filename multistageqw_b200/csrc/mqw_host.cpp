@@ -368,9 +368,12 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
       const PassGeomHost geo = pass_geom(precision, n, l, threads, ls);
       if (geo.threads != threads || geo.lane_smem != ls) continue;  // shape not built here
       const int g0 = default_group(precision, geo, n);
-      for (int g : {1, 2, 4, g0}) {
+      std::vector<int> groups = {1, 2, 4};
+      if (g0 != 1 && g0 != 2 && g0 != 4) groups.push_back(g0);
+      if (want.group && std::find(groups.begin(), groups.end(), want.group) == groups.end())
+        groups.push_back(want.group);
+      for (int g : groups) {
         if (want.group && g != want.group) continue;
-        if (g == g0 && g0 <= 4 && g0 != 3) continue;  // already a candidate
         for (int lanes : {1, 2}) {
           if (want.lanes && lanes != want.lanes) continue;
           if (g > kMaxGroup || (size_t)g * lanes * walk_bytes(precision, geo, n) > budget) continue;
@@ -1232,6 +1235,39 @@ mqw_status mqw_build_diag(mqw_ctx* ctx, int n, const double* raw, float* hp,
   CK(cudaMemcpyAsync(&o, d_out.p, sizeof o, cudaMemcpyDeviceToHost, st));
   if (hp) CK(cudaMemcpyAsync(hp, d_hp.p, N * sizeof(float), cudaMemcpyDeviceToHost, st));
   if (energies) CK(cudaMemcpyAsync(energies, d_e.p, N * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CK(cudaStreamSynchronize(st));
+  if (info) {
+    info->e0 = o.e0;
+    info->emax = o.emax;
+    info->mid = o.mid;
+    info->e_abs = o.e_abs;
+    info->e_loc = o.e_loc;
+  }
+  return MQW_OK;
+}
+
+mqw_status mqw_diag_moments(mqw_ctx* ctx, int n, const double* raw, double* moments,
+                            mqw_diag_info* info) {
+  mqw_status s = check_ctx(ctx);
+  if (s != MQW_OK) return s;
+  if (n < 1 || n > MQW_MAX_N || !raw || !moments)
+    return fail(ctx, MQW_ERR_INVALID, "diag_moments: bad arguments");
+  const size_t N = (size_t)1 << n;
+  DevMem d_raw, d_hp, d_out, d_scr, d_mom;
+  CK(d_raw.ensure(params_per(n) * sizeof(double)));
+  CK(d_hp.ensure(N * sizeof(float)));
+  CK(d_out.ensure(sizeof(DiagOut)));
+  CK(d_scr.ensure(diag_scratch_bytes(n, 1)));
+  CK(d_mom.ensure(moments_scratch_bytes()));
+  cudaStream_t st = ctx->stream;
+  CK(cudaMemcpyAsync(d_raw.p, raw, params_per(n) * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(launch_diag(n, 1, d_raw.as<double>(), d_hp.as<float>(), nullptr, d_out.as<DiagOut>(),
+                 d_scr.p, st));
+  CK(launch_moments(n, d_hp.as<float>(), d_mom.p, st));
+  DiagOut o;
+  CK(cudaMemcpyAsync(&o, d_out.p, sizeof o, cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(moments, d_mom.as<char>() + moments_scratch_bytes() - 4 * sizeof(double),
+                     4 * sizeof(double), cudaMemcpyDeviceToHost, st));
   CK(cudaStreamSynchronize(st));
   if (info) {
     info->e0 = o.e0;

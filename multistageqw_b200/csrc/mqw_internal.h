@@ -52,6 +52,11 @@ cudaError_t launch_diag(int n, int count, const double* raw, float* hp,
                         double* energies, DiagOut* out, void* scratch,
                         cudaStream_t stream);
 
+// Moments mean(hp^k), k = 1..4, of a 2^n diagonal into the last four
+// doubles of `scratch` (moments_scratch_bytes()).
+size_t moments_scratch_bytes();
+cudaError_t launch_moments(int n, const float* hp, void* scratch, cudaStream_t stream);
+
 // ---- Chebyshev coefficients --------------------------------------------
 // One entry per (instance, stage, sample) "coefficient job".
 struct CoefJob {

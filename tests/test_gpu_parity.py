@@ -261,3 +261,17 @@ def test_wide_tile_2_13_matches(ctx, orc, n):
     r64 = ctx.run_problems(n, 2, raw, precision="fp64", samples=2, graph=0)
     assert abs(r13["p"][0] - r12["p"][0]) <= 1e-6
     assert abs(r13["p"][0] - r64["p"][0]) <= 1e-5
+
+
+@pytest.mark.parametrize("n", [8, 15, 20])
+def test_diag_moments(ctx, orc, n):
+    """GPU moments of the shifted diagonal against numpy on the oracle's
+    bit-identical diagonal (FP64 sums; relative 1e-12)."""
+    raw = orc.sk_instances(n, 1, 2100 + n)[0]
+    _, hp, _ = orc.energies_ref(n, raw)
+    x = hp.astype(np.float64)
+    ref = np.array([np.mean(x), np.mean(x ** 2), np.mean(x ** 3), np.mean(x ** 4)])
+    m = ctx.diag_moments(n, raw)
+    scale = np.array([np.sqrt(ref[1]), ref[1], ref[1] ** 1.5, ref[1] ** 2])
+    assert np.all(np.abs(m - ref) <= 1e-12 * scale), (m, ref)
+    assert np.array_equal(m, ctx.diag_moments(n, raw))  # deterministic
