@@ -76,6 +76,9 @@ typedef struct mqw_options {
                       or 256 (twice the amplitudes per thread), 0 = autotuned */
   int lane_smem;   /* grid-path partners along the warp-lane axes: 1 from
                       shared memory, -1 by warp shuffles, 0 = autotuned */
+  int tma;         /* grid-path tile staging (FP32): 1 bulk copies (TMA)
+                      completing on an mbarrier, -1 per-thread cp.async,
+                      0 = autotuned */
   int stage1_basis; /* 1 (default): FP32 walks of an instance share one
                        Chebyshev basis for their first stage (built once,
                        recombined per walk); 0: every walk runs its own
@@ -240,6 +243,13 @@ mqw_status mqw_plan_results(mqw_plan* plan, double* p_out, float* total_t,
 mqw_status mqw_plan_stats(const mqw_plan* plan, mqw_run_stats* stats);
 void mqw_plan_destroy(mqw_plan* plan);
 
+/* Failure-path self-test of the device-side bounded waits: runs one pass
+ * whose tile copies can never complete (its mbarrier expects bytes nobody
+ * sends), so every CTA's wait gives up after 5 ms, records the error and
+ * returns. Returns MQW_ERR_TIMEOUT when the kernel reported it as designed
+ * (the context stays usable); any other status is a failure. */
+mqw_status mqw_selftest_wait_timeout(mqw_ctx* ctx);
+
 /* The grid-path shape the autotuner picks for n-spin walks in `precision`
  * on this context (tuning now if it has not yet): tile of 2^tile_log
  * amplitudes per CTA, spread over 2^cluster_log CTAs; global_axes axes whose
@@ -249,6 +259,7 @@ typedef struct mqw_grid_shape {
   int tile_log, cluster_log, global_axes, group, lanes;
   int threads;     /* threads per CTA */
   int lane_smem;   /* 1: lane-axis partners from shared memory */
+  int tma;         /* 1: tiles staged by bulk copies */
   double us_per_walk_pass;
 } mqw_grid_shape;
 mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,

@@ -58,6 +58,7 @@ class Options(ctypes.Structure):
         ("lanes", ctypes.c_int),
         ("threads", ctypes.c_int),
         ("lane_smem", ctypes.c_int),
+        ("tma", ctypes.c_int),
         ("stage1_basis", ctypes.c_int),
     ]
 
@@ -81,6 +82,7 @@ class GridShape(ctypes.Structure):
         ("lanes", ctypes.c_int),
         ("threads", ctypes.c_int),
         ("lane_smem", ctypes.c_int),
+        ("tma", ctypes.c_int),
         ("us_per_walk_pass", ctypes.c_double),
     ]
 
@@ -138,6 +140,7 @@ def _bind(L):
         "mqw_clenshaw_noalloc": (i, [i, i, i, _vp, _vp, f, f, _vp, _vp, _vp]),
         "mqw_grid_shape_for": (i, [_vp, i, i, _P(GridShape)]),
         "mqw_diag_moments": (i, [_vp, i, _P(d), _P(d), _P(DiagInfo)]),
+        "mqw_selftest_wait_timeout": (i, [_vp]),
         "mqw_mlp_linear_forward": (i, [i, i, i, _vp, _vp, _vp, _vp, i, _vp]),
         "mqw_mlp_linear_backward": (i, [i, i, i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, i, _vp]),
         "mqw_mlp_adam": (i, [i, _vp, _vp, _vp, _vp, _vp, f, f, f, f, f, i, _vp]),
@@ -179,7 +182,7 @@ def _ptr(a, ct):
 
 def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_max_n=0,
           stage_scale=None, tile_log=0, graph=1, lanes=0, threads=0, lane_smem=0,
-          stage1_basis=1):
+          tma=0, stage1_basis=1):
     o = Options()
     lib().mqw_default_options(ctypes.byref(o))
     o.precision = {"fp32": FP32, "fp64": FP64, FP32: FP32, FP64: FP64}[precision]
@@ -192,6 +195,7 @@ def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_ma
     o.lanes = int(lanes)
     o.threads = int(threads)
     o.lane_smem = int(lane_smem)
+    o.tma = int(tma)
     o.stage1_basis = int(stage1_basis)
     keep = None
     if stage_scale is not None:

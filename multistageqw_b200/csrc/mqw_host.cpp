@@ -70,6 +70,7 @@ struct GridShape {
   int lmax = 0, group = 1, lanes = 1;
   int threads = 0;  // CTA threads at the widest tile (0: 512)
   int lane_smem = 0;  // lane axes: 1 shared memory, -1 shuffles, 0 (want): any
+  int tma = 0;        // staging: 1 bulk copies, -1 cp.async, 0 (want): any
   double us = 0.0;  // timed microseconds per walk-pass (0: not timed)
 };
 constexpr int kMaxLanes = 4;
@@ -80,6 +81,9 @@ struct mqw_ctx {
   std::string err;
   int sm_count = 0;
   DevMem state, norm_part, kappa, diag_scratch, tune_coef;
+  // Device error word: kernels whose bounded waits give up set bit 0; the
+  // host reads and clears it when it collects results.
+  DevMem dev_err;
   DevMem basis;  // stage-1 basis of the instance in flight (+ its partial P)
   // Bumped whenever a shared scratch buffer is reallocated: a plan's captured
   // graph holds the old addresses and is re-captured when this changes.
@@ -172,6 +176,7 @@ void default_opts(mqw_options* o) {
   o->lanes = 0;
   o->threads = 0;
   o->lane_smem = 0;
+  o->tma = 0;
   o->stage1_basis = 1;
 }
 
@@ -241,6 +246,17 @@ mqw_status check_ctx(mqw_ctx* ctx) {
   return MQW_OK;
 }
 
+// Reads and clears the device error word (after the work that may set it
+// has completed): MQW_ERR_TIMEOUT when a kernel's bounded wait gave up.
+mqw_status take_device_error(mqw_ctx* ctx) {
+  unsigned v = 0;
+  CK(cudaMemcpy(&v, ctx->dev_err.p, sizeof v, cudaMemcpyDeviceToHost));
+  if (v == 0) return MQW_OK;
+  CK(cudaMemset(ctx->dev_err.p, 0, sizeof v));
+  return fail(ctx, MQW_ERR_TIMEOUT,
+              "a grid-path pass gave up waiting for its tile's bulk copies (error word %#x)", v);
+}
+
 int walk_slots(const PassGeomHost& geo) { return geo.nu > 0 ? 4 : 3; }
 
 size_t walk_bytes(int precision, const PassGeomHost& geo, int n) {
@@ -263,9 +279,9 @@ int default_group(int precision, const PassGeomHost& geo, int n) {
 // tilings) over G zero-filled walks on each of `lanes` concurrent streams.
 // Returns microseconds per walk-pass.
 mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
-                            int G, int lanes, int threads, int lane_smem,
+                            int G, int lanes, int threads, int lane_smem, int tma,
                             double* us_per_walk) {
-  const PassGeomHost geo = pass_geom(precision, n, lmax, threads, lane_smem);
+  const PassGeomHost geo = pass_geom(precision, n, lmax, threads, lane_smem, tma);
   const size_t N = (size_t)1 << n;
   const size_t amp = precision == 0 ? 8 : 16;
   const int slots = walk_slots(geo);
@@ -286,6 +302,8 @@ mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
     pp.C = geo.C;
     pp.threads = geo.threads;
     pp.lane_smem = geo.lane_smem;
+    pp.tma = geo.tma;
+    pp.err = ctx->dev_err.as<unsigned>();
     pp.a = geo.a;
     pp.tiling = (r & 1) ? 2 : 1;
     pp.count = G;
@@ -330,6 +348,8 @@ mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
   CK(cudaEventElapsedTime(&ms, e0, e1));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  mqw_status es = take_device_error(ctx);
+  if (es != MQW_OK) return es;
   *us_per_walk = 1000.0 * ms / (reps * W);
   return MQW_OK;
 }
@@ -340,8 +360,8 @@ mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
 mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridShape* out) {
   const auto key = std::make_pair(precision, n);
   auto it = ctx->tuned.find(key);
-  const bool fixed_none =
-      !want.lmax && !want.group && !want.lanes && !want.threads && !want.lane_smem;
+  const bool fixed_none = !want.lmax && !want.group && !want.lanes && !want.threads &&
+                          !want.lane_smem && !want.tma;
   if (it != ctx->tuned.end() && fixed_none) {
     *out = it->second;
     return MQW_OK;
@@ -350,50 +370,88 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)8 << 30;
   const size_t budget = std::min(free_b / 4, (size_t)16 << 30);
+  const bool log = getenv("MQW_TUNE_LOG") != nullptr;
+  auto fits = [&](const PassGeomHost& geo, int g, int lanes) {
+    return g <= kMaxGroup && (size_t)g * lanes * walk_bytes(precision, geo, n) <= budget;
+  };
+  auto time = [&](const GridShape& c, double* us) -> mqw_status {
+    const PassGeomHost geo = pass_geom(precision, n, c.lmax, c.threads, c.lane_smem > 0, c.tma > 0);
+    mqw_status s = time_grid_config(ctx, precision, n, c.lmax, c.group, c.lanes, c.threads,
+                                    c.lane_smem > 0, c.tma > 0, us);
+    if (s == MQW_OK && log)
+      fprintf(stderr,
+              "mqw tune: precision %d n %d tile %d cluster %d global %d threads %d lane_smem %d "
+              "tma %d group %d lanes %d: %.3f us/walk-pass\n",
+              precision, n, geo.L, geo.C, geo.nu, c.threads ? c.threads : 512, geo.lane_smem,
+              geo.tma, c.group, c.lanes, *us);
+    return s;
+  };
+  // Stage 1: the pass shape — tile cap (the default widest tile, one
+  // narrower, and in FP32 the 2^13 tile when the default leaves axes to
+  // global memory), threads, lane axes, staging — each timed with one walk
+  // per launch on two lanes (one if two do not fit).
+  std::vector<int> caps = {def_l, def_l - 1};
+  if (precision == 0 && n > 2 * def_l - 4) caps.insert(caps.begin() + 1, def_l + 1);
   double best = 1e300;
   GridShape b;
   b.lmax = want.lmax ? want.lmax : def_l;
   b.group = want.group ? want.group : 1;
   b.lanes = want.lanes ? want.lanes : 1;
-  // Tile caps: the default widest tile, one narrower, and in FP32 the 2^13
-  // tile when the default leaves axes to global memory.
-  std::vector<int> caps = {def_l, def_l - 1};
-  if (precision == 0 && n > 2 * def_l - 4) caps.insert(caps.begin() + 1, def_l + 1);
+  b.threads = want.threads == 256 ? 256 : 0;
+  b.lane_smem = want.lane_smem;
+  b.tma = want.tma;
   for (int l : caps) {
     if (want.lmax && l != want.lmax) continue;
     for (int threads : {0, 256})
-    for (int ls : {0, 1}) {
-      if (want.threads && (want.threads == 256) != (threads == 256)) continue;
-      if (want.lane_smem && (want.lane_smem > 0) != (ls == 1)) continue;
-      const PassGeomHost geo = pass_geom(precision, n, l, threads, ls);
-      if (geo.threads != threads || geo.lane_smem != ls) continue;  // shape not built here
-      const int g0 = default_group(precision, geo, n);
-      std::vector<int> groups = {1, 2, 4};
-      if (g0 != 1 && g0 != 2 && g0 != 4) groups.push_back(g0);
-      if (want.group && std::find(groups.begin(), groups.end(), want.group) == groups.end())
-        groups.push_back(want.group);
-      for (int g : groups) {
-        if (want.group && g != want.group) continue;
-        for (int lanes : {1, 2}) {
-          if (want.lanes && lanes != want.lanes) continue;
-          if (g > kMaxGroup || (size_t)g * lanes * walk_bytes(precision, geo, n) > budget) continue;
+      for (int ls : {0, 1})
+        for (int tma : {0, 1}) {
+          if (want.threads && (want.threads == 256) != (threads == 256)) continue;
+          if (want.lane_smem && (want.lane_smem > 0) != (ls == 1)) continue;
+          if (want.tma && (want.tma > 0) != (tma == 1)) continue;
+          const PassGeomHost geo = pass_geom(precision, n, l, threads, ls, tma);
+          if (geo.threads != threads || geo.lane_smem != ls || geo.tma != tma) continue;
+          GridShape c;
+          c.lmax = l;
+          c.threads = threads;
+          c.lane_smem = ls ? 1 : -1;
+          c.tma = tma ? 1 : -1;
+          c.group = want.group ? want.group : 1;
+          c.lanes = want.lanes ? want.lanes : (fits(geo, c.group, 2) ? 2 : 1);
+          if (!fits(geo, c.group, c.lanes)) continue;
           double us = 0.0;
-          mqw_status s = time_grid_config(ctx, precision, n, l, g, lanes, threads, ls, &us);
+          mqw_status s = time(c, &us);
           if (s != MQW_OK) return s;
-          if (getenv("MQW_TUNE_LOG"))
-            fprintf(stderr, "mqw tune: precision %d n %d tile %d cluster %d global %d threads %d lane_smem %d group %d lanes %d: %.3f us/walk-pass\n",
-                    precision, n, geo.L, geo.C, geo.nu, threads ? threads : 512, ls, g, lanes, us);
-          // Prefer the earlier candidate (larger tile, fewer walks in flight)
+          // Prefer the earlier candidate (larger tile, simpler variant)
           // unless a later one is clearly faster.
           if (us < best * 0.98) {
             best = us;
-            b.lmax = l;
-            b.group = g;
-            b.lanes = lanes;
-            b.threads = threads;
-            b.lane_smem = ls ? 1 : -1;
-            b.us = us;
+            c.us = us;
+            b = c;
           }
+        }
+  }
+  // Stage 2: walks per launch and lanes for that shape.
+  if (best < 1e300 && (!want.group || !want.lanes)) {
+    const PassGeomHost geo = pass_geom(precision, n, b.lmax, b.threads, b.lane_smem > 0, b.tma > 0);
+    const int g0 = default_group(precision, geo, n);
+    std::vector<int> groups = {1, 2, 4};
+    if (g0 != 1 && g0 != 2 && g0 != 4) groups.push_back(g0);
+    const GridShape base = b;
+    for (int g : groups) {
+      if (want.group && g != want.group) continue;
+      for (int lanes : {1, 2}) {
+        if (want.lanes && lanes != want.lanes) continue;
+        if ((g == base.group && lanes == base.lanes) || !fits(geo, g, lanes)) continue;
+        GridShape c = base;
+        c.group = g;
+        c.lanes = lanes;
+        double us = 0.0;
+        mqw_status s = time(c, &us);
+        if (s != MQW_OK) return s;
+        if (us < best * 0.98) {
+          best = us;
+          c.us = us;
+          b = c;
         }
       }
     }
@@ -475,6 +533,8 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
       pp.C = geo.C;
       pp.threads = geo.threads;
       pp.lane_smem = geo.lane_smem;
+      pp.tma = geo.tma;
+      pp.err = ctx->dev_err.as<unsigned>();
       pp.a = geo.a;
       pp.tiling = (r & 1) ? 2 : 1;
       pp.count = G;
@@ -561,6 +621,8 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int Kb, int kb_cap,
     pp.C = geo.C;
     pp.threads = geo.threads;
     pp.lane_smem = geo.lane_smem;
+    pp.tma = geo.tma;
+    pp.err = ctx->dev_err.as<unsigned>();
     pp.a = geo.a;
     pp.tiling = ((R - j) & 1) ? 2 : 1;
     pp.count = 1;
@@ -646,7 +708,7 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
   for (auto& kv : grid_by_n) {
     const int n = kv.first;
     const GridShape gs = P.grid_geo.at(n);
-    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0);
+    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, gs.tma > 0);
     const int G = gs.group;
     const std::vector<int>& ws = kv.second;
     const int kb_cap = P.basis_kb.count(n) ? P.basis_kb.at(n) : 0;
@@ -731,7 +793,9 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     gs.lanes = std::min(std::max(0, P.opt.lanes), kMaxLanes);
     gs.threads = P.opt.threads == 256 ? 256 : 0;
     gs.lane_smem = P.opt.lane_smem;
-    if (!gs.lmax || !gs.group || !gs.lanes || !P.opt.threads || !P.opt.lane_smem) {
+    gs.tma = P.opt.tma;
+    if (!gs.lmax || !gs.group || !gs.lanes || !P.opt.threads || !P.opt.lane_smem ||
+        !P.opt.tma) {
       GridShape want = gs;
       want.threads = P.opt.threads;  // 0: tuned, else fixed
       GridShape t;
@@ -742,7 +806,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     gs.group = std::min(std::min(gs.group, kMaxGroup), kv.second);
     const int ngroups = (kv.second + gs.group - 1) / gs.group;
     gs.lanes = std::max(1, std::min(gs.lanes, ngroups));
-    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0);
+    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, gs.tma > 0);
     P.grid_geo[n] = gs;
     lanes_max = std::max(lanes_max, gs.lanes);
     const size_t N = (size_t)1 << n;
@@ -925,6 +989,9 @@ mqw_status mqw_create(mqw_ctx** out, int device) {
   ctx->device = device;
   ctx->sm_count = prop.multiProcessorCount;
   if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return MQW_ERR_CUDA;
+  if (ctx->dev_err.ensure(sizeof(unsigned)) != cudaSuccess ||
+      cudaMemset(ctx->dev_err.p, 0, sizeof(unsigned)) != cudaSuccess)
     return MQW_ERR_CUDA;
   *out = ctx.release();
   return MQW_OK;
@@ -1125,6 +1192,8 @@ mqw_status mqw_plan_results(mqw_plan* plan, double* p_out, float* total_t,
   if (s != MQW_OK) return s;
   if (!plan->executed) return fail(ctx, MQW_ERR_INVALID, "plan not executed");
   CK(cudaDeviceSynchronize());
+  s = take_device_error(ctx);
+  if (s != MQW_OK) return s;
   const int count = plan->count;
   std::vector<double> pm(count);
   std::vector<DiagOut> dg(count);
@@ -1151,6 +1220,49 @@ mqw_status mqw_plan_results(mqw_plan* plan, double* p_out, float* total_t,
   return MQW_OK;
 }
 
+mqw_status mqw_selftest_wait_timeout(mqw_ctx* ctx) {
+  mqw_status st = check_ctx(ctx);
+  if (st != MQW_OK) return st;
+  // One FP32 n = 14 pass with bulk-copy staging whose mbarrier expects 16
+  // bytes that no copy delivers: every CTA's bounded wait (5 ms) runs out,
+  // sets the error word and returns. Nothing else is in flight.
+  const int n = 14;
+  const size_t N = (size_t)1 << n;
+  const PassGeomHost geo = pass_geom(0, n, 0, 0, 0, 1);
+  CK(ctx->grow(ctx->state, 3 * N * 8 + N * sizeof(float)));
+  CK(ctx->grow(ctx->norm_part, (N >> geo.L) * sizeof(double)));
+  CK(ctx->tune_coef.ensure(64 * sizeof(float)));
+  CK(cudaMemsetAsync(ctx->state.p, 0, 3 * N * 8 + N * sizeof(float), ctx->stream));
+  CK(cudaMemsetAsync(ctx->tune_coef.p, 0, 64 * sizeof(float), ctx->stream));
+  char* base = ctx->state.as<char>();
+  PassParams pp{};
+  pp.n = n;
+  pp.L = geo.L;
+  pp.C = 0;
+  pp.a = geo.a;
+  pp.tma = 1;
+  pp.tiling = 1;
+  pp.count = 1;
+  pp.err = ctx->dev_err.as<unsigned>();
+  pp.wait_ns = 5000000ull;
+  pp.test_stall = 1;
+  PassWalk& W = pp.walk[0];
+  W.active = 1;
+  W.psi = base;
+  W.bin = W.bout = base + N * 8;
+  W.part = base + 2 * N * 8;
+  W.hp = reinterpret_cast<const float*>(base + 3 * N * 8);
+  W.coef = ctx->tune_coef.as<float>();
+  W.norm_part = ctx->norm_part.as<double>();
+  W.gamma = 1.0f;
+  W.scale = 64.0f;
+  W.r = 4;
+  W.K = 40;
+  CK(launch_pass(0, pp, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return take_device_error(ctx);
+}
+
 mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,
                               mqw_grid_shape* out) {
   mqw_status st = check_ctx(ctx);
@@ -1161,10 +1273,11 @@ mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,
   want.group = want.lanes = 0;  // nothing fixed
   st = tune_grid(ctx, precision, n, want, &gs);
   if (st != MQW_OK) return st;
-  const PassGeomHost geo = pass_geom(precision, n, gs.lmax, gs.threads, gs.lane_smem > 0);
+  const PassGeomHost geo = pass_geom(precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, gs.tma > 0);
   out->tile_log = geo.L;
   out->threads = geo.threads ? geo.threads : 512;
   out->lane_smem = geo.lane_smem;
+  out->tma = geo.tma;
   out->cluster_log = geo.C;
   out->global_axes = geo.nu;
   out->group = gs.group;
@@ -1335,6 +1448,8 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
     pp.C = geo.C;
     pp.threads = geo.threads;
     pp.lane_smem = geo.lane_smem;
+    pp.tma = geo.tma;
+    pp.err = ctx->dev_err.as<unsigned>();
     pp.a = geo.a;
     pp.tiling = (r & 1) ? 2 : 1;
     pp.count = 1;

@@ -141,8 +141,13 @@ struct PassParams {
                        // or 256 (more pairs per thread)
   int lane_smem;       // 1: lane-axis partners from shared memory (FP32,
                        // tiles of 2^12 and 2^13), 0: warp shuffles
+  int tma;             // 1: the tile's b, P, psi and D arrive by bulk copies
+                       // (TMA) on an mbarrier, FP32 single-CTA tiles
   int tiling;          // 1 or 2
   int count;
+  unsigned* err;       // device error word (bit 0: a bounded wait gave up)
+  unsigned long long wait_ns;  // limit of each bounded wait (0: 200 ms)
+  int test_stall;      // test hook: expect bytes that never arrive
   PassWalk walk[kMaxGroup];
 };
 struct PassGeomHost {
@@ -150,11 +155,12 @@ struct PassGeomHost {
   int C;               // cluster log (tile of 2^(L+C) amplitudes over 2^C CTAs)
   int threads;         // CTA threads (0: default 512)
   int lane_smem;       // lane axes through shared memory instead of shuffles
+  int tma;             // tile staging by bulk copies (TMA) instead of cp.async
 };
 // Geometry for n; lmax > 0 caps the tile (log2 amplitudes), else the
 // precision's default cap (or MQW_PASS_TILE_LOG) applies.
 PassGeomHost pass_geom(int precision, int n, int lmax = 0, int threads = 0,
-                        int lane_smem = 0);
+                        int lane_smem = 0, int tma = 0);
 cudaError_t launch_pass(int precision, const PassParams& p,
                         cudaStream_t stream);
 

@@ -95,6 +95,7 @@ extern "C" mqw_status mqw_clenshaw_noalloc(int precision, int n, int K,
     pp.C = geo.C;
     pp.threads = geo.threads;
     pp.lane_smem = geo.lane_smem;
+    pp.tma = geo.tma;
     pp.a = geo.a;
     pp.tiling = (r & 1) ? 2 : 1;
     pp.count = 1;

@@ -212,19 +212,6 @@ __device__ __forceinline__ V4<R> cpsi4(R c, bool odd, const V4<R>& p) {
              : V4<R>{c * p.x, c * p.y, c * p.z, c * p.w};
 }
 
-struct TileMap {
-  int n, L, a, tiling;
-  size_t tile;
-  // Global amplitude index of in-tile position pos (an even position for a
-  // pair; the pair's second amplitude is index + 1).
-  __device__ __forceinline__ size_t index(int pos) const {
-    if (tiling == 1) return (tile << L) | (size_t)pos;
-    const int amask = (1 << a) - 1;
-    return (size_t)(pos & amask) | (tile << a) |
-           ((size_t)(pos >> a) << (n - L + a));
-  }
-};
-
 // Asynchronous global->shared copies (cp.async, sm_80+): the loads of a
 // whole tile are in flight at once without holding registers.
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -343,6 +330,53 @@ __device__ __forceinline__ void cluster_barrier() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n"
                "barrier.cluster.wait.acquire.aligned;\n" ::: "memory");
 }
+// Bulk copies (TMA, no multicast) into this CTA's shared memory, completing
+// on an mbarrier, and bounded waits on it: a wait gives up after `limit_ns`
+// of %globaltimer time so that a copy that never lands cannot hang the GPU.
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+               : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
+                                                  unsigned long long limit_ns) {
+  const unsigned long long t0 = global_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (global_ns() - t0 > limit_ns) return false;
+  return true;
+}
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
+                                          unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
 // The block barrier, or the cluster barrier when the tile spans a cluster.
 template <int CL>
 __device__ __forceinline__ void tile_barrier() {
@@ -394,9 +428,9 @@ template <int LT, int TB = kPassThreads> struct PassShape {
   // With RP >= 8 a thread has the registers to keep P_r (the partial read by
   // the finish) in registers; smaller RP stages it in shared memory.
   static constexpr bool kStageP = kRP < 8;
-  template <typename R>
+  template <typename R, bool StageP = kStageP>
   static constexpr size_t smem() {
-    return (size_t)kPairs * ((kStageP ? 3 : 2) * 4 * sizeof(R) + sizeof(float2));
+    return (size_t)kPairs * ((StageP ? 3 : 2) * 4 * sizeof(R) + sizeof(float2));
   }
 };
 
@@ -418,16 +452,22 @@ constexpr int pass_min_blocks() {
   return 65536 / per_cta > 1 ? 65536 / per_cta : 1;
 }
 
-template <typename R, int LT, int CL, int TB, bool LS = false>
+// TMA: the tile's b_{r+1} (straight into the exchange tile), P_r, psi and D
+// arrive by bulk copies issued by one warp — one per vector for a T1 tile
+// (contiguous), one per 16-amplitude row for T2 — on one mbarrier, instead of
+// per-thread loads and cp.async; P is then always staged in shared memory.
+template <typename R, int LT, int CL, int TB, bool LS = false, bool TMA = false>
 __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
                                   pass_min_blocks<LT, TB, sizeof(R) == 4, CL>())
     pass_kernel(PassParams p) {
   using S = PassShape<LT, TB>;
   constexpr int RP = S::kRP, LOGT = S::kLogT, T = S::kThreads;
-  constexpr bool kStageP = S::kStageP;
+  constexpr bool kStageP = S::kStageP || TMA;
+  static_assert(!TMA || CL == 0, "bulk-copy staging is for single-CTA tiles");
   constexpr int LL = LT + CL;  // tile bits of the tiling
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[32];
+  __shared__ __align__(8) unsigned long long tma_bar;
   const PassWalk& W = p.walk[blockIdx.y];
   if (!W.active) return;
   const int n = p.n, a = p.a;
@@ -497,22 +537,64 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
       if (LT + k >= q0 && LT + k < q1) padd(acc, rv.v[k]);
   };
 
-  // Stage P_r (unless it goes to registers), psi and D for this thread's
-  // own pairs.
-#pragma unroll
-  for (int j = 0; j < RP; j++) {
-    const unsigned gi = g0 + j * gstride;
-    const int o = j * T + tid;
-    if (kStageP && !first) cp_async_pair<R>(sp + 4 * o, part + 2 * (size_t)gi);
-    if (!uni) cp_async_pair<R>(ss + 4 * o, psi + 2 * (size_t)gi);
-    cp_async8(sd + o, hp + gi);
-  }
   Pair<R> va[RP];  // b_{r+1}
   Pair<R> pv[kStageP ? 1 : RP];  // P_r when kept in registers
+  if constexpr (TMA) {
+    // The tile as rows of contiguous amplitudes: T1 is one row of 2^LT,
+    // T2 is 2^(LT-a) rows of 2^a (row k at tile position k 2^a).
+    const int row_log = p.tiling == 1 ? LT : a;
+    const unsigned rows = 1u << (LT - row_log);
+    const unsigned row_amps = 1u << row_log;
+    const unsigned vec_bytes = row_amps * 2u * (unsigned)sizeof(R);
+    const unsigned d_bytes = row_amps * (unsigned)sizeof(float);
+    if (tid == 0) mbar_init(&tma_bar, 1);
+    __syncthreads();
+    if (tid < 32) {
+      if (tid == 0) {
+        const unsigned per_row = (first ? 0u : 2u * vec_bytes) + (uni ? 0u : vec_bytes) + d_bytes;
+        mbar_arrive_expect_tx(&tma_bar, rows * per_row + (p.test_stall ? 16u : 0u));
+      }
+      __syncwarp();
+      for (unsigned k = tid; k < rows; k += 32) {
+        const unsigned g = p.tiling == 1 ? (tile << LT)
+                                         : ((tile << a) | (k << (n - LT + a)));
+        const unsigned pos = k * row_amps;
+        if (!first) {
+          bulk_load(sx + 2 * (size_t)pos, bin + 2 * (size_t)g, vec_bytes, &tma_bar);
+          bulk_load(sp + 2 * (size_t)pos, part + 2 * (size_t)g, vec_bytes, &tma_bar);
+        }
+        if (!uni) bulk_load(ss + 2 * (size_t)pos, psi + 2 * (size_t)g, vec_bytes, &tma_bar);
+        bulk_load(reinterpret_cast<float*>(sd) + pos, hp + g, d_bytes, &tma_bar);
+      }
+    }
+    const unsigned long long limit = p.wait_ns ? p.wait_ns : 200000000ull;
+    const bool ok = mbar_wait_bounded(&tma_bar, 0, limit);
+    if (__syncthreads_or(!ok)) {
+      // Give up on this tile: report, wait (bounded) for any copy still in
+      // flight into this CTA's shared memory, and leave.
+      if (tid == 0 && p.err) atomicOr(p.err, 1u);
+      mbar_wait_bounded(&tma_bar, 0, limit);
+      __syncthreads();
+      return;
+    }
 #pragma unroll
-  for (int j = 0; j < RP; j++) {
-    va[j] = first ? pzero<R>() : pld(bin + 2 * (size_t)(g0 + j * gstride));
-    if constexpr (!kStageP) pv[j] = first ? pzero<R>() : pld(part + 2 * (size_t)(g0 + j * gstride));
+    for (int j = 0; j < RP; j++) va[j] = first ? pzero<R>() : pld(sx + 4 * (tid | (j << LOGT)));
+  } else {
+    // Stage P_r (unless it goes to registers), psi and D for this thread's
+    // own pairs.
+#pragma unroll
+    for (int j = 0; j < RP; j++) {
+      const unsigned gi = g0 + j * gstride;
+      const int o = j * T + tid;
+      if (kStageP && !first) cp_async_pair<R>(sp + 4 * o, part + 2 * (size_t)gi);
+      if (!uni) cp_async_pair<R>(ss + 4 * o, psi + 2 * (size_t)gi);
+      cp_async8(sd + o, hp + gi);
+    }
+#pragma unroll
+    for (int j = 0; j < RP; j++) {
+      va[j] = first ? pzero<R>() : pld(bin + 2 * (size_t)(g0 + j * gstride));
+      if constexpr (!kStageP) pv[j] = first ? pzero<R>() : pld(part + 2 * (size_t)(g0 + j * gstride));
+    }
   }
   const double kap = W.kappa ? *W.kappa : 1.0;
   const R scale = (R)W.scale;
@@ -522,7 +604,7 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   Pair<R> vb[RP];  // b_r
   if (first) {
     const R cr = (R)((double)W.coef[r] * kap);
-    cp_async_wait_all();
+    if constexpr (!TMA) cp_async_wait_all();
 #pragma unroll
     for (int j = 0; j < RP; j++) {
       const V4<R> pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * (j * T + tid));
@@ -530,10 +612,12 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
     }
   } else {
     const R ag = (r == 0 ? a_fin : a_mid) * gamma;
+    if constexpr (!TMA) {  // (with TMA the exchange tile already holds b_{r+1})
 #pragma unroll
-    for (int j = 0; j < RP; j++) pst(sx + 4 * (tid | (j << LOGT)), va[j]);
-    tile_barrier<CL>();
-    cp_async_wait_all();
+      for (int j = 0; j < RP; j++) pst(sx + 4 * (tid | (j << LOGT)), va[j]);
+      tile_barrier<CL>();
+      cp_async_wait_all();
+    }
 #pragma unroll
     for (int j = 0; j < RP; j++) {
       const Remote rv = cluster_load(j, fb0, fb1);
@@ -816,7 +900,7 @@ int max_cluster_log() {
 }
 }  // namespace
 
-PassGeomHost pass_geom(int precision, int n, int lmax, int threads, int lane_smem) {
+PassGeomHost pass_geom(int precision, int n, int lmax, int threads, int lane_smem, int tma) {
   // Tile: 2^L amplitudes of b_{r+1} and 2^L of b_r in shared memory
   // (64 KB at L = 12 in FP32, 3 CTAs per SM). Rows of 2^a = 16 amplitudes
   // (128 bytes in FP32) keep T2 loads coalesced. L is chosen so the two
@@ -859,21 +943,23 @@ PassGeomHost pass_geom(int precision, int n, int lmax, int threads, int lane_sme
   g.threads = (threads == 256 && L == cap && g.C == 0) ? 256 : 0;
   // Lane axes through shared memory: FP32 single-CTA tiles of 2^12 or 2^13.
   g.lane_smem = (lane_smem && precision == 0 && g.C == 0 && L >= cap) ? 1 : 0;
+  // Bulk-copy staging: FP32 single-CTA tiles.
+  g.tma = (tma && precision == 0 && g.C == 0) ? 1 : 0;
   return g;
 }
 
 namespace {
-template <typename R, int LT, int CL, int TB = kPassThreads, bool LS = false>
+template <typename R, int LT, int CL, int TB = kPassThreads, bool LS = false, bool TMA = false>
 cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
   using S = PassShape<LT, TB>;
   static size_t configured = 0;
-  const size_t smem = S::template smem<R>();
+  const size_t smem = S::template smem<R, S::kStageP || TMA>();
   if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB, LS>,
+    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB, LS, TMA>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (CL > 3) {
-      e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB, LS>,
+      e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB, LS, TMA>,
                                cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
       if (e != cudaSuccess) return e;
     }
@@ -881,7 +967,7 @@ cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
   }
   const dim3 grid((unsigned)((size_t)1 << (p.n - LT)), p.count);
   if constexpr (CL == 0) {
-    pass_kernel<R, LT, 0, TB, LS><<<grid, S::kThreads, smem, stream>>>(p);
+    pass_kernel<R, LT, 0, TB, LS, TMA><<<grid, S::kThreads, smem, stream>>>(p);
     return cudaGetLastError();
   } else {
     cudaLaunchConfig_t cfg = {};
@@ -896,8 +982,20 @@ cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, pass_kernel<R, LT, CL, TB, LS>, p);
+    return cudaLaunchKernelEx(&cfg, pass_kernel<R, LT, CL, TB, LS, TMA>, p);
   }
+}
+
+// FP32 single-CTA tile variants: threads (512/256), lane axes (shuffles or
+// shared memory) and staging (cp.async or bulk copies).
+template <typename R, int LT, int TB>
+cudaError_t launch_pass_variant(const PassParams& p, cudaStream_t stream) {
+  if (p.lane_smem) {
+    if (p.tma) return launch_pass_lt<R, LT, 0, TB, true, true>(p, stream);
+    return launch_pass_lt<R, LT, 0, TB, true, false>(p, stream);
+  }
+  if (p.tma) return launch_pass_lt<R, LT, 0, TB, false, true>(p, stream);
+  return launch_pass_lt<R, LT, 0, TB, false, false>(p, stream);
 }
 
 // The widest tile with a cluster of 2^C CTAs.
@@ -906,10 +1004,8 @@ cudaError_t launch_pass_cluster(const PassParams& p, cudaStream_t stream) {
   switch (p.C) {
     case 0:
       if constexpr (sizeof(R) == 4) {
-        if (p.lane_smem) {
-          if (p.threads == 256) return launch_pass_lt<R, LT, 0, 256, true>(p, stream);
-          return launch_pass_lt<R, LT, 0, kPassThreads, true>(p, stream);
-        }
+        if (p.threads == 256) return launch_pass_variant<R, LT, 256>(p, stream);
+        return launch_pass_variant<R, LT, kPassThreads>(p, stream);
       }
       if (p.threads == 256) return launch_pass_lt<R, LT, 0, 256>(p, stream);
       return launch_pass_lt<R, LT, 0>(p, stream);
@@ -927,6 +1023,20 @@ cudaError_t launch_pass_t(const PassParams& p, cudaStream_t stream) {
   if (p.C != 0 && p.L != cap) return cudaErrorInvalidValue;
   if (p.threads == 256 && p.L != cap) return cudaErrorInvalidValue;
   if (p.lane_smem && (sizeof(R) != 4 || p.C != 0 || p.L < cap)) return cudaErrorInvalidValue;
+  if (p.tma && (sizeof(R) != 4 || p.C != 0)) return cudaErrorInvalidValue;
+  if constexpr (sizeof(R) == 4) {
+    if (p.tma && p.L < cap) {
+      switch (p.L) {
+        case 6: return launch_pass_lt<R, 6, 0, kPassThreads, false, true>(p, stream);
+        case 7: return launch_pass_lt<R, 7, 0, kPassThreads, false, true>(p, stream);
+        case 8: return launch_pass_lt<R, 8, 0, kPassThreads, false, true>(p, stream);
+        case 9: return launch_pass_lt<R, 9, 0, kPassThreads, false, true>(p, stream);
+        case 10: return launch_pass_lt<R, 10, 0, kPassThreads, false, true>(p, stream);
+        case 11: return launch_pass_lt<R, 11, 0, kPassThreads, false, true>(p, stream);
+        default: return cudaErrorInvalidValue;
+      }
+    }
+  }
   switch (p.L) {
     case 6: return launch_pass_lt<R, 6, 0>(p, stream);
     case 7: return launch_pass_lt<R, 7, 0>(p, stream);
@@ -942,8 +1052,7 @@ cudaError_t launch_pass_t(const PassParams& p, cudaStream_t stream) {
     case 13:
       if constexpr (sizeof(R) == 4) {
         if (p.C != 0 || p.threads == 256) return cudaErrorInvalidValue;
-        if (p.lane_smem) return launch_pass_lt<R, 13, 0, kPassThreads, true>(p, stream);
-        return launch_pass_lt<R, 13, 0>(p, stream);
+        return launch_pass_variant<R, 13, kPassThreads>(p, stream);
       }
       return cudaErrorInvalidValue;
     default: return cudaErrorInvalidValue;

@@ -275,3 +275,31 @@ def test_diag_moments(ctx, orc, n):
     scale = np.array([np.sqrt(ref[1]), ref[1], ref[1] ** 1.5, ref[1] ** 2])
     assert np.all(np.abs(m - ref) <= 1e-12 * scale), (m, ref)
     assert np.array_equal(m, ctx.diag_moments(n, raw))  # deterministic
+
+
+@pytest.mark.parametrize("n,tile", [(16, 0), (20, 12), (24, 11), (24, 13)])
+def test_bulk_copy_staging_matches_cp_async(ctx, orc, n, tile):
+    """Tiles staged by bulk copies on an mbarrier (TMA) against per-thread
+    cp.async staging: the same arithmetic, so equal results up to nothing
+    (bit-identical per-sample values), and within FP32 of FP64."""
+    raw = orc.sk_instances(n, 1, 2500 + n)
+    kw = dict(samples=3, graph=0, group=1, lanes=1, tile_log=tile, threads=512, lane_smem=-1,
+              stage1_basis=0)
+    r_t = ctx.run_problems(n, 2, raw, precision="fp32", tma=1, **kw)
+    r_c = ctx.run_problems(n, 2, raw, precision="fp32", tma=-1, **kw)
+    assert r_t["p"][0] == r_c["p"][0]
+    r64 = ctx.run_problems(n, 2, raw, precision="fp64", samples=3, graph=0)
+    assert abs(r_t["p"][0] - r64["p"][0]) <= 1e-5
+
+
+def test_bounded_wait_reports_timeout_and_context_survives(ctx, orc, mqw):
+    """A pass whose bulk copies can never complete (its mbarrier expects
+    bytes nobody sends) gives up after its 5 ms bound, reports
+    MQW_ERR_TIMEOUT through the device error word, and the context keeps
+    working."""
+    st = mqw.lib().mqw_selftest_wait_timeout(ctx.h)
+    assert st == 5, st  # MQW_ERR_TIMEOUT
+    raw = orc.sk_instances(14, 1, 3)
+    r = ctx.run_problems(14, 2, raw, samples=2, tma=1)
+    o = orc.run_problems(14, 2, raw, 1, 2, "f64")
+    assert abs(r["p"][0] - o["p"][0]) <= 1e-5
