@@ -48,8 +48,11 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # ncu capture of the workload (cold caches: ncu flushes them between
 # replays), keyed by config.workload: profiles/pass_kernel_sk_n20_m4.md
 # (29.40 MB per 2^20-amplitude launch) and profiles/pass_kernel_sk_n24_global.md
-# (469.8 + 233.0 MB per 2^24-amplitude launch).
-DRAM_BYTES_PER_TERM_AMP = {"sk_n20_m4": 29.40e6 / 2**20, "sk_n24_m4": 702.8e6 / 2**24}
+# (469.8 + 233.0 MB per 2^24-amplitude launch); for n = 28 the same pass
+# shape captured on an n = 26 walk, per amplitude (2373.8 MB per 2^26-amplitude
+# first-stage launch, profiles/launches_sk_n28_m3.md).
+DRAM_BYTES_PER_TERM_AMP = {"sk_n20_m4": 29.40e6 / 2**20, "sk_n24_m4": 702.8e6 / 2**24,
+                           "sk_n28_m3_seed7": 2373.8e6 / 2**26}
 # Host memory the CPU legs may use at once (all worker processes together).
 CPU_MEM_BUDGET = 24 << 30
 

@@ -452,10 +452,12 @@ constexpr int pass_min_blocks() {
   return 65536 / per_cta > 1 ? 65536 / per_cta : 1;
 }
 
-// TMA: the tile's b_{r+1} (straight into the exchange tile), P_r, psi and D
-// arrive by bulk copies issued by one warp — one per vector for a T1 tile
-// (contiguous), one per 16-amplitude row for T2 — on one mbarrier, instead of
-// per-thread loads and cp.async; P is then always staged in shared memory.
+// TMA: in T1 passes (contiguous tiles) the tile's b_{r+1} (straight into the
+// exchange tile), P_r, psi and D arrive by four bulk copies issued by one
+// thread on one mbarrier, instead of per-thread loads and cp.async; P is then
+// always staged in shared memory. T2 tiles (2^(LT-4) rows of 16 amplitudes)
+// keep the per-thread path: one bulk copy per 64-128 byte row measured 2.6x
+// slower than cp.async.
 template <typename R, int LT, int CL, int TB, bool LS = false, bool TMA = false>
 __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
                                   pass_min_blocks<LT, TB, sizeof(R) == 4, CL>())
@@ -539,9 +541,9 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
 
   Pair<R> va[RP];  // b_{r+1}
   Pair<R> pv[kStageP ? 1 : RP];  // P_r when kept in registers
-  if constexpr (TMA) {
-    // The tile as rows of contiguous amplitudes: T1 is one row of 2^LT,
-    // T2 is 2^(LT-a) rows of 2^a (row k at tile position k 2^a).
+  const bool bulk = TMA && p.tiling == 1;
+  if (bulk) {
+    // The tile as rows of contiguous amplitudes (T1: one row of 2^LT).
     const int row_log = p.tiling == 1 ? LT : a;
     const unsigned rows = 1u << (LT - row_log);
     const unsigned row_amps = 1u << row_log;
@@ -604,7 +606,7 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   Pair<R> vb[RP];  // b_r
   if (first) {
     const R cr = (R)((double)W.coef[r] * kap);
-    if constexpr (!TMA) cp_async_wait_all();
+    if (!bulk) cp_async_wait_all();
 #pragma unroll
     for (int j = 0; j < RP; j++) {
       const V4<R> pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * (j * T + tid));
@@ -612,7 +614,7 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
     }
   } else {
     const R ag = (r == 0 ? a_fin : a_mid) * gamma;
-    if constexpr (!TMA) {  // (with TMA the exchange tile already holds b_{r+1})
+    if (!bulk) {  // (with bulk copies the exchange tile already holds b_{r+1})
 #pragma unroll
       for (int j = 0; j < RP; j++) pst(sx + 4 * (tid | (j << LOGT)), va[j]);
       tile_barrier<CL>();
