@@ -64,7 +64,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mqw", choices=["mqw", "reference"])
     ap.add_argument("--workload", default="sk_n20_m4",
-                    choices=["sk_n20_m4", "mixed", "n28", "precision"])
+                    choices=["sk_n20_m4", "mixed", "n28", "precision", "mixed_full"])
     ap.add_argument("--n", type=int, default=20)
     ap.add_argument("--m", type=int, default=4)
     ap.add_argument("--batch", type=int, default=2, help="instances per step per GPU")
@@ -276,14 +276,13 @@ def make_batch(M, a, rank):
     """(n list, m list, raw concatenated, description) for the workload."""
     seed = replica_seed(a.seed, rank)
     if a.workload == "mixed":
-        # The mixed batch: n uniform in {12, 14, 16, 18, 20}, m in {2..5}.
-        rng = np.random.default_rng(seed)
-        ns = rng.choice([12, 14, 16, 18, 20], a.batch).tolist()
-        ms = rng.integers(2, 6, a.batch).tolist()
-        raws = [M.sk_instances(n, 1, int(rng.integers(1 << 31)))[0] for n in ns]
+        # The mixed batch (n uniform in {12, 14, 16, 18, 20}, m in {2..5}):
+        # its first a.batch instances.
+        from multistageqw_b200 import studies
+        ns, ms, raw = studies.mixed_batch(a.batch, seed)
         desc = {"workload": "sk_mixed_n12-20_m2-5", "n": "12..20 (even)", "m": "2..5",
-                "note": f"{a.batch}-instance seeded subset of the 4096-instance mixed batch"}
-        return ns, ms, np.concatenate(raws), desc
+                "note": f"{a.batch}-instance seeded batch drawn like the 4096-instance mixed batch"}
+        return ns, ms, raw, desc
     if a.workload == "n28":
         raw = M.sk_instances(28, 1, 7)
         desc = {"workload": "sk_n28_m3_seed7", "n": 28, "m": 3,
@@ -337,6 +336,14 @@ def main():
     if a.impl == "reference":
         if rank == 0:
             print(json.dumps(reference_arm(a)), flush=True)
+        return
+
+    if a.workload == "mixed_full":
+        # The whole 4 096-instance mixed batch in one plan (a study run of
+        # a few minutes, not a bench line): one JSON report.
+        if rank == 0:
+            from multistageqw_b200 import studies
+            print(json.dumps(studies.mixed_batch_study(a.batch if a.batch > 2 else 4096)), flush=True)
         return
 
     if a.workload == "precision":

@@ -131,3 +131,66 @@ def precision_study(n: int = 24, m: int = 4, count: int = 32, gap_max: float = 1
     if expect_e_loc is not None:
         rep["e_loc_equals_screen"] = bool(list(expect_e_loc)[:len(e_loc)] == e_loc)
     return rep
+
+
+def mixed_batch(count: int = 4096, seed: int = 0):
+    """The mixed batch: `count` seeded SK instances (J, h ~ N(0,1)) with n
+    uniform in {12, 14, 16, 18, 20} and m uniform in {2, 3, 4, 5}. Returns
+    (n list, m list, raw values back to back)."""
+    from . import sk_instances
+    rng = np.random.default_rng(seed)
+    ns = rng.choice([12, 14, 16, 18, 20], count).tolist()
+    ms = rng.integers(2, 6, count).tolist()
+    raws = [sk_instances(n, 1, int(rng.integers(1 << 31)))[0] for n in ns]
+    return ns, ms, np.concatenate(raws)
+
+
+def mixed_batch_study(count: int = 4096, seed: int = 0, fp64_subset: int = 128) -> dict:
+    """The whole mixed batch as one plan in FP32 (timed after a warm-up plan
+    that tunes every n), and its first `fp64_subset` instances again in FP64
+    for |dP| per instance."""
+    from . import Plan, params_per_instance
+    ns, ms, raw = mixed_batch(count, seed)
+    ctx = Context(0)
+    # Tune each n once (the autotuner's timing is not part of the batch).
+    warm_idx = [ns.index(n) for n in sorted(set(ns))]
+    offs = np.cumsum([0] + [params_per_instance(n) for n in ns])
+    warm_raw = np.concatenate([raw[offs[i]:offs[i + 1]] for i in warm_idx])
+    wp = Plan(ctx, [ns[i] for i in warm_idx], [ms[i] for i in warm_idx], warm_raw, samples=2, graph=0)
+    wp.execute()
+    wp.results()
+    wp.close()
+    t0 = time.time()
+    plan = Plan(ctx, ns, ms, raw, graph=0)
+    t_create = time.time() - t0
+    t1 = time.time()
+    plan.execute()
+    r32 = plan.results()
+    t_exec = time.time() - t1
+    st = plan.stats()
+    plan.close()
+    k = min(fp64_subset, count)
+    sub = raw[:offs[k]]
+    p64 = Plan(ctx, ns[:k], ms[:k], sub, precision="fp64", graph=0)
+    t2 = time.time()
+    p64.execute()
+    r64 = p64.results()
+    t_64 = time.time() - t2
+    p64.close()
+    ctx.close()
+    dP = np.abs(r32["p"][:k] - r64["p"])
+    by_n = {}
+    for n in sorted(set(ns)):
+        idx = [i for i in range(count) if ns[i] == n]
+        by_n[str(n)] = {"instances": len(idx), "mean_p": float(np.mean(r32["p"][idx]))}
+    return {
+        "metric": "mixed batch: instances/s over the whole batch (FP32), |dP| vs FP64",
+        "instances": count, "seed": seed, "n": "12..20 (even)", "m": "2..5",
+        "seconds_create": t_create, "seconds_execute_and_read": t_exec,
+        "instances_per_s": count / t_exec,
+        "device_ms_propagation": st["kernel_ms"], "launches": st["launches"],
+        "term_amps": st["term_amps"], "pass_amps": st["pass_amps"],
+        "fp64_subset": k, "seconds_fp64_subset": t_64,
+        "max_abs_dP": float(dP.max()), "mean_abs_dP": float(dP.mean()),
+        "by_n": by_n,
+    }
