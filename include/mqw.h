@@ -50,7 +50,11 @@ typedef enum mqw_status {
 
 typedef enum mqw_precision {
   MQW_FP32 = 0, /* complex64 state, FP32 recurrence (the reference's precision) */
-  MQW_FP64 = 1  /* complex128 state, FP64 recurrence (the GPU oracle) */
+  MQW_FP64 = 1, /* complex128 state, FP64 recurrence (the GPU oracle) */
+  MQW_FP32_COMPENSATED = 2 /* complex64 state, FP32 recurrence whose n-term
+                              partner sums are compensated (TwoSum): about one
+                              rounding per sum; grid path only (n >= 6), no
+                              stage-1 basis */
 } mqw_precision;
 
 typedef struct mqw_options {

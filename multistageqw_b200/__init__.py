@@ -30,7 +30,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libmqw.so")
 CLI_PATH = os.path.join(_HERE, "_lib", "MultiQW")
 
 SAMPLES = 100
-FP32, FP64 = 0, 1
+FP32, FP64, FP32C = 0, 1, 2  # FP32C: FP32 with compensated partner sums
 
 _STATUS = {
     0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory",
@@ -185,7 +185,8 @@ def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_ma
           tma=0, stage1_basis=1):
     o = Options()
     lib().mqw_default_options(ctypes.byref(o))
-    o.precision = {"fp32": FP32, "fp64": FP64, FP32: FP32, FP64: FP64}[precision]
+    o.precision = {"fp32": FP32, "fp64": FP64, "fp32c": FP32C, FP32: FP32, FP64: FP64,
+                   FP32C: FP32C}[precision]
     o.samples = int(samples)
     o.cheb_tol = float(cheb_tol)
     o.group = int(group)
@@ -314,8 +315,8 @@ class Context:
 
     def clenshaw(self, n: int, coeffs, hp, gamma: float, scale: float, psi, precision="fp32"):
         """psi: complex array of 2^n amplitudes; returns sum_k c_k T_k(H~) psi."""
-        prec = FP32 if precision == "fp32" else FP64
-        ct = np.complex64 if prec == FP32 else np.complex128
+        prec = {"fp32": FP32, "fp64": FP64, "fp32c": FP32C}[precision]
+        ct = np.complex128 if prec == FP64 else np.complex64
         psi = np.ascontiguousarray(psi, dtype=ct)
         out = np.zeros_like(psi)
         coeffs = np.ascontiguousarray(coeffs, dtype=np.float32)

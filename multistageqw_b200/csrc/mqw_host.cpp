@@ -186,7 +186,8 @@ struct mqw_plan {
   mqw_ctx* ctx = nullptr;
   mqw_options opt{};
   int count = 0;
-  int precision = 0;
+  int precision = 0;   // storage: 0 FP32, 1 FP64
+  int comp = 0;        // MQW_FP32_COMPENSATED: compensated partner sums
   int samples = MQW_SAMPLES;
   std::vector<int> n, m;                 // per instance (caller order)
   std::vector<int> order;                // instances sorted by n (stable)
@@ -535,6 +536,7 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
       pp.lane_smem = geo.lane_smem;
       pp.tma = geo.tma;
       pp.err = ctx->dev_err.as<unsigned>();
+      pp.comp = P.comp;
       pp.a = geo.a;
       pp.tiling = (r & 1) ? 2 : 1;
       pp.count = G;
@@ -803,6 +805,12 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       if (s != MQW_OK) return s;
       gs = t;
     }
+    if (P.comp) {  // the compensated kernel exists in the default shape only
+      gs.threads = 0;
+      gs.lane_smem = -1;
+      gs.tma = -1;
+      gs.lmax = std::min(gs.lmax, 12);
+    }
     gs.group = std::min(std::min(gs.group, kMaxGroup), kv.second);
     const int ngroups = (kv.second + gs.group - 1) / gs.group;
     gs.lanes = std::max(1, std::min(gs.lanes, ngroups));
@@ -861,7 +869,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
   // Stage-1 basis: the largest first-stage degree per n decides the buffer;
   // an n whose basis would not fit the budget runs without it.
   P.basis_kb.clear();
-  if (P.opt.stage1_basis && P.precision == 0) {
+  if (P.opt.stage1_basis && P.precision == 0 && !P.comp) {
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)8 << 30;
     const size_t budget = std::min(free_b / 4, (size_t)8 << 30);
@@ -1042,8 +1050,10 @@ mqw_status mqw_plan_create(mqw_ctx* ctx, int count, const int* n, const int* m,
   mqw_options opt;
   default_opts(&opt);
   if (opt_in) opt = *opt_in;
-  if (opt.precision != MQW_FP32 && opt.precision != MQW_FP64)
-    return fail(ctx, MQW_ERR_INVALID, "precision must be MQW_FP32 or MQW_FP64");
+  if (opt.precision != MQW_FP32 && opt.precision != MQW_FP64 &&
+      opt.precision != MQW_FP32_COMPENSATED)
+    return fail(ctx, MQW_ERR_INVALID,
+                "precision must be MQW_FP32, MQW_FP64 or MQW_FP32_COMPENSATED");
   if (opt.samples < 1 || opt.samples > MQW_SAMPLES)
     return fail(ctx, MQW_ERR_INVALID, "samples must be in 1..100");
   if (!(opt.cheb_tol > 0.0) || opt.cheb_tol >= 1.0)
@@ -1058,7 +1068,9 @@ mqw_status mqw_plan_create(mqw_ctx* ctx, int count, const int* n, const int* m,
   P->ctx = ctx;
   P->opt = opt;
   P->count = count;
-  P->precision = opt.precision;
+  P->comp = opt.precision == MQW_FP32_COMPENSATED;
+  P->precision = P->comp ? MQW_FP32 : opt.precision;
+  P->opt.precision = P->precision;
   P->samples = opt.samples;
   P->n.assign(n, n + count);
   P->m.assign(m, m + count);
@@ -1082,8 +1094,9 @@ mqw_status mqw_plan_create(mqw_ctx* ctx, int count, const int* n, const int* m,
   std::vector<int> p_cnt(count);
   const int res_max =
       opt.resident_max_n < 0 ? 0
-      : opt.resident_max_n == 0 ? resident_max_n(opt.precision)
-      : std::min(opt.resident_max_n, resident_max_n(opt.precision));
+      : P->comp ? 5  // compensated sums live in the grid path (n >= 6)
+      : opt.resident_max_n == 0 ? resident_max_n(P->precision)
+      : std::min(opt.resident_max_n, resident_max_n(P->precision));
   int p_total = 0;
   std::vector<float> gam(MQW_MAX_M), st(MQW_MAX_M), times(MQW_MAX_M * MQW_SAMPLES);
   for (int k = 0; k < count; k++) {
@@ -1420,9 +1433,11 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
                         float scale, const void* psi, void* out) {
   mqw_status s = check_ctx(ctx);
   if (s != MQW_OK) return s;
-  if ((precision != MQW_FP32 && precision != MQW_FP64) || n < 6 || n > MQW_MAX_N ||
-      K < 1 || !coeffs || !hp || !psi || !out)
+  if ((precision != MQW_FP32 && precision != MQW_FP64 && precision != MQW_FP32_COMPENSATED) ||
+      n < 6 || n > MQW_MAX_N || K < 1 || !coeffs || !hp || !psi || !out)
     return fail(ctx, MQW_ERR_INVALID, "clenshaw: bad arguments (n must be in 6..30)");
+  const int comp = precision == MQW_FP32_COMPENSATED;
+  if (comp) precision = MQW_FP32;  // FP32 storage, compensated partner sums
   const size_t N = (size_t)1 << n;
   const size_t amp = precision == 0 ? 8 : 16;
   const PassGeomHost geo = pass_geom(precision, n);
@@ -1468,6 +1483,7 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
     W.r = r;
     W.K = K;
     W.psi_uniform = 0;
+    pp.comp = comp;
     CK(launch_pass(precision, pp, st));
   }
   CK(cudaMemcpyAsync(out, X, N * amp, cudaMemcpyDeviceToHost, st));

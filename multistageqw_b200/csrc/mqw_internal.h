@@ -143,6 +143,7 @@ struct PassParams {
                        // tiles of 2^12 and 2^13), 0: warp shuffles
   int tma;             // 1: the tile's b, P, psi and D arrive by bulk copies
                        // (TMA) on an mbarrier, FP32 single-CTA tiles
+  int comp;            // 1: compensated partner sums (FP32-compensated mode)
   int tiling;          // 1 or 2
   int count;
   unsigned* err;       // device error word (bit 0: a bounded wait gave up)

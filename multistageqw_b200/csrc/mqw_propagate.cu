@@ -390,29 +390,60 @@ __device__ __forceinline__ void tile_barrier() {
 // (exchange tile sx in shared memory), and bits above index the thread's own
 // registers v[]. Every loop is unrolled at compile time; [q0, q1) only
 // predicates whole axes.
+// Accumulator of an amplitude pair's bit-flip partners. Plain: packed adds.
+// Compensated (FP32, COMP): each component is a TwoSum (Knuth's error-free
+// addition) pair (s, e) whose error term e collects the rounding of every
+// addition, so the partner sum is accurate to about one rounding instead of
+// about sqrt(n) of them.
+template <typename R, bool COMP> struct PartnerSum {
+  Pair<R> acc = pzero<R>();
+  __device__ __forceinline__ void add(const Pair<R>& v) { padd(acc, v); }
+  __device__ __forceinline__ Pair<R> value() const { return acc; }
+};
+__device__ __forceinline__ void two_sum(float& s, float& e, float v) {
+  const float t = __fadd_rn(s, v);
+  const float bp = __fsub_rn(t, s);
+  e = __fadd_rn(e, __fadd_rn(__fsub_rn(s, __fsub_rn(t, bp)), __fsub_rn(v, bp)));
+  s = t;
+}
+template <> struct PartnerSum<float, true> {
+  V4<float> s{0.0f, 0.0f, 0.0f, 0.0f}, e{0.0f, 0.0f, 0.0f, 0.0f};
+  __device__ __forceinline__ void add(const Pair<float>& p) {
+    const V4<float> v = to4(p);
+    two_sum(s.x, e.x, v.x);
+    two_sum(s.y, e.y, v.y);
+    two_sum(s.z, e.z, v.z);
+    two_sum(s.w, e.w, v.w);
+  }
+  __device__ __forceinline__ Pair<float> value() const {
+    return from4(V4<float>{__fadd_rn(s.x, e.x), __fadd_rn(s.y, e.y), __fadd_rn(s.z, e.z),
+                           __fadd_rn(s.w, e.w)});
+  }
+};
+
 // LS: the lane axes are read from the exchange tile too (one 16-byte shared
 // load per partner pair instead of four 32-bit shuffles: the same bytes
 // through the shared-memory pipe, a quarter of the instructions).
-template <typename R, int LT, int LOGT, int RP, bool LS = false>
-__device__ __forceinline__ Pair<R> axis_sum(const Pair<R> (&v)[RP], int j,
-                                           const R* sx, int q0, int q1,
-                                           int tid) {
-  Pair<R> acc = pzero<R>();
-  if (q0 <= 0) padd(acc, pswap<R>(v[j]));
+template <typename R, int LT, int LOGT, int RP, bool LS = false, bool COMP = false>
+__device__ __forceinline__ PartnerSum<R, COMP> axis_sum(const Pair<R> (&v)[RP], int j,
+                                                       const R* sx, int q0, int q1,
+                                                       int tid) {
+  PartnerSum<R, COMP> acc;
+  if (q0 <= 0) acc.add(pswap<R>(v[j]));
   const int pp = tid | (j << LOGT);
 #pragma unroll
   for (int q = 1; q <= 5 && q < LT; q++)
     if (q >= q0 && q < q1) {
-      if constexpr (LS) padd(acc, pld(sx + 4 * (pp ^ (1 << (q - 1)))));
-      else padd(acc, pshfl(v[j], 1 << (q - 1)));
+      if constexpr (LS) acc.add(pld(sx + 4 * (pp ^ (1 << (q - 1)))));
+      else acc.add(pshfl(v[j], 1 << (q - 1)));
     }
 #pragma unroll
   for (int q = 6; q <= LOGT && q < LT; q++)
-    if (q >= q0 && q < q1) padd(acc, pld(sx + 4 * (pp ^ (1 << (q - 1)))));
+    if (q >= q0 && q < q1) acc.add(pld(sx + 4 * (pp ^ (1 << (q - 1)))));
 #pragma unroll
   for (int k = 0; (1 << k) < RP; k++) {
     const int q = LOGT + 1 + k;
-    if (q >= q0 && q < q1) padd(acc, v[j ^ (1 << k)]);
+    if (q >= q0 && q < q1) acc.add(v[j ^ (1 << k)]);
   }
   return acc;
 }
@@ -458,7 +489,10 @@ constexpr int pass_min_blocks() {
 // always staged in shared memory. T2 tiles (2^(LT-4) rows of 16 amplitudes)
 // keep the per-thread path: one bulk copy per 64-128 byte row measured 2.6x
 // slower than cp.async.
-template <typename R, int LT, int CL, int TB, bool LS = false, bool TMA = false>
+// COMP: the partner sums are compensated (PartnerSum<float, true>): the
+// FP32-compensated precision mode.
+template <typename R, int LT, int CL, int TB, bool LS = false, bool TMA = false,
+          bool COMP = false>
 __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
                                   pass_min_blocks<LT, TB, sizeof(R) == 4, CL>())
     pass_kernel(PassParams p) {
@@ -533,10 +567,10 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
       if (LT + k >= q0 && LT + k < q1) rv.v[k] = pld_cluster((const R*)nullptr, peer_sx[k] + off);
     return rv;
   };
-  auto cluster_add = [&](Pair<R>& acc, const Remote& rv, int q0, int q1) {
+  auto cluster_add = [&](PartnerSum<R, COMP>& acc, const Remote& rv, int q0, int q1) {
 #pragma unroll
     for (int k = 0; k < CL; k++)
-      if (LT + k >= q0 && LT + k < q1) padd(acc, rv.v[k]);
+      if (LT + k >= q0 && LT + k < q1) acc.add(rv.v[k]);
   };
 
   Pair<R> va[RP];  // b_{r+1}
@@ -623,7 +657,7 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
 #pragma unroll
     for (int j = 0; j < RP; j++) {
       const Remote rv = cluster_load(j, fb0, fb1);
-      Pair<R> accp = axis_sum<R, LT, LOGT, RP, LS>(va, j, sx, fb0, fb1, tid);
+      PartnerSum<R, COMP> accp = axis_sum<R, LT, LOGT, RP, LS, COMP>(va, j, sx, fb0, fb1, tid);
       cluster_add(accp, rv, fb0, fb1);
       const unsigned gi = g0 + j * gstride;
       for (int u0 = 0; u0 < nu; u0 += 4) {
@@ -633,9 +667,9 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
           if (u0 + u < nu) gv[u] = pld(bin + 2 * (size_t)(gi ^ (1u << (LL + u0 + u))));
 #pragma unroll
         for (int u = 0; u < 4; u++)
-          if (u0 + u < nu) padd(accp, gv[u]);
+          if (u0 + u < nu) accp.add(gv[u]);
       }
-      const V4<R> acc = to4(accp);
+      const V4<R> acc = to4(accp.value());
       V4<R> pr;
       if constexpr (kStageP) pr = ld4<R>(sp + 4 * (j * T + tid));
       else pr = to4(pv[kStageP ? 0 : j]);
@@ -668,9 +702,9 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
 #pragma unroll
   for (int j = 0; j < RP; j++) {
     const Remote rv = cluster_load(j, 0, LL);
-    Pair<R> accp = axis_sum<R, LT, LOGT, RP, LS>(vb, j, sx, 0, LT, tid);
+    PartnerSum<R, COMP> accp = axis_sum<R, LT, LOGT, RP, LS, COMP>(vb, j, sx, 0, LT, tid);
     cluster_add(accp, rv, 0, LL);
-    const V4<R> acc = to4(accp);
+    const V4<R> acc = to4(accp.value());
     const int o = j * T + tid;
     const V4<R> pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * o);
     const float2 d = sd[o];
@@ -951,17 +985,18 @@ PassGeomHost pass_geom(int precision, int n, int lmax, int threads, int lane_sme
 }
 
 namespace {
-template <typename R, int LT, int CL, int TB = kPassThreads, bool LS = false, bool TMA = false>
+template <typename R, int LT, int CL, int TB = kPassThreads, bool LS = false, bool TMA = false,
+          bool COMP = false>
 cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
   using S = PassShape<LT, TB>;
   static size_t configured = 0;
   const size_t smem = S::template smem<R, S::kStageP || TMA>();
   if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB, LS, TMA>,
+    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB, LS, TMA, COMP>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if (CL > 3) {
-      e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB, LS, TMA>,
+      e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB, LS, TMA, COMP>,
                                cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
       if (e != cudaSuccess) return e;
     }
@@ -969,7 +1004,7 @@ cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
   }
   const dim3 grid((unsigned)((size_t)1 << (p.n - LT)), p.count);
   if constexpr (CL == 0) {
-    pass_kernel<R, LT, 0, TB, LS, TMA><<<grid, S::kThreads, smem, stream>>>(p);
+    pass_kernel<R, LT, 0, TB, LS, TMA, COMP><<<grid, S::kThreads, smem, stream>>>(p);
     return cudaGetLastError();
   } else {
     cudaLaunchConfig_t cfg = {};
@@ -984,7 +1019,7 @@ cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
     attr[0].val.clusterDim.z = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, pass_kernel<R, LT, CL, TB, LS, TMA>, p);
+    return cudaLaunchKernelEx(&cfg, pass_kernel<R, LT, CL, TB, LS, TMA, COMP>, p);
   }
 }
 
@@ -1022,6 +1057,23 @@ cudaError_t launch_pass_cluster(const PassParams& p, cudaStream_t stream) {
 template <typename R>
 cudaError_t launch_pass_t(const PassParams& p, cudaStream_t stream) {
   constexpr int cap = sizeof(R) == 4 ? 12 : 11;
+  if constexpr (sizeof(R) == 4) {
+    if (p.comp) {  // compensated partner sums: the default shape only
+      if (p.C != 0 || p.threads == 256 || p.lane_smem || p.tma) return cudaErrorInvalidValue;
+      switch (p.L) {
+        case 6: return launch_pass_lt<R, 6, 0, kPassThreads, false, false, true>(p, stream);
+        case 7: return launch_pass_lt<R, 7, 0, kPassThreads, false, false, true>(p, stream);
+        case 8: return launch_pass_lt<R, 8, 0, kPassThreads, false, false, true>(p, stream);
+        case 9: return launch_pass_lt<R, 9, 0, kPassThreads, false, false, true>(p, stream);
+        case 10: return launch_pass_lt<R, 10, 0, kPassThreads, false, false, true>(p, stream);
+        case 11: return launch_pass_lt<R, 11, 0, kPassThreads, false, false, true>(p, stream);
+        case 12: return launch_pass_lt<R, 12, 0, kPassThreads, false, false, true>(p, stream);
+        default: return cudaErrorInvalidValue;
+      }
+    }
+  } else {
+    if (p.comp) return cudaErrorInvalidValue;
+  }
   if (p.C != 0 && p.L != cap) return cudaErrorInvalidValue;
   if (p.threads == 256 && p.L != cap) return cudaErrorInvalidValue;
   if (p.lane_smem && (sizeof(R) != 4 || p.C != 0 || p.L < cap)) return cudaErrorInvalidValue;

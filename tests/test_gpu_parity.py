@@ -303,3 +303,32 @@ def test_bounded_wait_reports_timeout_and_context_survives(ctx, orc, mqw):
     r = ctx.run_problems(14, 2, raw, samples=2, tma=1)
     o = orc.run_problems(14, 2, raw, 1, 2, "f64")
     assert abs(r["p"][0] - o["p"][0]) <= 1e-5
+
+
+@pytest.mark.parametrize("n", [14, 20])
+def test_compensated_fp32_is_closer_to_fp64(ctx, orc, n):
+    """FP32 with compensated partner sums against plain FP32: both within the
+    target of FP64, the compensated state closer to it."""
+    raw = orc.sk_instances(n, 1, 2700 + n)[0]
+    hp, _, info = ctx.build_diag(n, raw)
+    g, _, t, _ = mqw_schedule(n, raw)
+    N = 1 << n
+    onenorm = float(np.float32(np.float32(info.e_abs) + np.float32(g[1]) * np.float32(n)))
+    s = float(np.float32(np.float32(onenorm) * t[1, 7]))
+    c = orc.cheb_coeffs(s).astype(np.float32)
+    rng = np.random.default_rng(n)
+    psi = ((rng.standard_normal(N) + 1j * rng.standard_normal(N)) / np.sqrt(2 * N))
+    ref = ctx.clenshaw(n, c, hp, float(g[1]), onenorm, psi, "fp64")
+    e32 = np.linalg.norm(ctx.clenshaw(n, c, hp, float(g[1]), onenorm, psi, "fp32") - ref)
+    e32c = np.linalg.norm(ctx.clenshaw(n, c, hp, float(g[1]), onenorm, psi, "fp32c") - ref)
+    nr = np.linalg.norm(ref)
+    assert e32 / nr < 2e-5 and e32c / nr < 2e-5
+    assert e32c < e32
+    r = ctx.run_problems(n, 3, raw, samples=4, precision="fp32c", graph=0)
+    r64 = ctx.run_problems(n, 3, raw, samples=4, precision="fp64", graph=0)
+    assert abs(r["p"][0] - r64["p"][0]) <= 1e-5
+
+
+def mqw_schedule(n, raw):
+    import multistageqw_b200 as M
+    return M.schedule(n, 3, raw)
