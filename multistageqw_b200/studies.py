@@ -6,10 +6,12 @@ arithmetic, the ones that define E_loc). The kept draws either come as a
 list (a precomputed screen; every gap is re-checked here on the GPU) or are
 screened here on the GPU. On them:
 
-* the whole path in FP32 and in FP64 on the GPU (`samples` samples each):
-  per-instance |dP| and the ground-state index of both paths;
-* for `state_walks` walks, the state after every stage in FP32 and FP64
-  (stage by stage through mqw_clenshaw): relative L2 error per stage;
+* the whole path in FP32, in FP32 with compensated partner sums and in FP64
+  on the GPU (`samples` samples each): per-instance |dP| and the
+  ground-state index of the paths;
+* for `state_walks` walks, the state after every stage in FP32, compensated
+  FP32 and FP64 (stage by stage through mqw_clenshaw): relative L2 error per
+  stage;
 * the Chebyshev degree per stage (mean over samples);
 * instances whose gap is below 1e-4 are flagged (there the reference's
   float-increment energies could order the two lowest states differently
@@ -63,7 +65,7 @@ def stage_states(ctx: Context, n: int, m: int, raw, sample: int, precision: str)
     hp, _, info = ctx.build_diag(n, raw)
     g, _, times, _ = schedule(n, m, raw)
     N = 1 << n
-    cdt = np.complex64 if precision == "fp32" else np.complex128
+    cdt = np.complex128 if precision == "fp64" else np.complex64
     psi = np.full(N, np.float32(1.0 / np.sqrt(N)), dtype=cdt)
     out, degrees = [], []
     for i in range(m):
@@ -89,9 +91,13 @@ def precision_study(n: int = 24, m: int = 4, count: int = 32, gap_max: float = 1
     r32 = ctx.run_problems(n, m, raws, samples=samples, precision="fp32")
     t32 = time.time() - t0
     t0 = time.time()
+    r32c = ctx.run_problems(n, m, raws, samples=samples, precision="fp32c")
+    t32c = time.time() - t0
+    t0 = time.time()
     r64 = ctx.run_problems(n, m, raws, samples=samples, precision="fp64")
     t64 = time.time() - t0
     dP = np.abs(r32["p"] - r64["p"])
+    dPc = np.abs(r32c["p"] - r64["p"])
     # Degrees per stage (the same rule the GPU applies), mean over samples.
     deg = np.zeros((len(kept), m))
     for k, inst in enumerate(kept):
@@ -104,10 +110,13 @@ def precision_study(n: int = 24, m: int = 4, count: int = 32, gap_max: float = 1
     state_err = []
     for w in range(min(state_walks, len(kept))):
         s32, _, eloc = stage_states(ctx, n, m, kept[w]["raw"], 0, "fp32")
+        s32c, _, _ = stage_states(ctx, n, m, kept[w]["raw"], 0, "fp32c")
         s64, _, _ = stage_states(ctx, n, m, kept[w]["raw"], 0, "fp64")
         state_err.append({
             "instance": w,
             "rel_l2_per_stage": [float(np.linalg.norm(a - b) / np.linalg.norm(b)) for a, b in zip(s32, s64)],
+            "rel_l2_per_stage_compensated": [float(np.linalg.norm(a - b) / np.linalg.norm(b))
+                                             for a, b in zip(s32c, s64)],
             "dP_sample0": float(abs(abs(s32[-1][eloc]) ** 2 - abs(s64[-1][eloc]) ** 2)),
         })
     ctx.close()
@@ -120,6 +129,8 @@ def precision_study(n: int = 24, m: int = 4, count: int = 32, gap_max: float = 1
         "gaps": [k["gap"] for k in kept],
         "gaps_below_1e-4": int(sum(k["gap"] < 1e-4 for k in kept)),
         "max_abs_dP": float(dP.max()), "mean_abs_dP": float(dP.mean()),
+        "max_abs_dP_compensated": float(dPc.max()), "mean_abs_dP_compensated": float(dPc.mean()),
+        "seconds_fp32_compensated": t32c,
         "p_fp32_mean": float(r32["p"].mean()), "p_fp64_mean": float(r64["p"].mean()),
         "e_loc_fp32_equals_fp64": bool(np.array_equal(r32["e_loc"], r64["e_loc"])),
         "degree_per_stage_mean": deg.mean(axis=0).tolist(),
