@@ -42,15 +42,14 @@ sys.path.insert(0, ROOT)
 
 METRIC = ("instances/s at n=20,m=4 (|ΔP|≤1e-5 vs FP64); "
           "mean P_gs learned vs heuristic")
-BYTES_PER_TERM_AMP = {"fp32": 36, "fp64": 72}  # algorithmic, see DESIGN.md
+BYTES_PER_TERM_AMP = {"fp32": 36, "fp32c": 36, "fp64": 72}  # algorithmic bytes per term·amp
 PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # DRAM bytes (read + write) per term·amp of one pass_kernel launch from an
 # ncu capture of the workload (cold caches: ncu flushes them between
-# replays), keyed by config.workload: profiles/pass_kernel_sk_n20_m4.md
-# (29.40 MB per 2^20-amplitude launch) and profiles/pass_kernel_sk_n24_global.md
-# (469.8 + 233.0 MB per 2^24-amplitude launch); for n = 28 the same pass
-# shape captured on an n = 26 walk, per amplitude (2373.8 MB per 2^26-amplitude
-# first-stage launch, profiles/launches_sk_n28_m3.md).
+# replays), keyed by config.workload: n = 20, 29.40 MB per 2^20-amplitude
+# launch; n = 24 (tile 2^11, 6 global axes), 469.8 + 233.0 MB per
+# 2^24-amplitude launch; n = 28, the same pass shape captured on an n = 26
+# walk, 2373.8 MB per 2^26-amplitude first-stage launch, per amplitude.
 DRAM_BYTES_PER_TERM_AMP = {"sk_n20_m4": 29.40e6 / 2**20, "sk_n24_m4": 702.8e6 / 2**24,
                            "sk_n28_m3_seed7": 2373.8e6 / 2**26}
 # Host memory the CPU legs may use at once (all worker processes together).
@@ -69,10 +68,13 @@ def parse():
     ap.add_argument("--m", type=int, default=4)
     ap.add_argument("--batch", type=int, default=2, help="instances per step per GPU")
     ap.add_argument("--samples", type=int, default=100)
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "fp32c"])
     ap.add_argument("--group", type=int, default=0, help="walks per launch (0: autotuned)")
     ap.add_argument("--tile-log", type=int, default=0, help="grid-path tile cap (0: autotuned)")
     ap.add_argument("--lanes", type=int, default=0, help="concurrent launch lanes (0: autotuned)")
+    ap.add_argument("--threads", type=int, default=0, help="CTA threads 512/256 (0: autotuned)")
+    ap.add_argument("--lane-smem", type=int, default=0, help="lane axes: 1 shared memory, -1 shuffles")
+    ap.add_argument("--tma", type=int, default=0, help="tile staging: 1 bulk copies, -1 cp.async")
     ap.add_argument("--seed", type=int, default=20)
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 |dP| check")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -386,7 +388,8 @@ def main():
     torch.cuda.set_stream(stream)
     ns, ms, raw, desc = make_batch(M, a, rank)
     count = len(ns)
-    shape = dict(group=a.group, tile_log=a.tile_log, lanes=a.lanes)
+    shape = dict(group=a.group, tile_log=a.tile_log, lanes=a.lanes, threads=a.threads,
+                 lane_smem=a.lane_smem, tma=a.tma)
     plan = M.Plan(ctx, ns, ms, raw, samples=a.samples, precision=a.precision, **shape)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
@@ -447,7 +450,7 @@ def main():
     # |dP| of the timed FP32 results against the FP64 path (first instance).
     check = None
     res = plan.results()
-    if not a.no_check and a.precision == "fp32":
+    if not a.no_check and a.precision != "fp64":
         n0, m0 = ns[0], ms[0]
         per0 = n0 * (n0 + 1) // 2
         r64 = M.Plan(ctx, [n0], [m0], raw[:per0], samples=a.samples, precision="fp64", graph=0)
@@ -487,7 +490,7 @@ def main():
             except Exception as ex:  # the baseline is reported, not required
                 cpu = {"value": None, "error": str(ex)}
         config = dict(desc)
-        if not (a.group or a.tile_log or a.lanes):
+        if not (a.group or a.tile_log or a.lanes or a.threads or a.lane_smem or a.tma):
             config["grid_shape"] = ctx.grid_shape(max(ns), a.precision)
         config["reference_term_amps_per_step"] = term_amps / a.steps
         config["pass_term_amps_per_step"] = pass_amps / a.steps
@@ -500,7 +503,7 @@ def main():
             "metric": METRIC, "value": value, "unit": "instances/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32" if a.precision == "fp32" else "f64",
+            "dtype": "f64" if a.precision == "fp64" else "f32",
             "data": "synthetic seeded SK instances (J,h ~ N(0,1)); reference datasets not used",
             "config": config,
             "e2e": {"value": e2e_val, "unit": "instances/s", "h2d_bytes_per_step": h2d,

@@ -810,6 +810,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       gs.lane_smem = -1;
       gs.tma = -1;
       gs.lmax = std::min(gs.lmax, 12);
+      if (pass_geom(P.precision, n, gs.lmax).C > 0) gs.lmax = 11;  // single-CTA tiles
     }
     gs.group = std::min(std::min(gs.group, kMaxGroup), kv.second);
     const int ngroups = (kv.second + gs.group - 1) / gs.group;
@@ -1440,7 +1441,10 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
   if (comp) precision = MQW_FP32;  // FP32 storage, compensated partner sums
   const size_t N = (size_t)1 << n;
   const size_t amp = precision == 0 ? 8 : 16;
-  const PassGeomHost geo = pass_geom(precision, n);
+  PassGeomHost geo = pass_geom(precision, n);
+  // Tiles spread over a cluster measured slower than one narrower tile with
+  // the remaining axes read from global memory; use the latter.
+  if (geo.C > 0) geo = pass_geom(precision, n, geo.L - 1);
   const int tiles = (int)(N >> geo.L);
   DevMem d_st, d_hp, d_c, d_np;
   CK(d_st.ensure(4 * N * amp));

@@ -305,7 +305,7 @@ def test_bounded_wait_reports_timeout_and_context_survives(ctx, orc, mqw):
     assert abs(r["p"][0] - o["p"][0]) <= 1e-5
 
 
-@pytest.mark.parametrize("n", [14, 20])
+@pytest.mark.parametrize("n", [14, 20, 22])
 def test_compensated_fp32_is_closer_to_fp64(ctx, orc, n):
     """FP32 with compensated partner sums against plain FP32: both within the
     target of FP64, the compensated state closer to it."""
