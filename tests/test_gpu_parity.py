@@ -332,3 +332,27 @@ def test_compensated_fp32_is_closer_to_fp64(ctx, orc, n):
 def mqw_schedule(n, raw):
     import multistageqw_b200 as M
     return M.schedule(n, 3, raw)
+
+
+def test_stage_scale_with_mixed_m(ctx, orc, mqw):
+    """Per-stage (gamma, t) multipliers laid out instance after instance for a
+    batch of different m: each instance gets its own, as when run alone."""
+    ns, ms = [12, 14, 12], [2, 4, 3]
+    raws = [orc.sk_instances(n, 1, 3100 + i)[0] for i, n in enumerate(ns)]
+    rng = np.random.default_rng(5)
+    scales = [rng.uniform(0.7, 1.4, (m, 2)).astype(np.float32) for m in ms]
+    plan = mqw.Plan(ctx, ns, ms, np.concatenate(raws), samples=5,
+                    stage_scale=np.concatenate(scales).ravel(), graph=0)
+    plan.execute()
+    p = plan.results()["p"]
+    plan.close()
+    for i, (n, m) in enumerate(zip(ns, ms)):
+        r = ctx.run_problems(n, m, raws[i][None, :], samples=5, stage_scale=scales[i].ravel())
+        assert abs(p[i] - r["p"][0]) <= 1e-6, i
+
+
+def test_grid_shape_query(ctx):
+    g = ctx.grid_shape(18)
+    assert 6 <= g["tile_log"] <= 13 and g["group"] >= 1 and g["lanes"] >= 1
+    assert g["threads"] in (256, 512) and g["us_per_walk_pass"] > 0
+    assert ctx.grid_shape(18) == g  # cached per context
