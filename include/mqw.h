@@ -87,6 +87,11 @@ typedef struct mqw_options {
                        Chebyshev basis for their first stage (built once,
                        recombined per walk); 0: every walk runs its own
                        first-stage recurrence */
+  int final_projection; /* 1 (default): FP32 walks of an instance get their
+                       last-stage P by projection onto one basis built from
+                       e_{E_loc} (the output norm is taken as the input norm,
+                       exact up to the 1e-6 Chebyshev tail); 0: every walk
+                       runs its own last-stage recurrence */
 } mqw_options;
 
 typedef struct mqw_diag_info {

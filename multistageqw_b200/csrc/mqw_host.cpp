@@ -84,7 +84,8 @@ struct mqw_ctx {
   // Device error word: kernels whose bounded waits give up set bit 0; the
   // host reads and clears it when it collects results.
   DevMem dev_err;
-  DevMem basis;  // stage-1 basis of the instance in flight (+ its partial P)
+  DevMem basis;      // shared bases of the instance in flight (+ their slots)
+  DevMem proj_part;  // last-stage projection partial dots, per lane
   // Bumped whenever a shared scratch buffer is reallocated: a plan's captured
   // graph holds the old addresses and is re-captured when this changes.
   unsigned long long scratch_gen = 1;
@@ -178,6 +179,7 @@ void default_opts(mqw_options* o) {
   o->lane_smem = 0;
   o->tma = 0;
   o->stage1_basis = 1;
+  o->final_projection = 1;
 }
 
 }  // namespace
@@ -208,9 +210,10 @@ struct mqw_plan {
   DevMem d_coef, d_coef_off, d_stages, d_walks;
   // Grid-path shape chosen for each n of the plan.
   std::map<int, GridShape> grid_geo;
-  // Stage-1 basis: vectors per instance (0 = not used for that n) and the
-  // unit coefficient list the basis passes read ([0, ..., 0, 1]).
-  std::map<int, int> basis_kb;
+  // Shared bases per n: vectors of the stage-1 and the last-stage basis
+  // (0 = not used for that n), and the unit coefficient list the basis passes
+  // read ([0, ..., 0, 1]).
+  std::map<int, int> basis_kb1, basis_kb2;
   DevMem d_unit;
   int unit_len = 0;
   // CUDA graph of the whole device pipeline, replayed by later executes.
@@ -471,10 +474,14 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
 // `lane` selects the lane's own slice of the shared scratch (state, norm
 // partials, kappa), sized for groups of `gmax` walks.
 // With `basis` set (the instance's stage-1 basis of Kb vectors), the first
-// stage is recombined from it instead of run as a recurrence per walk.
+// stage is recombined from it instead of run as a recurrence per walk; with
+// `last` set (the last-stage basis of Kl vectors from e_{E_loc}), the last
+// stage is a projection onto it that yields P directly. `proj` is the lane's
+// projection scratch.
 mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
                           const PassGeomHost& geo, int lane, int gmax,
-                          const void* basis, int Kb, cudaStream_t stream) {
+                          const float* basis, int Kb, const float* last, int Kl,
+                          double* proj, cudaStream_t stream) {
   mqw_ctx* ctx = P.ctx;
   const int n = P.walks[widx[0]].n;
   const size_t N = (size_t)1 << n;
@@ -507,6 +514,28 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
       const ResidentWalk& w = P.walks[widx[g]];
       K[g] = st < w.stages ? P.degree[w.stage_desc_off + st] : 0;
       Kmax = std::max(Kmax, K[g]);
+    }
+    if (last && st == max_stages - 1 && st > 0) {
+      ProjectParams pr{};
+      pr.basis = last;
+      pr.n = n;
+      pr.L = geo.L;
+      pr.Kb = Kl;
+      pr.count = G;
+      pr.part = proj;
+      for (int g = 0; g < G; g++) {
+        const ResidentWalk& w = P.walks[widx[g]];
+        const int job = w.stage_desc_off + st;
+        ProjectWalk& Q = pr.walk[g];
+        Q.coef = coef + P.coef_off[job];
+        Q.K = K[g];
+        Q.psi = buf(g, pi[g]);
+        Q.kappa = kappa + g;
+        Q.p_out = p_sample + w.p_off;
+      }
+      CK(launch_project(pr, stream));
+      if (P.counting) P.stats.launches += 2;
+      break;  // the walks' P are written; nothing follows the last stage
     }
     if (st == 0 && basis) {
       CombineParams cp{};
@@ -598,23 +627,43 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
   return MQW_OK;
 }
 
-// Builds the stage-1 basis w_0 .. w_{Kb-1} of the instance of walk w0 into
-// ctx->basis (slot 0 holds the passes' partial P, slot 1 + j holds w_j as a
-// complex vector; their real parts then go to the real basis that follows
-// the Kb_cap + 1 complex slots, where the recombination reads them):
-// Kb single-walk passes with c = [0, .., 0, 1] at an even top index R >= Kb,
-// so that b_R = psi0 and every later pass is b_r = 2 H~ b_{r+1} - b_{r+2};
-// the passes stop at r = R - Kb + 1 >= 1 (the r = 0 form is never used).
-mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int Kb, int kb_cap,
-                       const PassGeomHost& geo, void** real_out, cudaStream_t stream) {
+// Layout of ctx->basis for one n (FP32): four complex slots — the basis
+// passes' partial P, the recurrence vector b (two when axes are read from
+// global memory), the start vector e_{E_loc} — then the real stage-1 basis
+// (kb1 vectors) and the real last-stage basis (kb2 vectors).
+struct BasisLayout {
+  char* base;
+  size_t N;
+  int kb1, kb2;
+  void* slot(int k) const { return base + (size_t)k * N * 8; }
+  float* real1() const { return reinterpret_cast<float*>(base + 4 * N * 8); }
+  float* real2() const { return real1() + (size_t)kb1 * N; }
+  static size_t bytes(int n, int kb1, int kb2) {
+    const size_t N = (size_t)1 << n;
+    return 4 * N * 8 + (size_t)(kb1 + kb2) * N * 4;
+  }
+};
+
+// Builds the real basis w_j = U_j(H~) v, j < Kb, of stage `stage` of the
+// instance of walk w0 into `real` (Kb vectors of 2^n floats): v is the
+// uniform state for the first stage and e_{E_loc} for the last. Kb
+// single-walk passes with c = [0, .., 0, 1] at an even top index R >= Kb, so
+// that b_R = v and every later pass is b_r = 2 H~ b_{r+1} - b_{r+2}; each
+// pass also stores Re(b_r) as w_j (the imaginary parts stay 0). The passes
+// stop at r = R - Kb + 1 >= 1 (the r = 0 form is never used).
+mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
+                       const BasisLayout& B, const PassGeomHost& geo, float* real,
+                       cudaStream_t stream) {
   mqw_ctx* ctx = P.ctx;
   const int n = w0.n;
   const size_t N = (size_t)1 << n;
-  const size_t amp = P.precision == 0 ? 8 : 16;
-  char* base = ctx->basis.as<char>();
-  auto slot = [&](int k) -> void* { return base + (size_t)k * N * amp; };
+  const bool from_eloc = stage > 0;
+  if (from_eloc) {
+    CK(launch_unit_eloc(B.slot(3), n, P.d_diag.as<DiagOut>() + w0.inst, stream));
+    if (P.counting) P.stats.launches++;
+  }
   const int R = Kb + (Kb & 1);
-  const int job = w0.stage_desc_off;
+  const int job = w0.stage_desc_off + stage;
   const float* unit = P.d_unit.as<float>() + (P.unit_len - 1 - R);
   for (int j = 0; j < Kb; j++) {
     PassParams pp{};
@@ -630,10 +679,14 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int Kb, int kb_cap,
     pp.count = 1;
     PassWalk& W = pp.walk[0];
     W.active = 1;
-    W.bin = slot(j == 0 ? 1 : j);  // not read by the first pass
-    W.bout = slot(1 + j);
-    W.part = slot(0);
-    W.psi = slot(1);  // not read: the uniform state
+    if (geo.nu == 0) {
+      W.bin = W.bout = B.slot(1);  // in place
+    } else {
+      W.bin = B.slot(1 + ((j + 1) & 1));  // not read by the first pass
+      W.bout = B.slot(1 + (j & 1));
+    }
+    W.part = B.slot(0);
+    W.psi = B.slot(3);  // read only for e_{E_loc}
     W.hp = P.d_hp.as<float>() + w0.hp_off;
     W.coef = unit;
     W.kappa = nullptr;
@@ -642,8 +695,9 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int Kb, int kb_cap,
     W.scale = P.onenorm[job];
     W.r = R - j;
     W.K = R + 1;
-    W.psi_uniform = 1;
+    W.psi_uniform = from_eloc ? 0 : 1;
     W.psi0 = (float)(1.0 / std::sqrt((double)N));
+    W.real_out = real + (size_t)j * N;
     CK(launch_pass(P.precision, pp, stream));
     if (P.counting) {
       P.stats.launches++;
@@ -651,10 +705,6 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int Kb, int kb_cap,
       P.stats.pass_amps += (double)N;
     }
   }
-  void* real = base + (size_t)(kb_cap + 1) * N * amp;
-  CK(launch_basis_real(slot(1), real, n, Kb, stream));
-  if (P.counting) P.stats.launches++;
-  *real_out = real;
   return MQW_OK;
 }
 
@@ -713,26 +763,35 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
     const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, gs.tma > 0);
     const int G = gs.group;
     const std::vector<int>& ws = kv.second;
-    const int kb_cap = P.basis_kb.count(n) ? P.basis_kb.at(n) : 0;
-    // Blocks of walks: one block per instance when the stage-1 basis is used
-    // (the basis is built before, and read during, the block), else all.
+    const int kb1 = P.basis_kb1.count(n) ? P.basis_kb1.at(n) : 0;
+    const int kb2 = P.basis_kb2.count(n) ? P.basis_kb2.at(n) : 0;
+    const BasisLayout B{ctx->basis.as<char>(), (size_t)1 << n, kb1, kb2};
+    // Blocks of walks: one block per instance when a shared basis is used
+    // (the bases are built before, and read during, the block), else all.
     size_t b0 = 0;
     while (b0 < ws.size()) {
       size_t b1 = ws.size();
-      const void* basis = nullptr;
-      int Kb = 0;
-      if (kb_cap > 0) {
+      const float* basis = nullptr;
+      const float* lastb = nullptr;
+      int Kb = 0, Kl = 0;
+      if (kb1 > 0 || kb2 > 0) {
         b1 = b0;
         while (b1 < ws.size() && P.walks[ws[b1]].inst == P.walks[ws[b0]].inst) b1++;
         const ResidentWalk& w0 = P.walks[ws[b0]];
         if (!w0.record_each && w0.stages >= 2) {
-          for (size_t k = b0; k < b1; k++)
+          for (size_t k = b0; k < b1; k++) {
             Kb = std::max(Kb, P.degree[P.walks[ws[k]].stage_desc_off]);
-          if (Kb <= kb_cap) {
-            void* real = nullptr;
-            mqw_status s = issue_basis(P, w0, Kb, kb_cap, geo, &real, stream);
+            Kl = std::max(Kl, P.degree[P.walks[ws[k]].stage_desc_off + w0.stages - 1]);
+          }
+          if (kb1 > 0 && Kb <= kb1) {
+            mqw_status s = issue_basis(P, w0, 0, Kb, B, geo, B.real1(), stream);
             if (s != MQW_OK) return s;
-            basis = real;
+            basis = B.real1();
+          }
+          if (kb2 > 0 && Kl <= kb2) {
+            mqw_status s = issue_basis(P, w0, w0.stages - 1, Kl, B, geo, B.real2(), stream);
+            if (s != MQW_OK) return s;
+            lastb = B.real2();
           }
         }
       }
@@ -745,7 +804,10 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
         const size_t a = b0 + (size_t)i * G;
         std::vector<int> grp(ws.begin() + a, ws.begin() + std::min(b1, a + G));
         const int lane = i % lanes;
-        mqw_status s = run_grid_group(P, grp, geo, lane, G, basis, basis ? Kb : 0,
+        double* proj = ctx->proj_part.as<double>() +
+                       (size_t)lane * G * std::max(kb2, 1) * (((size_t)1 << n) >> geo.L) * 2;
+        mqw_status s = run_grid_group(P, grp, geo, lane, G, basis, basis ? Kb : 0, lastb,
+                                      lastb ? Kl : 0, proj,
                                       lane == 0 ? stream : ctx->lane_stream[lane]);
         if (s != MQW_OK) return s;
       }
@@ -867,33 +929,48 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
                            (double)(1u << P.walks[w].n);
     if (!P.walk_is_grid[w]) res.push_back(P.walks[w]);
   }
-  // Stage-1 basis: the largest first-stage degree per n decides the buffer;
-  // an n whose basis would not fit the budget runs without it.
-  P.basis_kb.clear();
-  if (P.opt.stage1_basis && P.precision == 0 && !P.comp) {
+  // Shared bases (FP32): the largest first- and last-stage degrees per n
+  // decide the buffers; an n whose bases would not fit the budget drops the
+  // last-stage basis first, then the stage-1 basis. The last-stage
+  // projection needs tiles of at least 2^10 amplitudes.
+  P.basis_kb1.clear();
+  P.basis_kb2.clear();
+  const bool want1 = P.opt.stage1_basis && P.precision == 0 && !P.comp;
+  const bool want2 = P.opt.final_projection && P.precision == 0 && !P.comp;
+  if (want1 || want2) {
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)8 << 30;
-    const size_t budget = std::min(free_b / 4, (size_t)8 << 30);
-    std::map<int, int> kb;
+    const size_t budget = std::min(free_b / 4, (size_t)16 << 30);
+    std::map<int, std::pair<int, int>> kb;
     for (size_t w = 0; w < P.walks.size(); w++) {
       const ResidentWalk& wk = P.walks[w];
       if (!P.walk_is_grid[w] || wk.record_each || wk.stages < 2) continue;
-      int& k = kb[wk.n];
-      k = std::max(k, P.degree[wk.stage_desc_off]);
+      auto& k = kb[wk.n];
+      k.first = std::max(k.first, P.degree[wk.stage_desc_off]);
+      k.second = std::max(k.second, P.degree[wk.stage_desc_off + wk.stages - 1]);
     }
-    size_t basis_b = 0;
+    size_t basis_b = 0, proj_b = 0;
     int rmax = 0;
     for (auto& e : kb) {
-      // Kb + 1 complex slots (P and the basis) and the real basis.
-      const size_t bytes = (size_t)(e.second + 1) * ((size_t)1 << e.first) * 8 +
-                           (size_t)e.second * ((size_t)1 << e.first) * 4;
-      if (e.second > kMaxBasis || bytes > budget) continue;
-      P.basis_kb[e.first] = e.second;
-      basis_b = std::max(basis_b, bytes);
-      rmax = std::max(rmax, e.second + (e.second & 1));
+      const int n = e.first;
+      const GridShape& gs = P.grid_geo.at(n);
+      const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads,
+                                         gs.lane_smem > 0, gs.tma > 0);
+      int k1 = want1 && e.second.first <= kMaxBasis ? e.second.first : 0;
+      int k2 = want2 && geo.L >= 10 && e.second.second <= kMaxBasis ? e.second.second : 0;
+      if (BasisLayout::bytes(n, k1, k2) > budget) k2 = 0;
+      if (BasisLayout::bytes(n, k1, k2) > budget) k1 = 0;
+      if (!k1 && !k2) continue;
+      P.basis_kb1[n] = k1;
+      P.basis_kb2[n] = k2;
+      basis_b = std::max(basis_b, BasisLayout::bytes(n, k1, k2));
+      proj_b = std::max(proj_b, (size_t)gs.lanes * gs.group * std::max(k2, 1) *
+                                    ((((size_t)1 << n) >> geo.L)) * 2 * sizeof(double));
+      rmax = std::max(rmax, std::max(k1 + (k1 & 1), k2 + (k2 & 1)));
     }
     if (basis_b) {
       CK(ctx->grow(ctx->basis, basis_b));
+      CK(ctx->grow(ctx->proj_part, proj_b));
       if (P.unit_len < rmax + 1) {
         std::vector<float> unit(rmax + 1, 0.0f);
         unit[rmax] = 1.0f;

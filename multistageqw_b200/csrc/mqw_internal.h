@@ -133,6 +133,8 @@ struct PassWalk {
   int psi_uniform;     // psi is the uniform state (psi0, 0): not read
   int active;
   float psi0;          // float(1/sqrt(2^n)), the uniform amplitude
+  float* real_out;     // basis passes (FP32): also store Re(b_r) here as a
+                       // real vector (nullptr: no)
 };
 struct PassParams {
   int n, L, a;
@@ -188,9 +190,30 @@ struct CombineParams {
   CombineWalk walk[kMaxGroup];
 };
 constexpr int kMaxBasis = 1024;  // basis vectors (stage-1 degree bound)
-// Real parts of Kb contiguous complex FP32 vectors of 2^n amplitudes.
-cudaError_t launch_basis_real(const void* cplx, void* real, int n, int Kb,
-                              cudaStream_t stream);
+// Last-stage projection. Only |psi_out[E_loc]|^2 of a walk's last stage is
+// used, and H~ is real symmetric, so
+//   psi_out[E_loc] = sum_k c_k (T_k(H~) psi)[E_loc] = sum_j d_j <w_j, psi>
+// with the basis w_j = U_j(H~) e_loc built once per instance (the same
+// pass_kernel recurrence started from the unit vector at E_loc) and d_j the
+// stage-1 recombination weights of the walk's last-stage coefficients. The
+// output norm is taken as the input norm: |f_K(x)| = 1 +- the 1e-6 tail on
+// [-1, 1], so P moves by at most 2e-6 relative.
+struct ProjectWalk {
+  const float* coef;   // the walk's last-stage coefficients c_0 .. c_{K-1}
+  int K;
+  const void* psi;     // last-stage input (interleaved complex, unnormalised)
+  const double* kappa; // 1/||psi||
+  double* p_out;       // receives |psi_out[E_loc]|^2 kappa^2
+};
+struct ProjectParams {
+  const float* basis;  // Kb real FP32 vectors of 2^n amplitudes
+  int n, L, Kb, count;
+  double* part;        // scratch: [2^(n-L) blocks][count][Kb][2] partial dots
+  ProjectWalk walk[kMaxGroup];
+};
+cudaError_t launch_project(const ProjectParams& p, cudaStream_t stream);
+// psi = the unit vector at E_loc of instance `inst` (complex FP32, 2^n).
+cudaError_t launch_unit_eloc(void* psi, int n, const DiagOut* diag, cudaStream_t stream);
 cudaError_t launch_combine(int precision, const CombineParams& p,
                            cudaStream_t stream);
 

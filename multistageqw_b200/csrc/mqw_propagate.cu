@@ -679,6 +679,15 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   }
 #pragma unroll
   for (int j = 0; j < RP; j++) pst(bout + 2 * (size_t)(g0 + j * gstride), vb[j]);
+  if constexpr (sizeof(R) == 4) {
+    if (W.real_out) {  // basis passes: the real parts as a real vector too
+#pragma unroll
+      for (int j = 0; j < RP; j++) {
+        const V4<R> v = to4(vb[j]);
+        *reinterpret_cast<float2*>(W.real_out + (g0 + j * gstride)) = make_float2(v.x, v.z);
+      }
+    }
+  }
   if (r == 0) {
     double nrm = 0.0;
 #pragma unroll
@@ -720,18 +729,6 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   }
   // A CTA's shared memory must outlive its peers' reads of it.
   if constexpr (CL > 0) cluster_barrier();
-}
-
-// The basis passes leave interleaved complex vectors with zero imaginary
-// parts; the recombination reads them as real vectors (half the bytes):
-// real[q] = amplitudes 4q .. 4q+3 of the contiguous complex basis.
-__global__ void basis_real_kernel(const float4* __restrict__ cplx, float4* __restrict__ real,
-                                  size_t quads) {
-  for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < quads;
-       q += (size_t)gridDim.x * blockDim.x) {
-    const float4 a = cplx[2 * q], b = cplx[2 * q + 1];
-    real[q] = make_float4(a.x, a.z, b.x, b.z);
-  }
 }
 
 // Stage-1 recombination of G walks (FP32): block b covers amplitudes
@@ -802,6 +799,133 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineParams p) {
     if (threadIdx.x == 0) p.walk[g].norm_part[blockIdx.x] = sum;
     __syncthreads();  // s_red is reused by the next walk's sum
   }
+}
+
+// Last-stage projection, partial dots: block b covers the 2^L amplitudes
+// [b 2^L, (b+1) 2^L) (2^L >= 1024); each thread holds 16 of them (4 quads)
+// of one walk's psi in registers and, eight basis vectors at a time,
+// accumulates w_j . psi (re, im) in FP64, reduces over the warp with
+// shuffles and leaves the warp's value in shared memory; the warps' values
+// are then summed in a fixed order into part[g][j][b]. The walks of a group
+// are done one after another over the same basis slice.
+constexpr int kProjThreads = 256;
+constexpr int kProjJ = 8;
+__global__ void __launch_bounds__(kProjThreads, 2) project_partial_kernel(ProjectParams p) {
+  constexpr int kWarps = kProjThreads / 32;
+  __shared__ double red[kWarps][kProjJ][2];
+  const int Kb = p.Kb, G = p.count;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const size_t N = (size_t)1 << p.n;
+  const size_t chunk = (size_t)1 << p.L;  // multiple of 4 * kProjThreads (L >= 10)
+  const int nq = (int)(chunk / (4 * kProjThreads));
+  const size_t base = (size_t)blockIdx.x * chunk;
+  const size_t tiles = N >> p.L;
+  for (int g = 0; g < G; g++) {
+    const float* psi = reinterpret_cast<const float*>(p.walk[g].psi);
+    for (int q0 = 0; q0 < nq; q0 += 4) {  // 16 amplitudes per thread per round
+      float4 ps[4][2];
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const size_t i = base + 4 * threadIdx.x + (size_t)(q0 + q) * 4 * kProjThreads;
+        const bool in = q0 + q < nq;
+        ps[q][0] = in ? __ldg(reinterpret_cast<const float4*>(psi + 2 * i)) : make_float4(0, 0, 0, 0);
+        ps[q][1] = in ? __ldg(reinterpret_cast<const float4*>(psi + 2 * i + 4)) : make_float4(0, 0, 0, 0);
+      }
+      for (int j0 = 0; j0 < Kb; j0 += kProjJ) {
+        double acc[kProjJ][2];
+#pragma unroll
+        for (int jj = 0; jj < kProjJ; jj++) acc[jj][0] = acc[jj][1] = 0.0;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          if (q0 + q >= nq) break;
+          const size_t i = base + 4 * threadIdx.x + (size_t)(q0 + q) * 4 * kProjThreads;
+          float4 w[kProjJ];
+#pragma unroll
+          for (int jj = 0; jj < kProjJ; jj++)
+            w[jj] = j0 + jj < Kb ? __ldg(reinterpret_cast<const float4*>(p.basis + (size_t)(j0 + jj) * N + i))
+                                 : make_float4(0, 0, 0, 0);
+          const float4 a = ps[q][0], b = ps[q][1];
+#pragma unroll
+          for (int jj = 0; jj < kProjJ; jj++) {
+            acc[jj][0] = fma((double)w[jj].x, (double)a.x, acc[jj][0]);
+            acc[jj][1] = fma((double)w[jj].x, (double)a.y, acc[jj][1]);
+            acc[jj][0] = fma((double)w[jj].y, (double)a.z, acc[jj][0]);
+            acc[jj][1] = fma((double)w[jj].y, (double)a.w, acc[jj][1]);
+            acc[jj][0] = fma((double)w[jj].z, (double)b.x, acc[jj][0]);
+            acc[jj][1] = fma((double)w[jj].z, (double)b.y, acc[jj][1]);
+            acc[jj][0] = fma((double)w[jj].w, (double)b.z, acc[jj][0]);
+            acc[jj][1] = fma((double)w[jj].w, (double)b.w, acc[jj][1]);
+          }
+        }
+#pragma unroll
+        for (int jj = 0; jj < kProjJ; jj++)
+#pragma unroll
+          for (int c = 0; c < 2; c++) {
+            double v = acc[jj][c];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if (lane == 0) red[warp][jj][c] = v;
+          }
+        __syncthreads();
+        if (threadIdx.x < 2 * kProjJ) {
+          const int jj = threadIdx.x >> 1, c = threadIdx.x & 1;
+          if (j0 + jj < Kb) {
+            double v = 0.0;
+            for (int k = 0; k < kWarps; k++) v += red[k][jj][c];
+            double* dst = p.part + ((((size_t)g * Kb) + j0 + jj) * tiles + blockIdx.x) * 2 + c;
+            *dst = q0 == 0 ? v : *dst + v;  // rounds of 16 amplitudes in order
+          }
+        }
+        __syncthreads();
+      }
+    }
+  }
+}
+
+// Last-stage projection, final: one block per walk sums its part[][j] over the
+// blocks (fixed order), forms A = sum_j d_j z_j (d_j real for even j,
+// imaginary for odd j) and writes P = |A|^2 kappa^2.
+__global__ void project_final_kernel(ProjectParams p) {
+  const int g = blockIdx.x;
+  const ProjectWalk& W = p.walk[g];
+  const int Kb = p.Kb;
+  const size_t tiles = (size_t)1 << (p.n - p.L);
+  __shared__ double sre[256], sim[256];
+  double are = 0.0, aim = 0.0;
+  for (int j = threadIdx.x; j < Kb; j += blockDim.x) {
+    double zr = 0.0, zi = 0.0;
+    const double* pj = p.part + (((size_t)g * Kb) + j) * tiles * 2;
+    for (size_t b = 0; b < tiles; b++) {
+      zr += pj[2 * b];
+      zi += pj[2 * b + 1];
+    }
+    const double cj = j < W.K ? (double)W.coef[j] : 0.0;
+    const double cj2 = j + 2 < W.K ? (double)W.coef[j + 2] : 0.0;
+    const double d = j == 0 ? cj - 0.5 * cj2 : 0.5 * (cj - cj2);
+    if (j & 1) {  // i d z
+      are -= d * zi;
+      aim += d * zr;
+    } else {
+      are += d * zr;
+      aim += d * zi;
+    }
+  }
+  sre[threadIdx.x] = are;
+  sim[threadIdx.x] = aim;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = 0.0, i = 0.0;
+    for (int t = 0; t < (int)blockDim.x; t++) {
+      r += sre[t];
+      i += sim[t];
+    }
+    const double k = W.kappa ? *W.kappa : 1.0;
+    *W.p_out = (r * r + i * i) * k * k;
+  }
+}
+
+// psi = e_{E_loc} (complex FP32): the start vector of the last-stage basis.
+__global__ void unit_eloc_kernel(float2* psi, const DiagOut* diag) {
+  psi[diag->e_loc] = make_float2(1.0f, 0.0f);
 }
 
 template <typename R>
@@ -1125,17 +1249,6 @@ cudaError_t launch_pass(int precision, const PassParams& p,
                         : launch_pass_t<double>(p, stream);
 }
 
-cudaError_t launch_basis_real(const void* cplx, void* real, int n, int Kb,
-                              cudaStream_t stream) {
-  if (n < 2 || n > kMaxN || Kb < 1 || Kb > kMaxBasis || !cplx || !real) return cudaErrorInvalidValue;
-  const size_t quads = ((size_t)Kb << n) / 4;
-  const size_t want = (quads + 255) / 256;
-  const unsigned blocks = (unsigned)(want < 8192 ? want : 8192);
-  basis_real_kernel<<<blocks, 256, 0, stream>>>(reinterpret_cast<const float4*>(cplx),
-                                               reinterpret_cast<float4*>(real), quads);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_combine(int precision, const CombineParams& p,
                            cudaStream_t stream) {
   if (precision != 0 || p.n < 6 || p.n > kMaxN || p.L < 6 || p.L > p.n || p.Kb < 1 ||
@@ -1156,6 +1269,30 @@ cudaError_t launch_combine(int precision, const CombineParams& p,
     case 7: combine_kernel<7><<<blocks, 256, 0, stream>>>(p); break;
     default: combine_kernel<8><<<blocks, 256, 0, stream>>>(p); break;
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_project(const ProjectParams& p, cudaStream_t stream) {
+  if (p.n < 10 || p.n > kMaxN || p.L < 10 || p.L > p.n || p.Kb < 1 || p.Kb > kMaxBasis ||
+      p.count < 1 || p.count > kMaxGroup || !p.basis || !p.part)
+    return cudaErrorInvalidValue;
+  for (int g = 0; g < p.count; g++)
+    if (p.walk[g].K < 1 || p.walk[g].K > p.Kb || !p.walk[g].coef || !p.walk[g].psi ||
+        !p.walk[g].p_out)
+      return cudaErrorInvalidValue;
+  const unsigned blocks = (unsigned)((size_t)1 << (p.n - p.L));
+  project_partial_kernel<<<blocks, kProjThreads, 0, stream>>>(p);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  project_final_kernel<<<p.count, 256, 0, stream>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unit_eloc(void* psi, int n, const DiagOut* diag, cudaStream_t stream) {
+  if (n < 1 || n > kMaxN || !psi || !diag) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(psi, 0, ((size_t)1 << n) * sizeof(float2), stream);
+  if (e != cudaSuccess) return e;
+  unit_eloc_kernel<<<1, 1, 0, stream>>>(reinterpret_cast<float2*>(psi), diag);
   return cudaGetLastError();
 }
 

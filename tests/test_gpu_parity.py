@@ -356,3 +356,32 @@ def test_grid_shape_query(ctx):
     assert 6 <= g["tile_log"] <= 13 and g["group"] >= 1 and g["lanes"] >= 1
     assert g["threads"] in (256, 512) and g["us_per_walk_pass"] > 0
     assert ctx.grid_shape(18) == g  # cached per context
+
+
+@pytest.mark.parametrize("n,m", [(15, 2), (17, 3), (20, 4), (22, 3)])
+def test_final_projection_matches_per_walk_last_stage(ctx, orc, n, m):
+    """The last stage as a projection onto the basis built from e_{E_loc}
+    (output norm taken as the input norm) against every walk running its own
+    last-stage recurrence and against FP64: per-sample P within 2e-6
+    relative (the Chebyshev tail bound) plus FP32 rounding."""
+    raw = orc.sk_instances(n, 1, 3300 + n)
+    kw = dict(samples=8, graph=0)
+    on = ctx.run_problems(n, m, raw, precision="fp32", **kw)
+    off = ctx.run_problems(n, m, raw, precision="fp32", final_projection=0, **kw)
+    r64 = ctx.run_problems(n, m, raw, precision="fp64", **kw)
+    p_on, p_off = on["p"][0], off["p"][0]
+    assert abs(p_on - p_off) <= 2e-6 * p_off + 1e-8, (p_on, p_off)
+    assert abs(p_on - r64["p"][0]) <= 1e-5
+    assert on["stats"]["pass_amps"] < off["stats"]["pass_amps"]
+    plan = mqw_plan_samples(ctx, n, m, raw)
+    assert np.all(plan >= 0.0) and np.all(plan <= 1.0)
+
+
+def mqw_plan_samples(ctx, n, m, raw):
+    import multistageqw_b200 as M
+    plan = M.Plan(ctx, n, m, raw, samples=8)
+    plan.execute()
+    plan.execute()  # graph replay
+    ps = plan.results(per_sample=True)["p_sample"]
+    plan.close()
+    return ps
