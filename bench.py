@@ -430,6 +430,7 @@ def main():
     # End to end through the public API from pinned host buffers.
     raw_pinned = torch.from_numpy(np.ascontiguousarray(raw)).pin_memory().numpy()
     e2e_ms = []
+    e2e_parts = {"create_ms": 0.0, "execute_call_ms": 0.0, "results_ms": 0.0}
     h2d = d2h = 0.0
     for _ in range(max(1, min(a.steps, 2))):
         flush.zero_()
@@ -437,13 +438,20 @@ def main():
         t0 = time.perf_counter()
         p2 = M.Plan(ctx, ns, ms, raw_pinned, samples=a.samples, precision=a.precision,
                     graph=0, **shape)
+        t1 = time.perf_counter()
         p2.execute()
+        t2 = time.perf_counter()
         r = p2.results()
         torch.cuda.synchronize(dev)
-        e2e_ms.append((time.perf_counter() - t0) * 1000.0)
+        t3 = time.perf_counter()
+        e2e_ms.append((t3 - t0) * 1000.0)
+        e2e_parts["create_ms"] += (t1 - t0) * 1000.0
+        e2e_parts["execute_call_ms"] += (t2 - t1) * 1000.0
+        e2e_parts["results_ms"] += (t3 - t2) * 1000.0
         st2 = p2.stats()
         h2d, d2h = st2["h2d_bytes"], st2["d2h_bytes"]
         p2.close()
+    e2e_parts = {k: v / len(e2e_ms) for k, v in e2e_parts.items()}
     e2e_total = max_over_ranks(sum(e2e_ms), world, dist, dev)
     e2e_val = world * instance_units(a, count) * len(e2e_ms) / (e2e_total / 1000.0)
 
@@ -507,7 +515,7 @@ def main():
             "data": "synthetic seeded SK instances (J,h ~ N(0,1)); reference datasets not used",
             "config": config,
             "e2e": {"value": e2e_val, "unit": "instances/s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h},
+                    "d2h_bytes_per_step": d2h, "per_step": e2e_parts},
             "gpu_launches": launches // max(1, a.steps),
             "roofline": roofline,
             "cpu_baseline": cpu,

@@ -806,7 +806,7 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineParams p) {
 // of one walk's psi in registers and, eight basis vectors at a time,
 // accumulates w_j . psi (re, im) in FP64, reduces over the warp with
 // shuffles and leaves the warp's value in shared memory; the warps' values
-// are then summed in a fixed order into part[g][j][b]. The walks of a group
+// are then summed in a fixed order into part[g][b][j]. The walks of a group
 // are done one after another over the same basis slice.
 constexpr int kProjThreads = 256;
 constexpr int kProjJ = 8;
@@ -871,7 +871,7 @@ __global__ void __launch_bounds__(kProjThreads, 2) project_partial_kernel(Projec
           if (j0 + jj < Kb) {
             double v = 0.0;
             for (int k = 0; k < kWarps; k++) v += red[k][jj][c];
-            double* dst = p.part + ((((size_t)g * Kb) + j0 + jj) * tiles + blockIdx.x) * 2 + c;
+            double* dst = p.part + ((((size_t)g * tiles) + blockIdx.x) * Kb + j0 + jj) * 2 + c;
             *dst = q0 == 0 ? v : *dst + v;  // rounds of 16 amplitudes in order
           }
         }
@@ -882,8 +882,9 @@ __global__ void __launch_bounds__(kProjThreads, 2) project_partial_kernel(Projec
 }
 
 // Last-stage projection, final: one block per walk sums its part[][j] over the
-// blocks (fixed order), forms A = sum_j d_j z_j (d_j real for even j,
-// imaginary for odd j) and writes P = |A|^2 kappa^2.
+// blocks (fixed order; consecutive threads read consecutive j), forms
+// A = sum_j d_j z_j (d_j real for even j, imaginary for odd j) and writes
+// P = |A|^2 kappa^2.
 __global__ void project_final_kernel(ProjectParams p) {
   const int g = blockIdx.x;
   const ProjectWalk& W = p.walk[g];
@@ -893,10 +894,11 @@ __global__ void project_final_kernel(ProjectParams p) {
   double are = 0.0, aim = 0.0;
   for (int j = threadIdx.x; j < Kb; j += blockDim.x) {
     double zr = 0.0, zi = 0.0;
-    const double* pj = p.part + (((size_t)g * Kb) + j) * tiles * 2;
+    const double* pj = p.part + ((size_t)g * tiles * Kb + j) * 2;
     for (size_t b = 0; b < tiles; b++) {
-      zr += pj[2 * b];
-      zi += pj[2 * b + 1];
+      const double2 v = *reinterpret_cast<const double2*>(pj + b * Kb * 2);
+      zr += v.x;
+      zi += v.y;
     }
     const double cj = j < W.K ? (double)W.coef[j] : 0.0;
     const double cj2 = j + 2 < W.K ? (double)W.coef[j + 2] : 0.0;
