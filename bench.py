@@ -403,7 +403,7 @@ def main():
     barrier()
     clocks = ClockSampler(gpu_selector(torch, local))
     step_ms, kern_ms = [], []
-    term_amps = pass_amps = 0.0
+    term_amps = pass_amps = aux_bytes = 0.0
     launches = term_launches = terms = 0
     for _ in range(a.steps):
         flush.zero_()
@@ -419,6 +419,7 @@ def main():
         kern_ms.append(st["kernel_ms"])
         term_amps += st["term_amps"]
         pass_amps += st["pass_amps"]
+        aux_bytes += st["aux_bytes"]
         launches += st["launches"]
         term_launches += st["term_launches"]
         terms = st["terms"]
@@ -470,10 +471,12 @@ def main():
 
     pk, pk_kind = peaks()
     kms = sum(kern_ms)
-    # Bytes of the Clenshaw passes actually executed (the stage-1 basis
-    # replaces most first-stage passes; term_amps counts the reference's
-    # work) over the device time of the whole propagation phase.
-    achieved = BYTES_PER_TERM_AMP[a.precision] * pass_amps / (kms / 1000.0) / 1e9 if kms > 0 else None
+    # Algorithmic bytes the propagation phase moved — the Clenshaw passes
+    # actually executed (36 B per term·amp) plus the shared-basis kernels'
+    # reads and writes (the bases replace most first- and last-stage passes;
+    # term_amps counts the reference's work) — over its device time.
+    moved = BYTES_PER_TERM_AMP[a.precision] * pass_amps + aux_bytes
+    achieved = moved / (kms / 1000.0) / 1e9 if kms > 0 else None
     peak = pk["hbm_gbs"]
     per_launch_amps = pass_amps / max(1, term_launches)
     dram = DRAM_BYTES_PER_TERM_AMP.get(desc["workload"])
@@ -502,6 +505,7 @@ def main():
             config["grid_shape"] = ctx.grid_shape(max(ns), a.precision)
         config["reference_term_amps_per_step"] = term_amps / a.steps
         config["pass_term_amps_per_step"] = pass_amps / a.steps
+        config["shared_basis_bytes_per_step"] = aux_bytes / a.steps
         config.update({"instances_per_step": count * world, "samples": a.samples,
                        "precision": a.precision, "group": a.group or "autotuned",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",

@@ -114,9 +114,12 @@ typedef struct mqw_run_stats {
   double h2d_bytes;         /* host-to-device bytes copied by the plan */
   double d2h_bytes;         /* device-to-host bytes copied by the plan */
   double pass_amps;         /* term x amplitudes the grid-path Clenshaw passes
-                               actually executed (stage-1 recombination
-                               replaces the per-walk first stage, so this can
-                               be below term_amps) */
+                               actually executed (the shared bases replace
+                               the per-walk first and last stages, so this
+                               can be well below term_amps) */
+  double aux_bytes;         /* device bytes the shared-basis kernels move:
+                               basis stores, recombination and projection
+                               reads and writes */
 } mqw_run_stats;
 
 typedef struct mqw_ctx mqw_ctx;

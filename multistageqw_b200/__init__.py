@@ -103,6 +103,7 @@ class RunStats(ctypes.Structure):
         ("h2d_bytes", ctypes.c_double),
         ("d2h_bytes", ctypes.c_double),
         ("pass_amps", ctypes.c_double),
+        ("aux_bytes", ctypes.c_double),
     ]
 
     def as_dict(self) -> dict:

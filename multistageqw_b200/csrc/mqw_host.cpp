@@ -534,7 +534,11 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
         Q.p_out = p_sample + w.p_off;
       }
       CK(launch_project(pr, stream));
-      if (P.counting) P.stats.launches += 2;
+      if (P.counting) {
+        P.stats.launches += 2;
+        // each walk reads the basis slice and its state once
+        P.stats.aux_bytes += (double)G * ((double)Kl * N * 4.0 + (double)N * 8.0);
+      }
       break;  // the walks' P are written; nothing follows the last stage
     }
     if (st == 0 && basis) {
@@ -553,7 +557,11 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
         C.norm_part = norm_part + (size_t)g * tiles;
       }
       CK(launch_combine(P.precision, cp, stream));
-      if (P.counting) P.stats.launches++;
+      if (P.counting) {
+        P.stats.launches++;
+        // the basis once per group, one complex state written per walk
+        P.stats.aux_bytes += (double)Kb * N * 4.0 + (double)G * N * 8.0;
+      }
       Kmax = 0;  // no recurrence passes for this stage
     }
     for (int r = Kmax - 1; r >= 0; r--) {
@@ -703,6 +711,7 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
       P.stats.launches++;
       P.stats.term_launches++;
       P.stats.pass_amps += (double)N;
+      P.stats.aux_bytes += (double)N * 4.0;  // the real part stored
     }
   }
   return MQW_OK;
@@ -841,6 +850,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
   P.counting = true;
   P.stats.launches = P.stats.term_launches = 0;
   P.stats.pass_amps = 0;
+  P.stats.aux_bytes = 0;
   P.stats.h2d_bytes = P.stats.d2h_bytes = 0;
   // Geometry and shared scratch for every n of the plan, sized up front so
   // that nothing is allocated while the pipeline is issued or captured.
