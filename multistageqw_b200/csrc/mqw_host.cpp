@@ -950,7 +950,9 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
   if (want1 || want2) {
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)8 << 30;
-    const size_t budget = std::min(free_b / 4, (size_t)16 << 30);
+    // Up to half the free memory (64 GB at most): at n = 28 the stage-1
+    // basis alone is ~K_1 GB.
+    const size_t budget = std::min(free_b / 2, (size_t)64 << 30);
     std::map<int, std::pair<int, int>> kb;
     for (size_t w = 0; w < P.walks.size(); w++) {
       const ResidentWalk& wk = P.walks[w];
