@@ -814,7 +814,7 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
         std::vector<int> grp(ws.begin() + a, ws.begin() + std::min(b1, a + G));
         const int lane = i % lanes;
         double* proj = ctx->proj_part.as<double>() +
-                       (size_t)lane * G * std::max(kb2, 1) * (((size_t)1 << n) >> geo.L) * 2;
+                       (size_t)lane * G * std::max(kb2, 1) * (((size_t)1 << n) / 2048) * 2;
         mqw_status s = run_grid_group(P, grp, geo, lane, G, basis, basis ? Kb : 0, lastb,
                                       lastb ? Kl : 0, proj,
                                       lane == 0 ? stream : ctx->lane_stream[lane]);
@@ -969,15 +969,16 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads,
                                          gs.lane_smem > 0, gs.tma > 0);
       int k1 = want1 && e.second.first <= kMaxBasis ? e.second.first : 0;
-      int k2 = want2 && geo.L >= 10 && e.second.second <= kMaxBasis ? e.second.second : 0;
+      int k2 = want2 && n >= 11 && e.second.second <= kMaxBasis ? e.second.second : 0;
       if (BasisLayout::bytes(n, k1, k2) > budget) k2 = 0;
       if (BasisLayout::bytes(n, k1, k2) > budget) k1 = 0;
       if (!k1 && !k2) continue;
       P.basis_kb1[n] = k1;
       P.basis_kb2[n] = k2;
       basis_b = std::max(basis_b, BasisLayout::bytes(n, k1, k2));
+      // projection partials: per lane, per walk, per 2048-amplitude block
       proj_b = std::max(proj_b, (size_t)gs.lanes * gs.group * std::max(k2, 1) *
-                                    ((((size_t)1 << n) >> geo.L)) * 2 * sizeof(double));
+                                    (((size_t)1 << n) / 2048) * 2 * sizeof(double));
       rmax = std::max(rmax, std::max(k1 + (k1 & 1), k2 + (k2 & 1)));
     }
     if (basis_b) {

@@ -208,7 +208,7 @@ struct ProjectWalk {
 struct ProjectParams {
   const float* basis;  // Kb real FP32 vectors of 2^n amplitudes
   int n, L, Kb, count;
-  double* part;        // scratch: [2^(n-L) blocks][count][Kb][2] partial dots
+  double* part;        // scratch: [count][2^n / 2048 blocks][Kb][2] partial dots
   ProjectWalk walk[kMaxGroup];
 };
 cudaError_t launch_project(const ProjectParams& p, cudaStream_t stream);

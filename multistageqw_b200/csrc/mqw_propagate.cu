@@ -801,127 +801,141 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineParams p) {
   }
 }
 
-// Last-stage projection, partial dots: block b covers the 2^L amplitudes
-// [b 2^L, (b+1) 2^L) (2^L >= 1024); each thread holds 16 of them (4 quads)
-// of one walk's psi in registers and, eight basis vectors at a time,
-// accumulates w_j . psi (re, im) in FP64, reduces over the warp with
+// Last-stage projection, partial dots: block b covers the kProjChunk
+// amplitudes [b kProjChunk, (b+1) kProjChunk); each thread holds 8 of them
+// (2 quads) of one walk's psi in registers and, eight basis vectors at a
+// time, accumulates w_j . psi (re, im) in FP64, reduces over the warp with
 // shuffles and leaves the warp's value in shared memory; the warps' values
 // are then summed in a fixed order into part[g][b][j]. The walks of a group
 // are done one after another over the same basis slice.
 constexpr int kProjThreads = 256;
 constexpr int kProjJ = 8;
+constexpr int kProjQuads = 2;
+constexpr size_t kProjChunk = (size_t)4 * kProjThreads * kProjQuads;  // 2048
 __global__ void __launch_bounds__(kProjThreads, 2) project_partial_kernel(ProjectParams p) {
   constexpr int kWarps = kProjThreads / 32;
   __shared__ double red[kWarps][kProjJ][2];
   const int Kb = p.Kb, G = p.count;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const size_t N = (size_t)1 << p.n;
-  const size_t chunk = (size_t)1 << p.L;  // multiple of 4 * kProjThreads (L >= 10)
-  const int nq = (int)(chunk / (4 * kProjThreads));
-  const size_t base = (size_t)blockIdx.x * chunk;
-  const size_t tiles = N >> p.L;
+  const size_t blocks = N / kProjChunk;
+  const size_t base = (size_t)blockIdx.x * kProjChunk;
   for (int g = 0; g < G; g++) {
     const float* psi = reinterpret_cast<const float*>(p.walk[g].psi);
-    for (int q0 = 0; q0 < nq; q0 += 4) {  // 16 amplitudes per thread per round
-      float4 ps[4][2];
+    float4 ps[kProjQuads][2];
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const size_t i = base + 4 * threadIdx.x + (size_t)(q0 + q) * 4 * kProjThreads;
-        const bool in = q0 + q < nq;
-        ps[q][0] = in ? __ldg(reinterpret_cast<const float4*>(psi + 2 * i)) : make_float4(0, 0, 0, 0);
-        ps[q][1] = in ? __ldg(reinterpret_cast<const float4*>(psi + 2 * i + 4)) : make_float4(0, 0, 0, 0);
-      }
-      for (int j0 = 0; j0 < Kb; j0 += kProjJ) {
-        double acc[kProjJ][2];
+    for (int q = 0; q < kProjQuads; q++) {
+      const size_t i = base + 4 * threadIdx.x + (size_t)q * 4 * kProjThreads;
+      ps[q][0] = __ldg(reinterpret_cast<const float4*>(psi + 2 * i));
+      ps[q][1] = __ldg(reinterpret_cast<const float4*>(psi + 2 * i + 4));
+    }
+    for (int j0 = 0; j0 < Kb; j0 += kProjJ) {
+      double acc[kProjJ][2];
 #pragma unroll
-        for (int jj = 0; jj < kProjJ; jj++) acc[jj][0] = acc[jj][1] = 0.0;
+      for (int jj = 0; jj < kProjJ; jj++) acc[jj][0] = acc[jj][1] = 0.0;
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-          if (q0 + q >= nq) break;
-          const size_t i = base + 4 * threadIdx.x + (size_t)(q0 + q) * 4 * kProjThreads;
-          float4 w[kProjJ];
-#pragma unroll
-          for (int jj = 0; jj < kProjJ; jj++)
-            w[jj] = j0 + jj < Kb ? __ldg(reinterpret_cast<const float4*>(p.basis + (size_t)(j0 + jj) * N + i))
-                                 : make_float4(0, 0, 0, 0);
-          const float4 a = ps[q][0], b = ps[q][1];
-#pragma unroll
-          for (int jj = 0; jj < kProjJ; jj++) {
-            acc[jj][0] = fma((double)w[jj].x, (double)a.x, acc[jj][0]);
-            acc[jj][1] = fma((double)w[jj].x, (double)a.y, acc[jj][1]);
-            acc[jj][0] = fma((double)w[jj].y, (double)a.z, acc[jj][0]);
-            acc[jj][1] = fma((double)w[jj].y, (double)a.w, acc[jj][1]);
-            acc[jj][0] = fma((double)w[jj].z, (double)b.x, acc[jj][0]);
-            acc[jj][1] = fma((double)w[jj].z, (double)b.y, acc[jj][1]);
-            acc[jj][0] = fma((double)w[jj].w, (double)b.z, acc[jj][0]);
-            acc[jj][1] = fma((double)w[jj].w, (double)b.w, acc[jj][1]);
-          }
-        }
+      for (int q = 0; q < kProjQuads; q++) {
+        const size_t i = base + 4 * threadIdx.x + (size_t)q * 4 * kProjThreads;
+        float4 w[kProjJ];
 #pragma unroll
         for (int jj = 0; jj < kProjJ; jj++)
+          w[jj] = j0 + jj < Kb ? __ldg(reinterpret_cast<const float4*>(p.basis + (size_t)(j0 + jj) * N + i))
+                               : make_float4(0, 0, 0, 0);
+        const float4 a = ps[q][0], b = ps[q][1];
 #pragma unroll
-          for (int c = 0; c < 2; c++) {
-            double v = acc[jj][c];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if (lane == 0) red[warp][jj][c] = v;
-          }
-        __syncthreads();
-        if (threadIdx.x < 2 * kProjJ) {
-          const int jj = threadIdx.x >> 1, c = threadIdx.x & 1;
-          if (j0 + jj < Kb) {
-            double v = 0.0;
-            for (int k = 0; k < kWarps; k++) v += red[k][jj][c];
-            double* dst = p.part + ((((size_t)g * tiles) + blockIdx.x) * Kb + j0 + jj) * 2 + c;
-            *dst = q0 == 0 ? v : *dst + v;  // rounds of 16 amplitudes in order
-          }
+        for (int jj = 0; jj < kProjJ; jj++) {
+          acc[jj][0] = fma((double)w[jj].x, (double)a.x, acc[jj][0]);
+          acc[jj][1] = fma((double)w[jj].x, (double)a.y, acc[jj][1]);
+          acc[jj][0] = fma((double)w[jj].y, (double)a.z, acc[jj][0]);
+          acc[jj][1] = fma((double)w[jj].y, (double)a.w, acc[jj][1]);
+          acc[jj][0] = fma((double)w[jj].z, (double)b.x, acc[jj][0]);
+          acc[jj][1] = fma((double)w[jj].z, (double)b.y, acc[jj][1]);
+          acc[jj][0] = fma((double)w[jj].w, (double)b.z, acc[jj][0]);
+          acc[jj][1] = fma((double)w[jj].w, (double)b.w, acc[jj][1]);
         }
-        __syncthreads();
       }
+#pragma unroll
+      for (int jj = 0; jj < kProjJ; jj++)
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+          double v = acc[jj][c];
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (lane == 0) red[warp][jj][c] = v;
+        }
+      __syncthreads();
+      if (threadIdx.x < 2 * kProjJ) {
+        const int jj = threadIdx.x >> 1, c = threadIdx.x & 1;
+        if (j0 + jj < Kb) {
+          double v = 0.0;
+          for (int k = 0; k < kWarps; k++) v += red[k][jj][c];
+          p.part[((((size_t)g * blocks) + blockIdx.x) * Kb + j0 + jj) * 2 + c] = v;
+        }
+      }
+      __syncthreads();
     }
   }
 }
 
-// Last-stage projection, final: one block per walk sums its part[][j] over the
-// blocks (fixed order; consecutive threads read consecutive j), forms
-// A = sum_j d_j z_j (d_j real for even j, imaginary for odd j) and writes
-// P = |A|^2 kappa^2.
-__global__ void project_final_kernel(ProjectParams p) {
+// Last-stage projection, final: one block per walk. For 64 basis vectors at
+// a time, 8 groups of threads sum every 8th block's partial (consecutive
+// threads read consecutive j), the 8 group sums are added in order, and the
+// walk's A = sum_j d_j z_j (d_j real for even j, imaginary for odd j) is
+// accumulated per thread and summed in order at the end: P = |A|^2 kappa^2.
+constexpr int kFinalJ = 64, kFinalGroups = 8;
+__global__ void __launch_bounds__(kFinalJ * kFinalGroups) project_final_kernel(ProjectParams p) {
   const int g = blockIdx.x;
   const ProjectWalk& W = p.walk[g];
   const int Kb = p.Kb;
-  const size_t tiles = (size_t)1 << (p.n - p.L);
-  __shared__ double sre[256], sim[256];
+  const size_t blocks = ((size_t)1 << p.n) / kProjChunk;
+  const int jj = threadIdx.x % kFinalJ, t = threadIdx.x / kFinalJ;
+  __shared__ double zr_s[kFinalGroups][kFinalJ], zi_s[kFinalGroups][kFinalJ];
   double are = 0.0, aim = 0.0;
-  for (int j = threadIdx.x; j < Kb; j += blockDim.x) {
+  for (int j0 = 0; j0 < Kb; j0 += kFinalJ) {
+    const int j = j0 + jj;
     double zr = 0.0, zi = 0.0;
-    const double* pj = p.part + ((size_t)g * tiles * Kb + j) * 2;
-    for (size_t b = 0; b < tiles; b++) {
-      const double2 v = *reinterpret_cast<const double2*>(pj + b * Kb * 2);
-      zr += v.x;
-      zi += v.y;
+    if (j < Kb) {
+      const double* pj = p.part + (((size_t)g * blocks) * Kb + j) * 2;
+      for (size_t b = t; b < blocks; b += kFinalGroups) {
+        const double2 v = *reinterpret_cast<const double2*>(pj + b * Kb * 2);
+        zr += v.x;
+        zi += v.y;
+      }
     }
-    const double cj = j < W.K ? (double)W.coef[j] : 0.0;
-    const double cj2 = j + 2 < W.K ? (double)W.coef[j + 2] : 0.0;
-    const double d = j == 0 ? cj - 0.5 * cj2 : 0.5 * (cj - cj2);
-    if (j & 1) {  // i d z
-      are -= d * zi;
-      aim += d * zr;
-    } else {
-      are += d * zr;
-      aim += d * zi;
+    zr_s[t][jj] = zr;
+    zi_s[t][jj] = zi;
+    __syncthreads();
+    if (t == 0 && j < Kb) {
+      double r = 0.0, i = 0.0;
+      for (int k = 0; k < kFinalGroups; k++) {
+        r += zr_s[k][jj];
+        i += zi_s[k][jj];
+      }
+      const double cj = j < W.K ? (double)W.coef[j] : 0.0;
+      const double cj2 = j + 2 < W.K ? (double)W.coef[j + 2] : 0.0;
+      const double d = j == 0 ? cj - 0.5 * cj2 : 0.5 * (cj - cj2);
+      if (j & 1) {  // i d z
+        are -= d * i;
+        aim += d * r;
+      } else {
+        are += d * r;
+        aim += d * i;
+      }
     }
+    __syncthreads();
   }
-  sre[threadIdx.x] = are;
-  sim[threadIdx.x] = aim;
+  if (t == 0) {
+    zr_s[0][jj] = are;
+    zi_s[0][jj] = aim;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     double r = 0.0, i = 0.0;
-    for (int t = 0; t < (int)blockDim.x; t++) {
-      r += sre[t];
-      i += sim[t];
+    for (int k = 0; k < kFinalJ; k++) {
+      r += zr_s[0][k];
+      i += zi_s[0][k];
     }
-    const double k = W.kappa ? *W.kappa : 1.0;
-    *W.p_out = (r * r + i * i) * k * k;
+    const double kap = W.kappa ? *W.kappa : 1.0;
+    *W.p_out = (r * r + i * i) * kap * kap;
   }
 }
 
@@ -1275,18 +1289,18 @@ cudaError_t launch_combine(int precision, const CombineParams& p,
 }
 
 cudaError_t launch_project(const ProjectParams& p, cudaStream_t stream) {
-  if (p.n < 10 || p.n > kMaxN || p.L < 10 || p.L > p.n || p.Kb < 1 || p.Kb > kMaxBasis ||
+  if (p.n < 11 || p.n > kMaxN || p.Kb < 1 || p.Kb > kMaxBasis ||
       p.count < 1 || p.count > kMaxGroup || !p.basis || !p.part)
     return cudaErrorInvalidValue;
   for (int g = 0; g < p.count; g++)
     if (p.walk[g].K < 1 || p.walk[g].K > p.Kb || !p.walk[g].coef || !p.walk[g].psi ||
         !p.walk[g].p_out)
       return cudaErrorInvalidValue;
-  const unsigned blocks = (unsigned)((size_t)1 << (p.n - p.L));
+  const unsigned blocks = (unsigned)(((size_t)1 << p.n) / kProjChunk);
   project_partial_kernel<<<blocks, kProjThreads, 0, stream>>>(p);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  project_final_kernel<<<p.count, 256, 0, stream>>>(p);
+  project_final_kernel<<<p.count, kFinalJ * kFinalGroups, 0, stream>>>(p);
   return cudaGetLastError();
 }
 
