@@ -235,10 +235,6 @@ struct FinalParams {
 cudaError_t launch_finalize(int precision, const FinalParams& p,
                             cudaStream_t stream);
 
-// Fill a state with the uniform superposition (float(1/sqrt(N)), 0).
-cudaError_t launch_uniform(int precision, void* psi, int n,
-                           cudaStream_t stream);
-
 // Mean of p_sample rows (fixed order) into p_mean.
 cudaError_t launch_mean(const double* p_sample, const int* p_off,
                         const int* p_cnt, int count, double* p_mean,

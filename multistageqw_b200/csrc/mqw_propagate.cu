@@ -198,13 +198,6 @@ template <> __device__ __forceinline__ void st4<double>(double* p, const V4<doub
   reinterpret_cast<double2*>(p)[0] = make_double2(v.x, v.y);
   reinterpret_cast<double2*>(p)[1] = make_double2(v.z, v.w);
 }
-template <typename R>
-__device__ __forceinline__ void add4(V4<R>& a, const V4<R>& b) {
-  a.x += b.x;
-  a.y += b.y;
-  a.z += b.z;
-  a.w += b.w;
-}
 // c * psi for a pair, c real (even term) or imaginary (odd term).
 template <typename R>
 __device__ __forceinline__ V4<R> cpsi4(R c, bool odd, const V4<R>& p) {
@@ -231,13 +224,6 @@ __device__ __forceinline__ void cp_async_pair(R* smem, const R* gmem) {
   if (sizeof(R) == 8) cp_async16(smem + 2, gmem + 2);
 }
 
-template <typename R>
-__device__ __forceinline__ V4<R> shfl4(const V4<R>& v, int lane_mask) {
-  return {__shfl_xor_sync(0xffffffffu, v.x, lane_mask),
-          __shfl_xor_sync(0xffffffffu, v.y, lane_mask),
-          __shfl_xor_sync(0xffffffffu, v.z, lane_mask),
-          __shfl_xor_sync(0xffffffffu, v.w, lane_mask)};
-}
 
 // A pair of neighbouring amplitudes as the hot loops carry it. FP32: two
 // 64-bit registers, each a packed (re, im), accumulated with sm_100's
@@ -964,14 +950,6 @@ __global__ void finalize_kernel(FinalParams p) {
   }
 }
 
-template <typename R>
-__global__ void uniform_kernel(typename Cplx<R>::T* psi, int n) {
-  const size_t N = (size_t)1 << n;
-  const R v = (R)(float)(1.0 / sqrt((double)N));
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < N;
-       i += (size_t)gridDim.x * blockDim.x)
-    psi[i] = mk<R>(v, (R)0);
-}
 
 __global__ void mean_kernel(const double* p_sample, const int* p_off,
                             const int* p_cnt, int count, double* p_mean) {
@@ -1321,17 +1299,6 @@ cudaError_t launch_finalize(int precision, const FinalParams& p,
   return cudaGetLastError();
 }
 
-cudaError_t launch_uniform(int precision, void* psi, int n,
-                           cudaStream_t stream) {
-  const size_t N = (size_t)1 << n;
-  const int T = 256;
-  const unsigned blocks = (unsigned)((N + T - 1) / T < 4096 ? (N + T - 1) / T : 4096);
-  if (precision == 0)
-    uniform_kernel<float><<<blocks, T, 0, stream>>>((float2*)psi, n);
-  else
-    uniform_kernel<double><<<blocks, T, 0, stream>>>((double2*)psi, n);
-  return cudaGetLastError();
-}
 
 cudaError_t launch_mean(const double* p_sample, const int* p_off,
                         const int* p_cnt, int count, double* p_mean,
