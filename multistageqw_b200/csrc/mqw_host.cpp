@@ -84,7 +84,22 @@ struct mqw_ctx {
   // Device error word: kernels whose bounded waits give up set bit 0; the
   // host reads and clears it when it collects results.
   DevMem dev_err;
-  DevMem basis;      // shared bases of the instance in flight (+ their slots)
+  DevMem basis, basis2;  // shared bases of the instance in flight and of
+                         // the next one (+ their slots)
+  // The basis stream builds the next instance's bases while the current
+  // instance's walks run; events order the two buffers' uses.
+  cudaStream_t basis_stream = nullptr;
+  cudaEvent_t basis_built[2] = {}, basis_free[2] = {};
+  cudaError_t ensure_basis_stream() {
+    cudaError_t e = cudaSuccess;
+    if (!basis_stream) e = cudaStreamCreateWithFlags(&basis_stream, cudaStreamNonBlocking);
+    for (int k = 0; k < 2 && e == cudaSuccess; k++) {
+      if (!basis_built[k]) e = cudaEventCreateWithFlags(&basis_built[k], cudaEventDisableTiming);
+      if (e == cudaSuccess && !basis_free[k])
+        e = cudaEventCreateWithFlags(&basis_free[k], cudaEventDisableTiming);
+    }
+    return e;
+  }
   DevMem proj_part;  // last-stage projection partial dots, per lane
   // Bumped whenever a shared scratch buffer is reallocated: a plan's captured
   // graph holds the old addresses and is re-captured when this changes.
@@ -214,6 +229,7 @@ struct mqw_plan {
   // (0 = not used for that n), and the unit coefficient list the basis passes
   // read ([0, ..., 0, 1]).
   std::map<int, int> basis_kb1, basis_kb2;
+  int basis_buffers = 1;  // 2: the next instance's bases are built ahead
   DevMem d_unit;
   int unit_len = 0;
   // CUDA graph of the whole device pipeline, replayed by later executes.
@@ -774,54 +790,114 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
     const std::vector<int>& ws = kv.second;
     const int kb1 = P.basis_kb1.count(n) ? P.basis_kb1.at(n) : 0;
     const int kb2 = P.basis_kb2.count(n) ? P.basis_kb2.at(n) : 0;
-    const BasisLayout B{ctx->basis.as<char>(), (size_t)1 << n, kb1, kb2};
     // Blocks of walks: one block per instance when a shared basis is used
     // (the bases are built before, and read during, the block), else all.
-    size_t b0 = 0;
-    while (b0 < ws.size()) {
-      size_t b1 = ws.size();
-      const float* basis = nullptr;
-      const float* lastb = nullptr;
-      int Kb = 0, Kl = 0;
+    struct Block {
+      size_t b0, b1;
+      int Kb, Kl;  // basis sizes (0: none)
+    };
+    std::vector<Block> blocks;
+    for (size_t b0 = 0; b0 < ws.size();) {
+      Block bk{b0, ws.size(), 0, 0};
       if (kb1 > 0 || kb2 > 0) {
-        b1 = b0;
+        size_t b1 = b0;
         while (b1 < ws.size() && P.walks[ws[b1]].inst == P.walks[ws[b0]].inst) b1++;
+        bk.b1 = b1;
         const ResidentWalk& w0 = P.walks[ws[b0]];
         if (!w0.record_each && w0.stages >= 2) {
+          int Kb = 0, Kl = 0;
           for (size_t k = b0; k < b1; k++) {
             Kb = std::max(Kb, P.degree[P.walks[ws[k]].stage_desc_off]);
             Kl = std::max(Kl, P.degree[P.walks[ws[k]].stage_desc_off + w0.stages - 1]);
           }
-          if (kb1 > 0 && Kb <= kb1) {
-            mqw_status s = issue_basis(P, w0, 0, Kb, B, geo, B.real1(), stream);
-            if (s != MQW_OK) return s;
-            basis = B.real1();
-          }
-          if (kb2 > 0 && Kl <= kb2) {
-            mqw_status s = issue_basis(P, w0, w0.stages - 1, Kl, B, geo, B.real2(), stream);
-            if (s != MQW_OK) return s;
-            lastb = B.real2();
-          }
+          bk.Kb = kb1 > 0 && Kb <= kb1 ? Kb : 0;
+          bk.Kl = kb2 > 0 && Kl <= kb2 ? Kl : 0;
         }
       }
+      blocks.push_back(bk);
+      b0 = bk.b1;
+    }
+    // The bases of block i+1 are built on the context's basis stream into
+    // the other of two buffers while block i's walks run (one buffer and no
+    // overlap when two do not fit): block i waits for its build, the build
+    // into a buffer waits until the block that last read it has joined.
+    const int nbuf = P.basis_buffers;
+    const BasisLayout Bs[2] = {{ctx->basis.as<char>(), (size_t)1 << n, kb1, kb2},
+                               {ctx->basis2.as<char>(), (size_t)1 << n, kb1, kb2}};
+    auto build = [&](const Block& bk, int buf, cudaStream_t st) -> mqw_status {
+      const ResidentWalk& w0 = P.walks[ws[bk.b0]];
+      const BasisLayout& B = Bs[buf];
+      if (bk.Kb) {
+        mqw_status s = issue_basis(P, w0, 0, bk.Kb, B, geo, B.real1(), st);
+        if (s != MQW_OK) return s;
+      }
+      if (bk.Kl) {
+        mqw_status s = issue_basis(P, w0, w0.stages - 1, bk.Kl, B, geo, B.real2(), st);
+        if (s != MQW_OK) return s;
+      }
+      return MQW_OK;
+    };
+    const bool overlap = nbuf == 2;
+    cudaStream_t bst = ctx->basis_stream;
+    if (overlap) {
+      // Buffers free and inputs ready: everything queued so far.
+      CK(cudaEventRecord(ctx->basis_free[0], stream));
+      CK(cudaEventRecord(ctx->basis_free[1], stream));
+    }
+    bool built_next = false;  // block i's bases already issued on bst
+    for (size_t bi = 0; bi < blocks.size(); bi++) {
+      const Block& bk = blocks[bi];
+      const int buf = overlap ? (int)(bi & 1) : 0;
+      const bool has = bk.Kb || bk.Kl;
+      if (has) {
+        if (overlap) {
+          if (!built_next) {
+            CK(cudaStreamWaitEvent(bst, ctx->basis_free[buf], 0));
+            mqw_status s = build(bk, buf, bst);
+            if (s != MQW_OK) return s;
+            CK(cudaEventRecord(ctx->basis_built[buf], bst));
+          }
+          CK(cudaStreamWaitEvent(stream, ctx->basis_built[buf], 0));
+        } else {
+          mqw_status s = build(bk, 0, stream);
+          if (s != MQW_OK) return s;
+        }
+      }
+      built_next = false;
+      const BasisLayout& B = Bs[buf];
+      const float* basis = bk.Kb ? B.real1() : nullptr;
+      const float* lastb = bk.Kl ? B.real2() : nullptr;
       // Groups are dealt round-robin to the lanes, which run concurrently.
-      const int nw = (int)(b1 - b0);
+      const int nw = (int)(bk.b1 - bk.b0);
       const int ngroups = (nw + G - 1) / G;
       const int lanes = std::min(gs.lanes, ngroups);
       CK(ctx->fork(stream, lanes));
+      // The next block's bases, overlapping this block's walks.
+      if (overlap && bi + 1 < blocks.size() && (blocks[bi + 1].Kb || blocks[bi + 1].Kl)) {
+        const int nb = (int)((bi + 1) & 1);
+        CK(cudaStreamWaitEvent(bst, ctx->basis_free[nb], 0));
+        mqw_status s = build(blocks[bi + 1], nb, bst);
+        if (s != MQW_OK) return s;
+        CK(cudaEventRecord(ctx->basis_built[nb], bst));
+        built_next = true;
+      }
       for (int i = 0; i < ngroups; i++) {
-        const size_t a = b0 + (size_t)i * G;
-        std::vector<int> grp(ws.begin() + a, ws.begin() + std::min(b1, a + G));
+        const size_t a = bk.b0 + (size_t)i * G;
+        std::vector<int> grp(ws.begin() + a, ws.begin() + std::min(bk.b1, a + G));
         const int lane = i % lanes;
         double* proj = ctx->proj_part.as<double>() +
                        (size_t)lane * G * std::max(kb2, 1) * (((size_t)1 << n) / 2048) * 2;
-        mqw_status s = run_grid_group(P, grp, geo, lane, G, basis, basis ? Kb : 0, lastb,
-                                      lastb ? Kl : 0, proj,
+        mqw_status s = run_grid_group(P, grp, geo, lane, G, basis, bk.Kb, lastb, bk.Kl, proj,
                                       lane == 0 ? stream : ctx->lane_stream[lane]);
         if (s != MQW_OK) return s;
       }
       CK(ctx->join(stream, lanes));
-      b0 = b1;
+      if (overlap) CK(cudaEventRecord(ctx->basis_free[buf], stream));
+    }
+    // The basis stream must be joined back before the end of a capture.
+    if (overlap) {
+      CK(cudaEventRecord(ctx->basis_built[0], bst));
+      CK(cudaStreamWaitEvent(stream, ctx->basis_built[0], 0));
     }
   }
   if (P.counting) CK(cudaEventRecord(P.ev1, stream));
@@ -981,8 +1057,14 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
                                     (((size_t)1 << n) / 2048) * 2 * sizeof(double));
       rmax = std::max(rmax, std::max(k1 + (k1 & 1), k2 + (k2 & 1)));
     }
+    P.basis_buffers = 1;
     if (basis_b) {
       CK(ctx->grow(ctx->basis, basis_b));
+      if (2 * basis_b <= budget) {  // a second buffer to build ahead into
+        CK(ctx->grow(ctx->basis2, basis_b));
+        CK(ctx->ensure_basis_stream());
+        P.basis_buffers = 2;
+      }
       CK(ctx->grow(ctx->proj_part, proj_b));
       if (P.unit_len < rmax + 1) {
         std::vector<float> unit(rmax + 1, 0.0f);
@@ -1105,6 +1187,11 @@ void mqw_destroy(mqw_ctx* ctx) {
     if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
   }
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+  if (ctx->basis_stream) cudaStreamDestroy(ctx->basis_stream);
+  for (int k = 0; k < 2; k++) {
+    if (ctx->basis_built[k]) cudaEventDestroy(ctx->basis_built[k]);
+    if (ctx->basis_free[k]) cudaEventDestroy(ctx->basis_free[k]);
+  }
   delete ctx;
 }
 
