@@ -1060,7 +1060,9 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     P.basis_buffers = 1;
     if (basis_b) {
       CK(ctx->grow(ctx->basis, basis_b));
-      static const bool ahead = !getenv("MQW_BASIS_AHEAD") || atoi(getenv("MQW_BASIS_AHEAD")) != 0;
+      // Building the next instance's bases ahead measured within 1% (the
+      // walks already keep the GPU busy), so it is opt-in: MQW_BASIS_AHEAD=1.
+      static const bool ahead = getenv("MQW_BASIS_AHEAD") && atoi(getenv("MQW_BASIS_AHEAD")) != 0;
       if (ahead && 2 * basis_b <= budget) {  // a second buffer to build ahead into
         CK(ctx->grow(ctx->basis2, basis_b));
         CK(ctx->ensure_basis_stream());
