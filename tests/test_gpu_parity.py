@@ -385,3 +385,30 @@ def mqw_plan_samples(ctx, n, m, raw):
     ps = plan.results(per_sample=True)["p_sample"]
     plan.close()
     return ps
+
+
+def test_basis_build_ahead_gives_identical_results(ctx, orc, mqw):
+    """Building the next instance's bases on a side stream (MQW_BASIS_AHEAD=1,
+    read once per process, so run in a child process) changes only the
+    schedule: per-sample P bit-identical to the in-order build."""
+    import json
+    import sys
+    raw = orc.sk_instances(16, 3, 4100)
+    plan = mqw.Plan(ctx, 16, 3, raw, samples=6, group=1, lanes=2)
+    plan.execute()
+    plan.execute()
+    ref = plan.results(per_sample=True)["p_sample"]
+    plan.close()
+    code = (
+        "import json, numpy as np, multistageqw_b200 as M\n"
+        "raw = M.sk_instances(16, 3, 4100)\n"
+        "c = M.Context(0)\n"
+        "pl = M.Plan(c, 16, 3, raw, samples=6, group=1, lanes=2)\n"
+        "pl.execute(); pl.execute()\n"
+        "print(json.dumps(pl.results(per_sample=True)['p_sample'].tolist()))\n")
+    env = dict(os.environ, MQW_BASIS_AHEAD="1")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env,
+                       cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))), timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = np.array(json.loads(r.stdout.strip().splitlines()[-1]))
+    assert np.array_equal(got, ref)
