@@ -118,3 +118,33 @@ def test_cheb_host_build_bit_exact_vs_oracle(mqw, orc):
         ref = orc.cheb_coeffs(sv).astype(np.float32)
         assert K[i] == len(ref), sv
         assert np.array_equal(coeffs[i].view(np.uint32), ref.view(np.uint32)), sv
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """The ctypes mirrors of the ABI structs have the header's sizes and field
+    offsets (compiled with the system C compiler)."""
+    import ctypes
+    import shutil
+    import subprocess
+    import multistageqw_b200 as M
+    if not shutil.which("gcc"):
+        pytest.skip("no C compiler")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    structs = {"mqw_options": M.Options, "mqw_run_stats": M.RunStats,
+               "mqw_diag_info": M.DiagInfo, "mqw_grid_shape": M.GridShape}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "mqw.h"', "int main(void) {"]
+    for name, cls in structs.items():
+        lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')
+        for field, _ in cls._fields_:
+            lines.append(f'  printf("{name}.{field} %zu\\n", offsetof({name}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(l.split() for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                 check=True).stdout.splitlines())
+    for name, cls in structs.items():
+        assert int(out[name]) == ctypes.sizeof(cls), name
+        for field, _ in cls._fields_:
+            assert int(out[f"{name}.{field}"]) == getattr(cls, field).offset, (name, field)
