@@ -460,7 +460,7 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
     std::vector<GridShape> cands = {base};
     for (int g : groups) {
       if (want.group && g != want.group) continue;
-      for (int lanes : {1, 2}) {
+      for (int lanes = 1; lanes <= kMaxLanes; lanes++) {
         if (want.lanes && lanes != want.lanes) continue;
         if ((g == base.group && lanes == base.lanes) || !fits(geo, g, lanes)) continue;
         GridShape c = base;
