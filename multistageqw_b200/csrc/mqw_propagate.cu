@@ -717,6 +717,10 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   if constexpr (CL > 0) cluster_barrier();
 }
 
+// The shared bases are streamed (hundreds of MB per walk group at n = 20)
+// with evict-first loads (__ldcs), so that they do not push the walks'
+// L2-resident states out of the cache for the passes running beside them.
+
 // Stage-1 recombination of G walks (FP32): block b covers amplitudes
 // [b 2^L, (b+1) 2^L), reads each real basis vector once for all G walks
 // (eight vectors in flight per thread), and leaves the block's |out|^2 in
@@ -763,12 +767,12 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineParams p) {
       float4 w[8];
 #pragma unroll
       for (int u = 0; u < 8; u++)
-        w[u] = __ldg(reinterpret_cast<const float4*>(basis + (size_t)(j + u) * N + i));
+        w[u] = __ldcs(reinterpret_cast<const float4*>(basis + (size_t)(j + u) * N + i));
 #pragma unroll
       for (int u = 0; u < 8; u++) accumulate(w[u], j + u, u & 1);  // j is even
     }
     for (; j < Kb; j++)
-      accumulate(__ldg(reinterpret_cast<const float4*>(basis + (size_t)j * N + i)), j, j & 1);
+      accumulate(__ldcs(reinterpret_cast<const float4*>(basis + (size_t)j * N + i)), j, j & 1);
 #pragma unroll
     for (int g = 0; g < G; g++) {
       float4* out = reinterpret_cast<float4*>(reinterpret_cast<float*>(p.walk[g].out) + 2 * i);
@@ -825,7 +829,7 @@ __global__ void __launch_bounds__(kProjThreads, 2) project_partial_kernel(Projec
         float4 w[kProjJ];
 #pragma unroll
         for (int jj = 0; jj < kProjJ; jj++)
-          w[jj] = j0 + jj < Kb ? __ldg(reinterpret_cast<const float4*>(p.basis + (size_t)(j0 + jj) * N + i))
+          w[jj] = j0 + jj < Kb ? __ldcs(reinterpret_cast<const float4*>(p.basis + (size_t)(j0 + jj) * N + i))
                                : make_float4(0, 0, 0, 0);
         const float4 a = ps[q][0], b = ps[q][1];
 #pragma unroll
