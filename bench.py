@@ -488,7 +488,9 @@ def main():
         "frac": achieved / peak if achieved else None,
         "traffic": dram * per_launch_amps if dram else None,
         "peak_source": f"hbm_gbs of {pk_kind}",
-        "kernel": "pass_kernel (grid-path fused Clenshaw pass)",
+        "kernel": ("propagation phase: pass_kernel (the dominant kernel, fused Clenshaw pass; "
+                   "bytes_per_launch and traffic are its per-launch figures) plus the "
+                   "shared-basis kernels (their bytes are in achieved)"),
         "bytes_per_launch": BYTES_PER_TERM_AMP[a.precision] * per_launch_amps,
         "avg_launch_us": 1000.0 * kms / max(1, term_launches),
     }
