@@ -473,6 +473,7 @@ def main():
                  "instances_checked": 1, "p_fp32": float(res["p"][0]), "p_fp64": float(p64)}
 
     pk, pk_kind = peaks()
+    tiers = ctx.measure_peaks() if rank == 0 else None
     kms = sum(kern_ms)
     # Algorithmic bytes the propagation phase moved — the Clenshaw passes
     # actually executed (36 B per term·amp) plus the shared-basis kernels'
@@ -494,6 +495,12 @@ def main():
         "bytes_per_launch": BYTES_PER_TERM_AMP[a.precision] * per_launch_amps,
         "avg_launch_us": 1000.0 * kms / max(1, term_launches),
     }
+    if tiers:
+        # The tier that holds the walks' working set (n <= 20: L2-resident):
+        # the same achieved bytes against the measured L2 copy bandwidth.
+        roofline["tiers_gbs"] = {k: round(v, 1) for k, v in tiers.items()}
+        if achieved:
+            roofline["frac_of_l2_copy"] = achieved / tiers["l2_copy_gbs"]
 
     if rank == 0:
         cpu = None

@@ -262,6 +262,16 @@ void mqw_plan_destroy(mqw_plan* plan);
  * (the context stays usable); any other status is a failure. */
 mqw_status mqw_selftest_wait_timeout(mqw_ctx* ctx);
 
+/* Measured bandwidth of the memory tiers a walk's working set can live in,
+ * GB/s: L2 (a 32 MB buffer read, and copied 16 MB to 16 MB, with L1-bypassing
+ * loads), shared memory (conflict-free 16-byte loads, 4 blocks per SM), HBM
+ * (a 1 GB to 1 GB copy). The roofline denominators for L2- and shared-memory-
+ * resident workloads. Allocates ~2 GB for the duration of the call. */
+typedef struct mqw_tier_peaks {
+  double l2_read_gbs, l2_copy_gbs, smem_gbs, hbm_copy_gbs;
+} mqw_tier_peaks;
+mqw_status mqw_measure_peaks(mqw_ctx* ctx, mqw_tier_peaks* out);
+
 /* The grid-path shape the autotuner picks for n-spin walks in `precision`
  * on this context (tuning now if it has not yet): tile of 2^tile_log
  * amplitudes per CTA, spread over 2^cluster_log CTAs; global_axes axes whose

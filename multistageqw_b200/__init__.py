@@ -91,6 +91,18 @@ class GridShape(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class TierPeaks(ctypes.Structure):
+    _fields_ = [
+        ("l2_read_gbs", ctypes.c_double),
+        ("l2_copy_gbs", ctypes.c_double),
+        ("smem_gbs", ctypes.c_double),
+        ("hbm_copy_gbs", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class RunStats(ctypes.Structure):
     _fields_ = [
         ("instances", ctypes.c_longlong),
@@ -143,6 +155,7 @@ def _bind(L):
         "mqw_grid_shape_for": (i, [_vp, i, i, _P(GridShape)]),
         "mqw_diag_moments": (i, [_vp, i, _P(d), _P(d), _P(DiagInfo)]),
         "mqw_selftest_wait_timeout": (i, [_vp]),
+        "mqw_measure_peaks": (i, [_vp, _P(TierPeaks)]),
         "mqw_mlp_linear_forward": (i, [i, i, i, _vp, _vp, _vp, _vp, i, _vp]),
         "mqw_mlp_linear_backward": (i, [i, i, i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, i, _vp]),
         "mqw_mlp_adam": (i, [i, _vp, _vp, _vp, _vp, _vp, f, f, f, f, f, i, _vp]),
@@ -344,6 +357,12 @@ class Context:
                                               _ptr(el, ctypes.c_uint32), ctypes.byref(stats)))
         del keep
         return {"p": p, "total_t": tt, "e_loc": el, "stats": stats.as_dict()}
+
+    def measure_peaks(self) -> dict:
+        """Measured GB/s of L2 (read, copy), shared memory and HBM (copy)."""
+        t = TierPeaks()
+        _check(self.h, lib().mqw_measure_peaks(self.h, ctypes.byref(t)))
+        return t.as_dict()
 
     def grid_shape(self, n: int, precision="fp32") -> dict:
         """The autotuned grid-path shape for n-spin walks (tunes on first use)."""

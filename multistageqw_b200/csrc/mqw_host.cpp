@@ -1424,6 +1424,15 @@ mqw_status mqw_plan_results(mqw_plan* plan, double* p_out, float* total_t,
   return MQW_OK;
 }
 
+mqw_status mqw_measure_peaks(mqw_ctx* ctx, mqw_tier_peaks* out) {
+  mqw_status st = check_ctx(ctx);
+  if (st != MQW_OK) return st;
+  if (!out) return fail(ctx, MQW_ERR_INVALID, "mqw_measure_peaks: null output");
+  CK(measure_tiers(ctx->stream, ctx->sm_count, &out->l2_read_gbs, &out->l2_copy_gbs,
+                   &out->smem_gbs, &out->hbm_copy_gbs));
+  return MQW_OK;
+}
+
 mqw_status mqw_selftest_wait_timeout(mqw_ctx* ctx) {
   mqw_status st = check_ctx(ctx);
   if (st != MQW_OK) return st;

@@ -52,6 +52,11 @@ cudaError_t launch_diag(int n, int count, const double* raw, float* hp,
                         double* energies, DiagOut* out, void* scratch,
                         cudaStream_t stream);
 
+// Bandwidth probes (GB/s) of L2 (read; copy), shared memory (read) and HBM
+// (copy); allocates and frees ~2 GB of probe buffers.
+cudaError_t measure_tiers(cudaStream_t st, int sm_count, double* l2_read_gbs,
+                          double* l2_copy_gbs, double* smem_gbs, double* hbm_copy_gbs);
+
 // Moments mean(hp^k), k = 1..4, of a 2^n diagonal into the last four
 // doubles of `scratch` (moments_scratch_bytes()).
 size_t moments_scratch_bytes();

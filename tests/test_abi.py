@@ -131,7 +131,8 @@ def test_struct_layouts_match_header(tmp_path):
         pytest.skip("no C compiler")
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     structs = {"mqw_options": M.Options, "mqw_run_stats": M.RunStats,
-               "mqw_diag_info": M.DiagInfo, "mqw_grid_shape": M.GridShape}
+               "mqw_diag_info": M.DiagInfo, "mqw_grid_shape": M.GridShape,
+               "mqw_tier_peaks": M.TierPeaks}
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "mqw.h"', "int main(void) {"]
     for name, cls in structs.items():
         lines.append(f'  printf("{name} %zu\\n", sizeof({name}));')

@@ -412,3 +412,12 @@ def test_basis_build_ahead_gives_identical_results(ctx, orc, mqw):
     assert r.returncode == 0, r.stderr[-2000:]
     got = np.array(json.loads(r.stdout.strip().splitlines()[-1]))
     assert np.array_equal(got, ref)
+
+
+def test_tier_peaks(ctx):
+    """The bandwidth probes: shared memory above L2 above HBM, HBM within
+    reach of the B200's nominal 7.7 TB/s."""
+    t = ctx.measure_peaks()
+    assert 2000 < t["hbm_copy_gbs"] < 9000, t
+    assert t["l2_read_gbs"] > t["hbm_copy_gbs"], t
+    assert t["smem_gbs"] > t["l2_read_gbs"], t
