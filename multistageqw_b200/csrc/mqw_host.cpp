@@ -59,11 +59,6 @@ struct DevMem {
   template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 
-// A context owns the reusable device scratch that plans share: the grid-path
-// state slots, norm partials, the coefficient pool and its tables, and the
-// diagonal's chunk partials. Plans of one context are executed one at a time
-// (the ABI's threading rule), so sharing is safe and repeated calls do not
-// pay for allocation.
 // Grid-path shape for one (precision, n): tile cap, walks per launch, and
 // concurrent launch lanes.
 struct GridShape {
@@ -75,6 +70,11 @@ struct GridShape {
 };
 constexpr int kMaxLanes = 4;
 
+// A context owns the reusable device scratch that plans share: the grid-path
+// state slots, norm partials, the coefficient pool and its tables, and the
+// diagonal's chunk partials. Plans of one context are executed one at a time
+// (the ABI's threading rule), so sharing is safe and repeated calls do not
+// pay for allocation.
 struct mqw_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -1700,7 +1700,7 @@ mqw_status mqw_multiqw(mqw_ctx* ctx, int n, int m, const char* filename,
   mqw_status s = check_ctx(ctx);
   if (s != MQW_OK) return s;
   if (!filename || n < 1 || n > MQW_MAX_N || m < 1 || m > MQW_MAX_M || start < 0 ||
-      problems < 0 || problems > (1ll << 31))
+      problems < 0 || problems > 0x7fffffffll)  // run_problems takes an int count
     return fail(ctx, MQW_ERR_INVALID, "multiqw: bad arguments");
   std::vector<double> raw((size_t)problems * params_per(n));
   s = mqw_read_instances(filename, n, start, problems, raw.data());
