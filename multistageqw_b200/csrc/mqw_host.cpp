@@ -67,6 +67,7 @@ struct GridShape {
   int lane_smem = 0;  // lane axes: 1 shared memory, -1 shuffles, 0 (want): any
   int tma = 0;        // staging: 1 bulk copies, -1 cp.async, 0 (want): any
   double us = 0.0;  // timed microseconds per walk-pass (0: not timed)
+  int bgroup = 1;   // walks per shared-basis group (>= group; set by the plan)
 };
 constexpr int kMaxLanes = 4;
 
@@ -497,22 +498,33 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
 // even r and y for odd r), otherwise it is updated in place, which keeps a
 // walk at 3 vectors so that two walks of n = 20 stay resident in L2. Pass r
 // uses tiling 1 for even r and tiling 2 for odd r.
+// `widx` (at most `gmax` walks) is a basis group: its stage-1 recombination
+// and its last-stage projection are one launch each, so that every basis
+// vector is read once per group; the recurrence stages run in pass groups of
+// `G` consecutive walks, each pass group through all of its stages before
+// the next starts (its states stay L2-resident meanwhile). Without bases,
+// `widx` is one pass group.
 // `lane` selects the lane's own slice of the shared scratch (state, norm
-// partials, kappa), sized for groups of `gmax` walks.
+// partials, kappa), sized for `gmax` walks.
 // With `basis` set (the instance's stage-1 basis of Kb vectors), the first
 // stage is recombined from it instead of run as a recurrence per walk; with
 // `last` set (the last-stage basis of Kl vectors from e_{E_loc}), the last
 // stage is a projection onto it that yields P directly. `proj` is the lane's
 // projection scratch.
 mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
-                          const PassGeomHost& geo, int lane, int gmax,
+                          const PassGeomHost& geo, int lane, int G, int gmax,
                           const float* basis, int Kb, const float* last, int Kl,
                           double* proj, cudaStream_t stream) {
   mqw_ctx* ctx = P.ctx;
   const int n = P.walks[widx[0]].n;
   const size_t N = (size_t)1 << n;
   const int tiles = (int)(N >> geo.L);
-  const int G = (int)widx.size();
+  // The recombination kernels use blocks of 2^rL amplitudes (enough blocks
+  // for whole waves at one block per SM); a walk's norm partials are laid
+  // out with the larger count of the two.
+  const int rL = std::min(geo.L, kRecombineLog);
+  const int rtiles = (int)(N >> rL);
+  const int W = (int)widx.size();
   const size_t amp = P.precision == 0 ? 8 : 16;
   const int slots = walk_slots(geo);
   char* base = P.ctx->state.as<char>() + (size_t)lane * gmax * slots * N * amp;
@@ -522,127 +534,31 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
   int pi[kMaxGroup], xs[kMaxGroup];
   const int ps = 2;
   const int ys = geo.nu > 0 ? 3 : -1;  // -1: b in place
-  for (int g = 0; g < G; g++) {
+  for (int g = 0; g < W; g++) {
     pi[g] = 0;
     xs[g] = 1;
   }
-  double* norm_part = P.ctx->norm_part.as<double>() + (size_t)lane * gmax * tiles;
+  double* norm_part = P.ctx->norm_part.as<double>() + (size_t)lane * gmax * rtiles;
   double* kappa = P.ctx->kappa.as<double>() + (size_t)lane * kMaxGroup;
   double* p_sample = P.d_p_sample.as<double>();
   const float* coef = P.d_coef.as<float>();
   const float* hp = P.d_hp.as<float>();
   const DiagOut* diag = P.d_diag.as<DiagOut>();
-  int max_stages = 0;
-  for (int g = 0; g < G; g++) max_stages = std::max(max_stages, P.walks[widx[g]].stages);
-  for (int st = 0; st < max_stages; st++) {
-    int K[kMaxGroup], Kmax = 0;
-    for (int g = 0; g < G; g++) {
-      const ResidentWalk& w = P.walks[widx[g]];
-      K[g] = st < w.stages ? P.degree[w.stage_desc_off + st] : 0;
-      Kmax = std::max(Kmax, K[g]);
-    }
-    if (last && st == max_stages - 1 && st > 0) {
-      ProjectParams pr{};
-      pr.basis = last;
-      pr.n = n;
-      pr.L = geo.L;
-      pr.Kb = Kl;
-      pr.count = G;
-      pr.part = proj;
-      for (int g = 0; g < G; g++) {
-        const ResidentWalk& w = P.walks[widx[g]];
-        const int job = w.stage_desc_off + st;
-        ProjectWalk& Q = pr.walk[g];
-        Q.coef = coef + P.coef_off[job];
-        Q.K = K[g];
-        Q.psi = buf(g, pi[g]);
-        Q.kappa = kappa + g;
-        Q.p_out = p_sample + w.p_off;
-      }
-      CK(launch_project(pr, stream));
-      if (P.counting) {
-        P.stats.launches += 2;
-        // each walk reads the basis slice and its state once
-        P.stats.aux_bytes += (double)G * ((double)Kl * N * 4.0 + (double)N * 8.0);
-      }
-      break;  // the walks' P are written; nothing follows the last stage
-    }
-    if (st == 0 && basis) {
-      CombineParams cp{};
-      cp.basis = basis;
-      cp.n = n;
-      cp.L = geo.L;
-      cp.Kb = Kb;
-      cp.count = G;
-      for (int g = 0; g < G; g++) {
-        const int job = P.walks[widx[g]].stage_desc_off;
-        CombineWalk& C = cp.walk[g];
-        C.coef = coef + P.coef_off[job];
-        C.K = K[g];
-        C.out = buf(g, xs[g]);
-        C.norm_part = norm_part + (size_t)g * tiles;
-      }
-      CK(launch_combine(P.precision, cp, stream));
-      if (P.counting) {
-        P.stats.launches++;
-        // the basis once per group, one complex state written per walk
-        P.stats.aux_bytes += (double)Kb * N * 4.0 + (double)G * N * 8.0;
-      }
-      Kmax = 0;  // no recurrence passes for this stage
-    }
-    for (int r = Kmax - 1; r >= 0; r--) {
-      PassParams pp{};
-      pp.n = n;
-      pp.L = geo.L;
-      pp.C = geo.C;
-      pp.threads = geo.threads;
-      pp.lane_smem = geo.lane_smem;
-      pp.tma = geo.tma;
-      pp.err = ctx->dev_err.as<unsigned>();
-      pp.comp = P.comp;
-      pp.a = geo.a;
-      pp.tiling = (r & 1) ? 2 : 1;
-      pp.count = G;
-      for (int g = 0; g < G; g++) {
-        PassWalk& W = pp.walk[g];
-        const ResidentWalk& w = P.walks[widx[g]];
-        W.active = r < K[g];
-        if (!W.active) continue;
-        const int job = w.stage_desc_off + st;
-        if (ys < 0) {
-          W.bin = W.bout = buf(g, xs[g]);
-        } else {
-          W.bin = buf(g, (r & 1) ? xs[g] : ys);
-          W.bout = buf(g, (r & 1) ? ys : xs[g]);
-        }
-        W.part = buf(g, ps);
-        W.psi = buf(g, pi[g]);
-        W.hp = hp + w.hp_off;
-        W.coef = coef + P.coef_off[job];
-        W.kappa = st == 0 ? nullptr : kappa + g;
-        W.norm_part = norm_part + (size_t)g * tiles;
-        W.gamma = P.jobs[job].gamma;
-        W.scale = P.onenorm[job];
-        W.r = r;
-        W.K = K[g];
-        W.psi_uniform = st == 0;  // every walk starts from the uniform state
-        W.psi0 = (float)(1.0 / std::sqrt((double)N));
-        if (P.counting) P.stats.pass_amps += (double)N;
-      }
-      CK(launch_pass(P.precision, pp, stream));
-      if (P.counting) {
-        P.stats.launches++;
-        P.stats.term_launches++;
-      }
-    }
+  auto degree = [&](int g, int st) {
+    const ResidentWalk& w = P.walks[widx[g]];
+    return st < w.stages ? P.degree[w.stage_desc_off + st] : 0;
+  };
+  // Stage-output bookkeeping of walks [g0, g1) after stage st: per-walk
+  // norms (and P where recorded), then the output becomes the next psi.
+  auto finalize = [&](int g0, int g1, int st, int parts) -> mqw_status {
     FinalParams fp{};
     int fc = 0;
-    for (int g = 0; g < G; g++) {
+    for (int g = g0; g < g1; g++) {
       const ResidentWalk& w = P.walks[widx[g]];
       if (st >= w.stages) continue;
       FinalTraj& F = fp.traj[fc++];
-      F.norm_part = norm_part + (size_t)g * tiles;
-      F.tiles = tiles;
+      F.norm_part = norm_part + (size_t)g * rtiles;
+      F.tiles = parts;
       F.kappa = kappa + g;
       F.out = buf(g, xs[g]);
       F.diag = diag + w.inst;
@@ -653,9 +569,126 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
     fp.count = fc;
     CK(launch_finalize(P.precision, fp, stream));
     if (P.counting) P.stats.launches++;
-    for (int g = 0; g < G; g++) {
+    for (int g = g0; g < g1; g++) {
       if (st >= P.walks[widx[g]].stages) continue;
       std::swap(pi[g], xs[g]);  // the output (slot x) becomes psi
+    }
+    return MQW_OK;
+  };
+  int max_stages = 0;
+  for (int g = 0; g < W; g++) max_stages = std::max(max_stages, P.walks[widx[g]].stages);
+  // The bases are used only by groups of one instance with the same m
+  // (>= 2), which issue_rest guarantees.
+  const bool combine = basis != nullptr;
+  const bool project = last != nullptr && max_stages > 1;
+  if (combine) {
+    CombineParams cp{};
+    cp.basis = basis;
+    cp.n = n;
+    cp.L = rL;
+    cp.Kb = Kb;
+    cp.count = W;
+    for (int g = 0; g < W; g++) {
+      const int job = P.walks[widx[g]].stage_desc_off;
+      CombineWalk& C = cp.walk[g];
+      C.coef = coef + P.coef_off[job];
+      C.K = degree(g, 0);
+      C.out = buf(g, xs[g]);
+      C.norm_part = norm_part + (size_t)g * rtiles;
+    }
+    CK(launch_combine(P.precision, cp, stream));
+    if (P.counting) {
+      P.stats.launches++;
+      // the basis once per group, one complex state written per walk
+      P.stats.aux_bytes += (double)Kb * N * 4.0 + (double)W * N * 8.0;
+    }
+    mqw_status s = finalize(0, W, 0, rtiles);
+    if (s != MQW_OK) return s;
+  }
+  // Recurrence stages [combine, end) of each pass group.
+  for (int g0 = 0; g0 < W; g0 += G) {
+    const int g1 = std::min(W, g0 + G);
+    int end = 0;
+    for (int g = g0; g < g1; g++) end = std::max(end, P.walks[widx[g]].stages);
+    if (project) end = max_stages - 1;
+    for (int st = combine ? 1 : 0; st < end; st++) {
+      int K[kMaxGroup], Kmax = 0;
+      for (int g = g0; g < g1; g++) {
+        K[g - g0] = degree(g, st);
+        Kmax = std::max(Kmax, K[g - g0]);
+      }
+      for (int r = Kmax - 1; r >= 0; r--) {
+        PassParams pp{};
+        pp.n = n;
+        pp.L = geo.L;
+        pp.C = geo.C;
+        pp.threads = geo.threads;
+        pp.lane_smem = geo.lane_smem;
+        pp.tma = geo.tma;
+        pp.err = ctx->dev_err.as<unsigned>();
+        pp.comp = P.comp;
+        pp.a = geo.a;
+        pp.tiling = (r & 1) ? 2 : 1;
+        pp.count = g1 - g0;
+        for (int g = g0; g < g1; g++) {
+          PassWalk& Wk = pp.walk[g - g0];
+          const ResidentWalk& w = P.walks[widx[g]];
+          Wk.active = r < K[g - g0];
+          if (!Wk.active) continue;
+          const int job = w.stage_desc_off + st;
+          if (ys < 0) {
+            Wk.bin = Wk.bout = buf(g, xs[g]);
+          } else {
+            Wk.bin = buf(g, (r & 1) ? xs[g] : ys);
+            Wk.bout = buf(g, (r & 1) ? ys : xs[g]);
+          }
+          Wk.part = buf(g, ps);
+          Wk.psi = buf(g, pi[g]);
+          Wk.hp = hp + w.hp_off;
+          Wk.coef = coef + P.coef_off[job];
+          Wk.kappa = st == 0 ? nullptr : kappa + g;
+          Wk.norm_part = norm_part + (size_t)g * rtiles;
+          Wk.gamma = P.jobs[job].gamma;
+          Wk.scale = P.onenorm[job];
+          Wk.r = r;
+          Wk.K = K[g - g0];
+          Wk.psi_uniform = st == 0;  // every walk starts from the uniform state
+          Wk.psi0 = (float)(1.0 / std::sqrt((double)N));
+          if (P.counting) P.stats.pass_amps += (double)N;
+        }
+        CK(launch_pass(P.precision, pp, stream));
+        if (P.counting) {
+          P.stats.launches++;
+          P.stats.term_launches++;
+        }
+      }
+      mqw_status s = finalize(g0, g1, st, tiles);
+      if (s != MQW_OK) return s;
+    }
+  }
+  if (project) {
+    const int st = max_stages - 1;
+    ProjectParams pr{};
+    pr.basis = last;
+    pr.n = n;
+    pr.L = rL;
+    pr.Kb = Kl;
+    pr.count = W;
+    pr.part = proj;
+    for (int g = 0; g < W; g++) {
+      const ResidentWalk& w = P.walks[widx[g]];
+      ProjectWalk& Q = pr.walk[g];
+      Q.coef = coef + P.coef_off[w.stage_desc_off + st];
+      Q.K = degree(g, st);
+      Q.psi = buf(g, pi[g]);
+      Q.kappa = kappa + g;
+      Q.p_out = p_sample + w.p_off;
+    }
+    CK(launch_project(pr, stream));
+    if (P.counting) {
+      P.stats.launches += 2;
+      // the basis once per group, each walk's state once
+      P.stats.aux_bytes += (double)Kl * N * 4.0 + (double)W * N * 8.0;
     }
   }
   return MQW_OK;
@@ -878,9 +911,16 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
       const float* basis = bk.Kb ? B.real1() : nullptr;
       const float* lastb = bk.Kl ? B.real2() : nullptr;
       // Groups are dealt round-robin to the lanes, which run concurrently.
+      // With shared bases a group is a basis group of up to gs.bgroup walks
+      // (pass groups of G inside it), and the block's walks are split into
+      // lanes x k groups of near-equal size so that the lanes finish
+      // together; otherwise a group is one pass group of G walks.
       const int nw = (int)(bk.b1 - bk.b0);
-      const int ngroups = (nw + G - 1) / G;
-      const int lanes = std::min(gs.lanes, ngroups);
+      const bool shared = bk.Kb || bk.Kl;
+      const int lanes = std::min(gs.lanes, (nw + G - 1) / G);
+      const int per = shared ? std::max(G, gs.bgroup) : G;
+      const int ngroups = shared ? lanes * ((nw + lanes * per - 1) / (lanes * per))
+                                 : (nw + G - 1) / G;
       CK(ctx->fork(stream, lanes));
       // The next block's bases, overlapping this block's walks.
       if (overlap && bi + 1 < blocks.size() && (blocks[bi + 1].Kb || blocks[bi + 1].Kl)) {
@@ -891,14 +931,19 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
         CK(cudaEventRecord(ctx->basis_built[nb], bst));
         built_next = true;
       }
-      for (int i = 0; i < ngroups; i++) {
-        const size_t a = bk.b0 + (size_t)i * G;
-        std::vector<int> grp(ws.begin() + a, ws.begin() + std::min(bk.b1, a + G));
+      size_t a = bk.b0;
+      for (int i = 0; i < ngroups && a < bk.b1; i++) {
+        const size_t size = shared ? (size_t)(nw / ngroups + (i < nw % ngroups ? 1 : 0))
+                                   : std::min((size_t)G, bk.b1 - a);
+        std::vector<int> grp(ws.begin() + a, ws.begin() + a + size);
+        a += size;
+        if (grp.empty()) continue;
         const int lane = i % lanes;
         double* proj = ctx->proj_part.as<double>() +
-                       (size_t)lane * G * std::max(kb2, 1) * (((size_t)1 << n) / 2048) * 2;
-        mqw_status s = run_grid_group(P, grp, geo, lane, G, basis, bk.Kb, lastb, bk.Kl, proj,
-                                      lane == 0 ? stream : ctx->lane_stream[lane]);
+                       (size_t)lane * gs.bgroup *
+                           (((size_t)1 << n) >> std::min(geo.L, kRecombineLog)) * 2;
+        mqw_status s = run_grid_group(P, grp, geo, lane, G, gs.bgroup, basis, bk.Kb, lastb,
+                                      bk.Kl, proj, lane == 0 ? stream : ctx->lane_stream[lane]);
         if (s != MQW_OK) return s;
       }
       CK(ctx->join(stream, lanes));
@@ -974,13 +1019,29 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     const int ngroups = (kv.second + gs.group - 1) / gs.group;
     gs.lanes = std::max(1, std::min(gs.lanes, ngroups));
     const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, gs.tma > 0);
+    // Walks per shared-basis group: the stage-1 recombination and the
+    // last-stage projection read each basis vector once per group, so the
+    // group is as large as the launch structures allow (kMaxGroup) within a
+    // state budget of a quarter of the free memory (16 GB at most).
+    // MQW_BASIS_GROUP caps it (1: one basis read per pass group).
+    gs.bgroup = gs.group;
+    if ((P.opt.stage1_basis || P.opt.final_projection) && P.precision == 0 && !P.comp) {
+      size_t free_b = 0, total_b = 0;
+      if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = (size_t)8 << 30;
+      const size_t budget = std::min(free_b / 4, (size_t)16 << 30);
+      int bg = std::min(kMaxGroup, kv.second);
+      if (const char* e = getenv("MQW_BASIS_GROUP")) bg = std::min(bg, std::max(1, atoi(e)));
+      while (bg > gs.group && (size_t)gs.lanes * bg * walk_bytes(P.precision, geo, n) > budget)
+        bg--;
+      gs.bgroup = std::max(gs.group, bg);
+    }
     P.grid_geo[n] = gs;
     lanes_max = std::max(lanes_max, gs.lanes);
     const size_t N = (size_t)1 << n;
     const size_t amp = P.precision == 0 ? 8 : 16;
-    const size_t walks = (size_t)gs.lanes * gs.group;
+    const size_t walks = (size_t)gs.lanes * gs.bgroup;
     state_b = std::max(state_b, walks * walk_slots(geo) * N * amp);
-    norm_b = std::max(norm_b, walks * (N >> geo.L) * sizeof(double));
+    norm_b = std::max(norm_b, walks * (N >> std::min(geo.L, kRecombineLog)) * sizeof(double));
   }
   CK(ctx->ensure_lanes(lanes_max));
   CK(ctx->grow(ctx->diag_scratch, P.diag_scratch_bytes));
@@ -1027,8 +1088,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
   }
   // Shared bases (FP32): the largest first- and last-stage degrees per n
   // decide the buffers; an n whose bases would not fit the budget drops the
-  // last-stage basis first, then the stage-1 basis. The last-stage
-  // projection needs tiles of at least 2^10 amplitudes.
+  // last-stage basis first, then the stage-1 basis.
   P.basis_kb1.clear();
   P.basis_kb2.clear();
   const bool want1 = P.opt.stage1_basis && P.precision == 0 && !P.comp;
@@ -1055,16 +1115,17 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads,
                                          gs.lane_smem > 0, gs.tma > 0);
       int k1 = want1 && e.second.first <= kMaxBasis ? e.second.first : 0;
-      int k2 = want2 && n >= 11 && e.second.second <= kMaxBasis ? e.second.second : 0;
+      int k2 = want2 && e.second.second <= kMaxBasis ? e.second.second : 0;
       if (BasisLayout::bytes(n, k1, k2) > budget) k2 = 0;
       if (BasisLayout::bytes(n, k1, k2) > budget) k1 = 0;
       if (!k1 && !k2) continue;
       P.basis_kb1[n] = k1;
       P.basis_kb2[n] = k2;
       basis_b = std::max(basis_b, BasisLayout::bytes(n, k1, k2));
-      // projection partials: per lane, per walk, per 2048-amplitude block
-      proj_b = std::max(proj_b, (size_t)gs.lanes * gs.group * std::max(k2, 1) *
-                                    (((size_t)1 << n) / 2048) * 2 * sizeof(double));
+      // projection partials: per lane, per walk, per recombination block
+      proj_b = std::max(proj_b, (size_t)gs.lanes * gs.bgroup *
+                                    (((size_t)1 << n) >> std::min(geo.L, kRecombineLog)) *
+                                    2 * sizeof(double));
       rmax = std::max(rmax, std::max(k1 + (k1 & 1), k2 + (k2 & 1)));
     }
     P.basis_buffers = 1;

@@ -195,6 +195,7 @@ struct CombineParams {
   CombineWalk walk[kMaxGroup];
 };
 constexpr int kMaxBasis = 1024;  // basis vectors (stage-1 degree bound)
+constexpr int kRecombineLog = 10;  // amplitudes per recombination block (log2, at most)
 // Last-stage projection. Only |psi_out[E_loc]|^2 of a walk's last stage is
 // used, and H~ is real symmetric, so
 //   psi_out[E_loc] = sum_k c_k (T_k(H~) psi)[E_loc] = sum_j d_j <w_j, psi>
@@ -202,7 +203,9 @@ constexpr int kMaxBasis = 1024;  // basis vectors (stage-1 degree bound)
 // pass_kernel recurrence started from the unit vector at E_loc) and d_j the
 // stage-1 recombination weights of the walk's last-stage coefficients. The
 // output norm is taken as the input norm: |f_K(x)| = 1 +- the 1e-6 tail on
-// [-1, 1], so P moves by at most 2e-6 relative.
+// [-1, 1], so P moves by at most 2e-6 relative. With w_j real,
+// sum_j d_j <w_j, psi> = <v, psi> for v = sum_j d_j w_j: the projection is
+// the stage-1 recombination of v followed by one dot product with psi.
 struct ProjectWalk {
   const float* coef;   // the walk's last-stage coefficients c_0 .. c_{K-1}
   int K;
@@ -213,7 +216,7 @@ struct ProjectWalk {
 struct ProjectParams {
   const float* basis;  // Kb real FP32 vectors of 2^n amplitudes
   int n, L, Kb, count;
-  double* part;        // scratch: [count][2^n / 2048 blocks][Kb][2] partial dots
+  double* part;        // scratch: [count][2^(n-L) blocks][2] partial <v, psi>
   ProjectWalk walk[kMaxGroup];
 };
 cudaError_t launch_project(const ProjectParams& p, cudaStream_t stream);

@@ -721,18 +721,27 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
 // with evict-first loads (__ldcs), so that they do not push the walks'
 // L2-resident states out of the cache for the passes running beside them.
 
-// Stage-1 recombination of G walks (FP32): block b covers amplitudes
-// [b 2^L, (b+1) 2^L), reads each real basis vector once for all G walks
-// (eight vectors in flight per thread), and leaves the block's |out|^2 in
-// norm_part[b] (fixed order: deterministic).
-template <int G>
-__global__ void __launch_bounds__(256) combine_kernel(CombineParams p) {
+// Recombination from a shared basis for G walks (FP32). Block b covers
+// amplitudes [b 2^L, (b+1) 2^L) and forms, per walk, v = sum_j d_j w_j
+// (d_0 = c_0 - c_2/2, d_j = (c_j - c_{j+2})/2; real for even j, imaginary for
+// odd j) from the real basis vectors w_j, each read once for all G walks
+// with eight vectors in flight per thread.
+//  * Stage-1 recombination (kProject false): v is the walk's stage output;
+//    it is written and the block's |v|^2 is left in norm_part[b].
+//  * Last-stage projection (kProject true): the walk's psi_out[E_loc] =
+//    sum_j d_j <w_j, psi> = <v, psi> (w_j real), so v is dotted with the
+//    walk's stage input psi in FP64 and the block's sum is left in
+//    part[g][b] (re, im); project_final_kernel adds the blocks.
+// All sums run in a fixed order (deterministic), and per walk the
+// arithmetic does not depend on G.
+template <int G, bool kProject, typename Params>
+__global__ void __launch_bounds__(256) recombine_kernel(Params p) {
   __shared__ float sd[G][kMaxBasis];
   __shared__ double s_red[32];
   const int Kb = p.Kb;
   for (int e = threadIdx.x; e < G * Kb; e += blockDim.x) {
     const int g = e / Kb, j = e % Kb;
-    const CombineWalk& W = p.walk[g];
+    const auto& W = p.walk[g];
     const float cj = j < W.K ? W.coef[j] : 0.0f;
     const float cj2 = j + 2 < W.K ? W.coef[j + 2] : 0.0f;
     sd[g][j] = j == 0 ? cj - 0.5f * cj2 : 0.5f * (cj - cj2);
@@ -742,9 +751,9 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineParams p) {
   const size_t chunk = (size_t)1 << p.L;
   const size_t base = (size_t)blockIdx.x * chunk;
   const float* __restrict__ basis = reinterpret_cast<const float*>(p.basis);
-  double nrm[G];
+  double acc[G][2];  // |v|^2 (stage 1) or <v, psi> (re, im; projection)
 #pragma unroll
-  for (int g = 0; g < G; g++) nrm[g] = 0.0;
+  for (int g = 0; g < G; g++) acc[g][0] = acc[g][1] = 0.0;
   for (size_t i = base + 4 * threadIdx.x; i < base + chunk; i += 4 * blockDim.x) {
     float re[G][4], im[G][4];
 #pragma unroll
@@ -755,11 +764,11 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineParams p) {
 #pragma unroll
       for (int g = 0; g < G; g++) {
         const float d = sd[g][j];
-        float* acc = odd ? im[g] : re[g];
-        acc[0] = fmaf(d, w.x, acc[0]);
-        acc[1] = fmaf(d, w.y, acc[1]);
-        acc[2] = fmaf(d, w.z, acc[2]);
-        acc[3] = fmaf(d, w.w, acc[3]);
+        float* a = odd ? im[g] : re[g];
+        a[0] = fmaf(d, w.x, a[0]);
+        a[1] = fmaf(d, w.y, a[1]);
+        a[2] = fmaf(d, w.z, a[2]);
+        a[3] = fmaf(d, w.w, a[3]);
       }
     };
     int j = 0;
@@ -775,157 +784,66 @@ __global__ void __launch_bounds__(256) combine_kernel(CombineParams p) {
       accumulate(__ldcs(reinterpret_cast<const float4*>(basis + (size_t)j * N + i)), j, j & 1);
 #pragma unroll
     for (int g = 0; g < G; g++) {
-      float4* out = reinterpret_cast<float4*>(reinterpret_cast<float*>(p.walk[g].out) + 2 * i);
-      out[0] = make_float4(re[g][0], im[g][0], re[g][1], im[g][1]);
-      out[1] = make_float4(re[g][2], im[g][2], re[g][3], im[g][3]);
+      if constexpr (kProject) {
+        const float* psi = reinterpret_cast<const float*>(p.walk[g].psi) + 2 * i;
+        const float4 a = __ldcs(reinterpret_cast<const float4*>(psi));
+        const float4 b = __ldcs(reinterpret_cast<const float4*>(psi + 4));
+        const float pr[4] = {a.x, a.z, b.x, b.z}, pi[4] = {a.y, a.w, b.y, b.w};
 #pragma unroll
-      for (int k = 0; k < 4; k++)
-        nrm[g] += (double)re[g][k] * re[g][k] + (double)im[g][k] * im[g][k];
+        for (int k = 0; k < 4; k++) {  // (re + i im)(pr + i pi)
+          acc[g][0] = fma((double)re[g][k], (double)pr[k], acc[g][0]);
+          acc[g][0] = fma(-(double)im[g][k], (double)pi[k], acc[g][0]);
+          acc[g][1] = fma((double)re[g][k], (double)pi[k], acc[g][1]);
+          acc[g][1] = fma((double)im[g][k], (double)pr[k], acc[g][1]);
+        }
+      } else {
+        float4* out = reinterpret_cast<float4*>(reinterpret_cast<float*>(p.walk[g].out) + 2 * i);
+        out[0] = make_float4(re[g][0], im[g][0], re[g][1], im[g][1]);
+        out[1] = make_float4(re[g][2], im[g][2], re[g][3], im[g][3]);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+          acc[g][0] += (double)re[g][k] * re[g][k] + (double)im[g][k] * im[g][k];
+      }
     }
   }
 #pragma unroll
   for (int g = 0; g < G; g++) {
-    const double sum = block_sum<float>(nrm[g], s_red);
-    if (threadIdx.x == 0) p.walk[g].norm_part[blockIdx.x] = sum;
-    __syncthreads();  // s_red is reused by the next walk's sum
-  }
-}
-
-// Last-stage projection, partial dots: block b covers the kProjChunk
-// amplitudes [b kProjChunk, (b+1) kProjChunk); each thread holds 8 of them
-// (2 quads) of one walk's psi in registers and, eight basis vectors at a
-// time, accumulates w_j . psi (re, im) in FP64, reduces over the warp with
-// shuffles and leaves the warp's value in shared memory; the warps' values
-// are then summed in a fixed order into part[g][b][j]. The walks of a group
-// are done one after another over the same basis slice.
-constexpr int kProjThreads = 256;
-constexpr int kProjJ = 8;
-constexpr int kProjQuads = 2;
-constexpr size_t kProjChunk = (size_t)4 * kProjThreads * kProjQuads;  // 2048
-__global__ void __launch_bounds__(kProjThreads, 2) project_partial_kernel(ProjectParams p) {
-  constexpr int kWarps = kProjThreads / 32;
-  __shared__ double red[kWarps][kProjJ][2];
-  const int Kb = p.Kb, G = p.count;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const size_t N = (size_t)1 << p.n;
-  const size_t blocks = N / kProjChunk;
-  const size_t base = (size_t)blockIdx.x * kProjChunk;
-  for (int g = 0; g < G; g++) {
-    const float* psi = reinterpret_cast<const float*>(p.walk[g].psi);
-    float4 ps[kProjQuads][2];
+    if constexpr (kProject) {
+      const size_t blocks = N >> p.L;
 #pragma unroll
-    for (int q = 0; q < kProjQuads; q++) {
-      const size_t i = base + 4 * threadIdx.x + (size_t)q * 4 * kProjThreads;
-      ps[q][0] = __ldg(reinterpret_cast<const float4*>(psi + 2 * i));
-      ps[q][1] = __ldg(reinterpret_cast<const float4*>(psi + 2 * i + 4));
-    }
-    for (int j0 = 0; j0 < Kb; j0 += kProjJ) {
-      double acc[kProjJ][2];
-#pragma unroll
-      for (int jj = 0; jj < kProjJ; jj++) acc[jj][0] = acc[jj][1] = 0.0;
-#pragma unroll
-      for (int q = 0; q < kProjQuads; q++) {
-        const size_t i = base + 4 * threadIdx.x + (size_t)q * 4 * kProjThreads;
-        float4 w[kProjJ];
-#pragma unroll
-        for (int jj = 0; jj < kProjJ; jj++)
-          w[jj] = j0 + jj < Kb ? __ldcs(reinterpret_cast<const float4*>(p.basis + (size_t)(j0 + jj) * N + i))
-                               : make_float4(0, 0, 0, 0);
-        const float4 a = ps[q][0], b = ps[q][1];
-#pragma unroll
-        for (int jj = 0; jj < kProjJ; jj++) {
-          acc[jj][0] = fma((double)w[jj].x, (double)a.x, acc[jj][0]);
-          acc[jj][1] = fma((double)w[jj].x, (double)a.y, acc[jj][1]);
-          acc[jj][0] = fma((double)w[jj].y, (double)a.z, acc[jj][0]);
-          acc[jj][1] = fma((double)w[jj].y, (double)a.w, acc[jj][1]);
-          acc[jj][0] = fma((double)w[jj].z, (double)b.x, acc[jj][0]);
-          acc[jj][1] = fma((double)w[jj].z, (double)b.y, acc[jj][1]);
-          acc[jj][0] = fma((double)w[jj].w, (double)b.z, acc[jj][0]);
-          acc[jj][1] = fma((double)w[jj].w, (double)b.w, acc[jj][1]);
-        }
+      for (int c = 0; c < 2; c++) {
+        const double sum = block_sum<float>(acc[g][c], s_red);
+        if (threadIdx.x == 0) p.part[((size_t)g * blocks + blockIdx.x) * 2 + c] = sum;
+        __syncthreads();  // s_red is reused by the next sum
       }
-#pragma unroll
-      for (int jj = 0; jj < kProjJ; jj++)
-#pragma unroll
-        for (int c = 0; c < 2; c++) {
-          double v = acc[jj][c];
-          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-          if (lane == 0) red[warp][jj][c] = v;
-        }
-      __syncthreads();
-      if (threadIdx.x < 2 * kProjJ) {
-        const int jj = threadIdx.x >> 1, c = threadIdx.x & 1;
-        if (j0 + jj < Kb) {
-          double v = 0.0;
-          for (int k = 0; k < kWarps; k++) v += red[k][jj][c];
-          p.part[((((size_t)g * blocks) + blockIdx.x) * Kb + j0 + jj) * 2 + c] = v;
-        }
-      }
-      __syncthreads();
+    } else {
+      const double sum = block_sum<float>(acc[g][0], s_red);
+      if (threadIdx.x == 0) p.walk[g].norm_part[blockIdx.x] = sum;
+      __syncthreads();  // s_red is reused by the next walk's sum
     }
   }
 }
 
-// Last-stage projection, final: one block per walk. For 64 basis vectors at
-// a time, 8 groups of threads sum every 8th block's partial (consecutive
-// threads read consecutive j), the 8 group sums are added in order, and the
-// walk's A = sum_j d_j z_j (d_j real for even j, imaginary for odd j) is
-// accumulated per thread and summed in order at the end: P = |A|^2 kappa^2.
-constexpr int kFinalJ = 64, kFinalGroups = 8;
-__global__ void __launch_bounds__(kFinalJ * kFinalGroups) project_final_kernel(ProjectParams p) {
+// Last-stage projection, final: one block per walk sums the walk's block
+// partials of <v, psi> in a fixed order (strided per thread, then the block
+// sum) and writes P = |<v, psi>|^2 kappa^2.
+__global__ void __launch_bounds__(256) project_final_kernel(ProjectParams p) {
+  __shared__ double s_red[32];
   const int g = blockIdx.x;
   const ProjectWalk& W = p.walk[g];
-  const int Kb = p.Kb;
-  const size_t blocks = ((size_t)1 << p.n) / kProjChunk;
-  const int jj = threadIdx.x % kFinalJ, t = threadIdx.x / kFinalJ;
-  __shared__ double zr_s[kFinalGroups][kFinalJ], zi_s[kFinalGroups][kFinalJ];
-  double are = 0.0, aim = 0.0;
-  for (int j0 = 0; j0 < Kb; j0 += kFinalJ) {
-    const int j = j0 + jj;
-    double zr = 0.0, zi = 0.0;
-    if (j < Kb) {
-      const double* pj = p.part + (((size_t)g * blocks) * Kb + j) * 2;
-      for (size_t b = t; b < blocks; b += kFinalGroups) {
-        const double2 v = *reinterpret_cast<const double2*>(pj + b * Kb * 2);
-        zr += v.x;
-        zi += v.y;
-      }
-    }
-    zr_s[t][jj] = zr;
-    zi_s[t][jj] = zi;
-    __syncthreads();
-    if (t == 0 && j < Kb) {
-      double r = 0.0, i = 0.0;
-      for (int k = 0; k < kFinalGroups; k++) {
-        r += zr_s[k][jj];
-        i += zi_s[k][jj];
-      }
-      const double cj = j < W.K ? (double)W.coef[j] : 0.0;
-      const double cj2 = j + 2 < W.K ? (double)W.coef[j + 2] : 0.0;
-      const double d = j == 0 ? cj - 0.5 * cj2 : 0.5 * (cj - cj2);
-      if (j & 1) {  // i d z
-        are -= d * i;
-        aim += d * r;
-      } else {
-        are += d * r;
-        aim += d * i;
-      }
-    }
-    __syncthreads();
+  const size_t blocks = ((size_t)1 << p.n) >> p.L;
+  const double* part = p.part + (size_t)g * blocks * 2;
+  double re = 0.0, im = 0.0;
+  for (size_t b = threadIdx.x; b < blocks; b += blockDim.x) {
+    re += part[2 * b];
+    im += part[2 * b + 1];
   }
-  if (t == 0) {
-    zr_s[0][jj] = are;
-    zi_s[0][jj] = aim;
-  }
-  __syncthreads();
+  re = block_sum<float>(re, s_red);
+  __syncthreads();  // s_red is reused
+  im = block_sum<float>(im, s_red);
   if (threadIdx.x == 0) {
-    double r = 0.0, i = 0.0;
-    for (int k = 0; k < kFinalJ; k++) {
-      r += zr_s[0][k];
-      i += zi_s[0][k];
-    }
     const double kap = W.kappa ? *W.kappa : 1.0;
-    *W.p_out = (r * r + i * i) * kap * kap;
+    *W.p_out = (re * re + im * im) * kap * kap;
   }
 }
 
@@ -1247,6 +1165,21 @@ cudaError_t launch_pass(int precision, const PassParams& p,
                         : launch_pass_t<double>(p, stream);
 }
 
+template <bool kProject, typename Params>
+void launch_recombine(const Params& p, cudaStream_t stream) {
+  const unsigned blocks = (unsigned)((size_t)1 << (p.n - p.L));
+  switch (p.count) {
+    case 1: recombine_kernel<1, kProject><<<blocks, 256, 0, stream>>>(p); break;
+    case 2: recombine_kernel<2, kProject><<<blocks, 256, 0, stream>>>(p); break;
+    case 3: recombine_kernel<3, kProject><<<blocks, 256, 0, stream>>>(p); break;
+    case 4: recombine_kernel<4, kProject><<<blocks, 256, 0, stream>>>(p); break;
+    case 5: recombine_kernel<5, kProject><<<blocks, 256, 0, stream>>>(p); break;
+    case 6: recombine_kernel<6, kProject><<<blocks, 256, 0, stream>>>(p); break;
+    case 7: recombine_kernel<7, kProject><<<blocks, 256, 0, stream>>>(p); break;
+    default: recombine_kernel<8, kProject><<<blocks, 256, 0, stream>>>(p); break;
+  }
+}
+
 cudaError_t launch_combine(int precision, const CombineParams& p,
                            cudaStream_t stream) {
   if (precision != 0 || p.n < 6 || p.n > kMaxN || p.L < 6 || p.L > p.n || p.Kb < 1 ||
@@ -1256,33 +1189,22 @@ cudaError_t launch_combine(int precision, const CombineParams& p,
     if (p.walk[g].K < 1 || p.walk[g].K > p.Kb || !p.walk[g].coef || !p.walk[g].out ||
         !p.walk[g].norm_part)
       return cudaErrorInvalidValue;
-  const unsigned blocks = (unsigned)((size_t)1 << (p.n - p.L));
-  switch (p.count) {
-    case 1: combine_kernel<1><<<blocks, 256, 0, stream>>>(p); break;
-    case 2: combine_kernel<2><<<blocks, 256, 0, stream>>>(p); break;
-    case 3: combine_kernel<3><<<blocks, 256, 0, stream>>>(p); break;
-    case 4: combine_kernel<4><<<blocks, 256, 0, stream>>>(p); break;
-    case 5: combine_kernel<5><<<blocks, 256, 0, stream>>>(p); break;
-    case 6: combine_kernel<6><<<blocks, 256, 0, stream>>>(p); break;
-    case 7: combine_kernel<7><<<blocks, 256, 0, stream>>>(p); break;
-    default: combine_kernel<8><<<blocks, 256, 0, stream>>>(p); break;
-  }
+  launch_recombine<false>(p, stream);
   return cudaGetLastError();
 }
 
 cudaError_t launch_project(const ProjectParams& p, cudaStream_t stream) {
-  if (p.n < 11 || p.n > kMaxN || p.Kb < 1 || p.Kb > kMaxBasis ||
+  if (p.n < 6 || p.n > kMaxN || p.L < 6 || p.L > p.n || p.Kb < 1 || p.Kb > kMaxBasis ||
       p.count < 1 || p.count > kMaxGroup || !p.basis || !p.part)
     return cudaErrorInvalidValue;
   for (int g = 0; g < p.count; g++)
     if (p.walk[g].K < 1 || p.walk[g].K > p.Kb || !p.walk[g].coef || !p.walk[g].psi ||
         !p.walk[g].p_out)
       return cudaErrorInvalidValue;
-  const unsigned blocks = (unsigned)(((size_t)1 << p.n) / kProjChunk);
-  project_partial_kernel<<<blocks, kProjThreads, 0, stream>>>(p);
+  launch_recombine<true>(p, stream);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
-  project_final_kernel<<<p.count, kFinalJ * kFinalGroups, 0, stream>>>(p);
+  project_final_kernel<<<p.count, 256, 0, stream>>>(p);
   return cudaGetLastError();
 }
 

@@ -414,6 +414,29 @@ def test_basis_build_ahead_gives_identical_results(ctx, orc, mqw):
     assert np.array_equal(got, ref)
 
 
+@pytest.mark.parametrize("n,m,samples", [(16, 3, 11), (20, 4, 8)])
+def test_basis_groups_give_identical_results(ctx, orc, mqw, monkeypatch, n, m, samples):
+    """The stage-1 recombination and the last-stage projection of a basis
+    group of walks read each basis vector once for all of them; per walk the
+    arithmetic is the one of a group of one (the FP32 sums in the same order;
+    FP64 norms to within their rounding), so per-sample P matches basis groups
+    of one walk (MQW_BASIS_GROUP=1, read at every plan) to 1e-12."""
+    raw = orc.sk_instances(n, 1, 4200 + n)
+
+    def run():
+        plan = mqw.Plan(ctx, n, m, raw, samples=samples, group=1, lanes=2, graph=0)
+        plan.execute()
+        ps = plan.results(per_sample=True)["p_sample"]
+        plan.close()
+        return ps
+
+    grouped = run()
+    monkeypatch.setenv("MQW_BASIS_GROUP", "1")
+    single = run()
+    np.testing.assert_allclose(grouped, single, rtol=1e-12, atol=0.0)
+    assert np.all(grouped > 0.0) and np.all(grouped <= 1.0)
+
+
 def test_tier_peaks(ctx):
     """The bandwidth probes: shared memory above L2 above HBM, HBM within
     reach of the B200's nominal 7.7 TB/s."""
