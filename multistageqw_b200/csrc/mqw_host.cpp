@@ -102,6 +102,9 @@ struct mqw_ctx {
     return e;
   }
   DevMem proj_part;  // last-stage projection partial dots, per lane
+  // Stage-2 product basis: the Y vectors, every walk's planar stage-2
+  // output, and the coefficient matrices (one instance at a time).
+  DevMem s2y, s2psi, s2c;
   // Bumped whenever a shared scratch buffer is reallocated: a plan's captured
   // graph holds the old addresses and is re-captured when this changes.
   unsigned long long scratch_gen = 1;
@@ -231,6 +234,11 @@ struct mqw_plan {
   // read ([0, ..., 0, 1]).
   std::map<int, int> basis_kb1, basis_kb2;
   int basis_buffers = 1;  // 2: the next instance's bases are built ahead
+  // Stage-2 product basis per n: the largest stage-2 degree (absent: not
+  // used for that n) and the walk capacity of ctx->s2psi.
+  std::map<int, int> s2_k2;
+  int s2_walks = 0;
+  int s2_mode = -1;  // MQW_STAGE2_BASIS: -1 auto, 0 off, 1 whenever it fits
   DevMem d_unit;
   int unit_len = 0;
   // CUDA graph of the whole device pipeline, replayed by later executes.
@@ -514,7 +522,8 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
 mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
                           const PassGeomHost& geo, int lane, int G, int gmax,
                           const float* basis, int Kb, const float* last, int Kl,
-                          double* proj, cudaStream_t stream) {
+                          double* proj, const float* ext_re, const float* ext_im,
+                          cudaStream_t stream) {
   mqw_ctx* ctx = P.ctx;
   const int n = P.walks[widx[0]].n;
   const size_t N = (size_t)1 << n;
@@ -580,6 +589,23 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
   // The bases are used only by groups of one instance with the same m
   // (>= 2), which issue_rest guarantees.
   const bool combine = basis != nullptr;
+  const bool ext = ext_re != nullptr;  // stage-2 outputs given (planar)
+  if (ext) {
+    UnpackParams up{};
+    up.n = n;
+    up.L = rL;
+    up.count = W;
+    for (int g = 0; g < W; g++)
+      up.walk[g] = UnpackWalk{ext_re + (size_t)g * N, ext_im + (size_t)g * N, buf(g, xs[g]),
+                              norm_part + (size_t)g * rtiles};
+    CK(launch_unpack(up, stream));
+    if (P.counting) {
+      P.stats.launches++;
+      P.stats.aux_bytes += (double)W * N * 16.0;
+    }
+    mqw_status s = finalize(0, W, 1, rtiles);
+    if (s != MQW_OK) return s;
+  }
   const bool project = last != nullptr && max_stages > 1;
   if (combine) {
     CombineParams cp{};
@@ -611,7 +637,7 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
     int end = 0;
     for (int g = g0; g < g1; g++) end = std::max(end, P.walks[widx[g]].stages);
     if (project) end = max_stages - 1;
-    for (int st = combine ? 1 : 0; st < end; st++) {
+    for (int st = ext ? 2 : (combine ? 1 : 0); st < end; st++) {
       int K[kMaxGroup], Kmax = 0;
       for (int g = g0; g < g1; g++) {
         K[g - g0] = degree(g, st);
@@ -711,30 +737,35 @@ struct BasisLayout {
   }
 };
 
-// Builds the real basis w_j = U_j(H~) v, j < Kb, of stage `stage` of the
-// instance of walk w0 into `real` (Kb vectors of 2^n floats): v is the
-// uniform state for the first stage and e_{E_loc} for the last. Kb
-// single-walk passes with c = [0, .., 0, 1] at an even top index R >= Kb, so
-// that b_R = v and every later pass is b_r = 2 H~ b_{r+1} - b_{r+2}; each
-// pass also stores Re(b_r) as w_j (the imaginary parts stay 0). The passes
-// stop at r = R - Kb + 1 >= 1 (the r = 0 form is never used).
-mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
-                       const BasisLayout& B, const PassGeomHost& geo, float* real,
+// State slots of one unit-coefficient pass chain: the partial P, the
+// recurrence vector b (b[1] only when axes are read from global memory) and
+// the start vector (not read when `uniform`: the uniform state).
+struct ChainSlots {
+  void* part;
+  void* b[2];
+  const void* start;
+  bool uniform;
+};
+
+// One unit-coefficient pass chain: w_j = U_j(H~) v, j < K, for the operator of
+// stage `stage` of the instance of walk w0 and the start vector v of `S`,
+// Re(w_j) stored at out_of(j) (real FP32, 2^n floats). K single-walk passes
+// with c = [0, .., 0, 1] at an even top index R >= K, so that b_R = v and
+// every later pass is b_r = 2 H~ b_{r+1} - b_{r+2}; each pass also stores
+// Re(b_r). The passes stop at r = R - K + 1 >= 1 (the r = 0 form is never
+// used).
+template <typename OutOf>
+mqw_status issue_chain(mqw_plan& P, const ResidentWalk& w0, int stage, int K,
+                       const ChainSlots& S, const PassGeomHost& geo, OutOf out_of,
                        cudaStream_t stream) {
   mqw_ctx* ctx = P.ctx;
-  const int n = w0.n;
-  const size_t N = (size_t)1 << n;
-  const bool from_eloc = stage > 0;
-  if (from_eloc) {
-    CK(launch_unit_eloc(B.slot(3), n, P.d_diag.as<DiagOut>() + w0.inst, stream));
-    if (P.counting) P.stats.launches++;
-  }
-  const int R = Kb + (Kb & 1);
+  const size_t N = (size_t)1 << w0.n;
+  const int R = K + (K & 1);
   const int job = w0.stage_desc_off + stage;
   const float* unit = P.d_unit.as<float>() + (P.unit_len - 1 - R);
-  for (int j = 0; j < Kb; j++) {
+  for (int j = 0; j < K; j++) {
     PassParams pp{};
-    pp.n = n;
+    pp.n = w0.n;
     pp.L = geo.L;
     pp.C = geo.C;
     pp.threads = geo.threads;
@@ -747,13 +778,13 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
     PassWalk& W = pp.walk[0];
     W.active = 1;
     if (geo.nu == 0) {
-      W.bin = W.bout = B.slot(1);  // in place
+      W.bin = W.bout = S.b[0];  // in place
     } else {
-      W.bin = B.slot(1 + ((j + 1) & 1));  // not read by the first pass
-      W.bout = B.slot(1 + (j & 1));
+      W.bin = S.b[(j + 1) & 1];  // not read by the first pass
+      W.bout = S.b[j & 1];
     }
-    W.part = B.slot(0);
-    W.psi = B.slot(3);  // read only for e_{E_loc}
+    W.part = S.part;
+    W.psi = S.start;
     W.hp = P.d_hp.as<float>() + w0.hp_off;
     W.coef = unit;
     W.kappa = nullptr;
@@ -762,9 +793,9 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
     W.scale = P.onenorm[job];
     W.r = R - j;
     W.K = R + 1;
-    W.psi_uniform = from_eloc ? 0 : 1;
+    W.psi_uniform = S.uniform ? 1 : 0;
     W.psi0 = (float)(1.0 / std::sqrt((double)N));
-    W.real_out = real + (size_t)j * N;
+    W.real_out = out_of(j);
     CK(launch_pass(P.precision, pp, stream));
     if (P.counting) {
       P.stats.launches++;
@@ -775,6 +806,97 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
   }
   return MQW_OK;
 }
+
+// Builds the real basis w_j = U_j(H~) v, j < Kb, of stage `stage` of the
+// instance of walk w0 into `real` (Kb vectors of 2^n floats): v is the
+// uniform state for the first stage and e_{E_loc} for the last.
+mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
+                       const BasisLayout& B, const PassGeomHost& geo, float* real,
+                       cudaStream_t stream) {
+  const size_t N = (size_t)1 << w0.n;
+  const bool from_eloc = stage > 0;
+  if (from_eloc) {
+    mqw_ctx* ctx = P.ctx;
+    CK(launch_unit_eloc(B.slot(3), w0.n, P.d_diag.as<DiagOut>() + w0.inst, stream));
+    if (P.counting) P.stats.launches++;
+  }
+  const ChainSlots S{B.slot(0), {B.slot(1), B.slot(2)}, B.slot(3), !from_eloc};
+  return issue_chain(P, w0, stage, Kb, S, geo, [&](int j) { return real + (size_t)j * N; },
+                     stream);
+}
+
+// The stage-2 product basis of one instance (FP32): Y_jk = U_k(H~_2) w_j for
+// the Kb stage-1 basis vectors w_j (in `basis`) and k < K2, one chain of K2
+// passes per w_j, dealt round-robin to `lanes` lanes (each on its own walk
+// slots of the shared state), then the coefficient matrices and the GEMM
+// that leave every walk's stage-2 output, planar, in ctx->s2psi.
+mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size_t b1,
+                        const float* basis, int Kb, int K2, const PassGeomHost& geo,
+                        int lanes, int gmax, cudaStream_t stream) {
+  mqw_ctx* ctx = P.ctx;
+  const ResidentWalk& w0 = P.walks[ws[b0]];
+  const int n = w0.n;
+  const size_t N = (size_t)1 << n;
+  const int nw = (int)(b1 - b0);
+  const S2Layout lay{Kb, K2};
+  float* Y = ctx->s2y.as<float>();
+  const int slots = walk_slots(geo);
+  CK(ctx->fork(stream, lanes));
+  for (int j = 0; j < Kb; j++) {
+    const int lane = j % lanes;
+    cudaStream_t st = lane == 0 ? stream : ctx->lane_stream[lane];
+    char* base = ctx->state.as<char>() + (size_t)lane * gmax * slots * N * 8;
+    auto slot = [&](int k) -> void* { return base + (size_t)k * N * 8; };
+    const ChainSlots S{slot(0), {slot(1), slot(2)}, slot(slots - 1), false};
+    CK(launch_real_to_complex(slot(slots - 1), basis + (size_t)j * N, n, st));
+    if (P.counting) {
+      P.stats.launches++;
+      P.stats.aux_bytes += (double)N * 12.0;
+    }
+    auto out_of = [&](int k) {
+      const int h = (j + k) & 1;
+      return Y + ((size_t)(h ? lay.rows(0) : 0) + lay.index(j, k)) * N;
+    };
+    mqw_status s = issue_chain(P, w0, 1, K2, S, geo, out_of, st);
+    if (s != MQW_OK) return s;
+  }
+  CK(ctx->join(stream, lanes));
+  const int col_stride = ((nw + 127) / 128) * 128;
+  S2CoefParams cp{};
+  cp.stages = P.d_stages.as<StageDesc>();
+  cp.coef = P.d_coef.as<float>();
+  cp.job0 = w0.stage_desc_off;
+  cp.m = w0.stages;
+  cp.walks = nw;
+  cp.col_stride = col_stride;
+  cp.lay = lay;
+  cp.rows_pad[0] = (lay.rows(0) + 7) / 8 * 8;
+  cp.rows_pad[1] = (lay.rows(1) + 7) / 8 * 8;
+  cp.C0 = ctx->s2c.as<float>();
+  cp.C1 = cp.C0 + (size_t)cp.rows_pad[0] * col_stride;
+  CK(launch_s2_coef(cp, stream));
+  S2GemmParams gp{};
+  gp.Y = Y;
+  gp.C0 = cp.C0;
+  gp.C1 = cp.C1;
+  for (int h = 0; h < 2; h++) {
+    gp.rows[h] = lay.rows(h);
+    gp.rows_pad[h] = cp.rows_pad[h];
+  }
+  gp.col_stride = col_stride;
+  gp.n = n;
+  gp.walks = nw;
+  gp.out_walks = P.s2_walks;
+  gp.out = ctx->s2psi.as<float>();
+  CK(launch_s2_gemm(gp, stream));
+  if (P.counting) {
+    P.stats.launches += 2;
+    // the product basis once, every walk's planar state written
+    P.stats.aux_bytes += (double)Kb * K2 * N * 4.0 + (double)nw * N * 8.0;
+  }
+  return MQW_OK;
+}
+
 
 // Diagonals (per group of equal n; instances are sorted by n) and the degree
 // pass.
@@ -910,6 +1032,20 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
       const BasisLayout& B = Bs[buf];
       const float* basis = bk.Kb ? B.real1() : nullptr;
       const float* lastb = bk.Kl ? B.real2() : nullptr;
+      // The stage-2 product basis of this instance (then no stage-1
+      // recombination: the walks start from their stage-2 outputs).
+      const ResidentWalk& wb = P.walks[ws[bk.b0]];
+      const int nwb = (int)(bk.b1 - bk.b0);
+      const bool s2 = !overlap && bk.Kb > 0 && P.s2_k2.count(n) && wb.stages >= 3 &&
+                      nwb <= P.s2_walks && (P.s2_mode > 0 || 2 * bk.Kb <= nwb);
+      if (s2) {
+        int K2b = 0;
+        for (size_t k = bk.b0; k < bk.b1; k++)
+          K2b = std::max(K2b, P.degree[P.walks[ws[k]].stage_desc_off + 1]);
+        mqw_status s = issue_stage2(P, ws, bk.b0, bk.b1, basis, bk.Kb, K2b, geo,
+                                    std::min(gs.lanes, bk.Kb), gs.bgroup, stream);
+        if (s != MQW_OK) return s;
+      }
       // Groups are dealt round-robin to the lanes, which run concurrently.
       // With shared bases a group is a basis group of up to gs.bgroup walks
       // (pass groups of G inside it), and the block's walks are split into
@@ -936,14 +1072,22 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
         const size_t size = shared ? (size_t)(nw / ngroups + (i < nw % ngroups ? 1 : 0))
                                    : std::min((size_t)G, bk.b1 - a);
         std::vector<int> grp(ws.begin() + a, ws.begin() + a + size);
+        const float* ext_re = nullptr;
+        const float* ext_im = nullptr;
+        if (s2) {
+          const size_t N = (size_t)1 << n;
+          ext_re = ctx->s2psi.as<float>() + (a - bk.b0) * N;
+          ext_im = ctx->s2psi.as<float>() + (P.s2_walks + (a - bk.b0)) * N;
+        }
         a += size;
         if (grp.empty()) continue;
         const int lane = i % lanes;
         double* proj = ctx->proj_part.as<double>() +
                        (size_t)lane * gs.bgroup *
                            (((size_t)1 << n) >> std::min(geo.L, kRecombineLog)) * 2;
-        mqw_status s = run_grid_group(P, grp, geo, lane, G, gs.bgroup, basis, bk.Kb, lastb,
-                                      bk.Kl, proj, lane == 0 ? stream : ctx->lane_stream[lane]);
+        mqw_status s = run_grid_group(P, grp, geo, lane, G, gs.bgroup, s2 ? nullptr : basis,
+                                      bk.Kb, lastb, bk.Kl, proj, ext_re, ext_im,
+                                      lane == 0 ? stream : ctx->lane_stream[lane]);
         if (s != MQW_OK) return s;
       }
       CK(ctx->join(stream, lanes));
@@ -1100,12 +1244,20 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     // basis alone is ~K_1 GB.
     const size_t budget = std::min(free_b / 2, (size_t)64 << 30);
     std::map<int, std::pair<int, int>> kb;
+    std::map<int, int> s2k;             // largest stage-2 degree (m >= 3 walks)
+    std::map<int, int> inst_walks;      // walks of one instance (largest)
+    std::map<std::pair<int, int>, int> per_inst;
     for (size_t w = 0; w < P.walks.size(); w++) {
       const ResidentWalk& wk = P.walks[w];
       if (!P.walk_is_grid[w] || wk.record_each || wk.stages < 2) continue;
       auto& k = kb[wk.n];
       k.first = std::max(k.first, P.degree[wk.stage_desc_off]);
       k.second = std::max(k.second, P.degree[wk.stage_desc_off + wk.stages - 1]);
+      if (wk.stages >= 3) {
+        s2k[wk.n] = std::max(s2k[wk.n], P.degree[wk.stage_desc_off + 1]);
+        const int c = ++per_inst[std::make_pair(wk.n, wk.inst)];
+        inst_walks[wk.n] = std::max(inst_walks[wk.n], c);
+      }
     }
     size_t basis_b = 0, proj_b = 0;
     int rmax = 0;
@@ -1129,12 +1281,48 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       rmax = std::max(rmax, std::max(k1 + (k1 & 1), k2 + (k2 & 1)));
     }
     P.basis_buffers = 1;
+    // Building the next instance's bases ahead measured within 1% (the walks
+    // already keep the GPU busy), so it is opt-in: MQW_BASIS_AHEAD=1.
+    static const bool ahead_env =
+        getenv("MQW_BASIS_AHEAD") && atoi(getenv("MQW_BASIS_AHEAD")) != 0;
+    const bool ahead = ahead_env && basis_b && 2 * basis_b <= budget;
+    // Stage-2 product basis (walks of m >= 3 with the stage-1 basis): worth
+    // it when its chains (one per stage-1 basis vector) are fewer than half
+    // of the instance's walks (MQW_STAGE2_BASIS=0 turns it off, =1 uses it
+    // whenever it fits); not with the build-ahead (its chains use the lanes'
+    // walk slots).
+    P.s2_k2.clear();
+    P.s2_walks = 0;
+    size_t s2y_b = 0, s2psi_n = 0, s2c_b = 0;
+    {
+      const char* env = getenv("MQW_STAGE2_BASIS");
+      const int mode = env ? atoi(env) : -1;
+      P.s2_mode = mode;
+      for (auto& e : s2k) {
+        const int n = e.first, K2 = e.second;
+        if (mode == 0 || ahead || !P.basis_kb1.count(n) || P.basis_kb1.at(n) == 0) continue;
+        const int k1 = P.basis_kb1.at(n), wpi = inst_walks[n];
+        if (mode < 0 && 2 * k1 > wpi) continue;
+        const size_t N = (size_t)1 << n;
+        const size_t yb = std::max(s2y_b, (size_t)k1 * K2 * N * 4);
+        const size_t pb = 2 * (size_t)std::max(P.s2_walks, wpi) * std::max(s2psi_n, N) * 4;
+        if (basis_b + yb + pb > budget) continue;
+        P.s2_k2[n] = K2;
+        P.s2_walks = std::max(P.s2_walks, wpi);
+        s2y_b = yb;
+        s2psi_n = std::max(s2psi_n, N);
+        s2c_b = std::max(s2c_b, ((size_t)k1 * K2 + 16) * (size_t)((wpi + 127) / 128 * 128) * 4);
+        rmax = std::max(rmax, K2 + (K2 & 1));
+      }
+    }
+    if (!P.s2_k2.empty()) {
+      CK(ctx->grow(ctx->s2y, s2y_b));
+      CK(ctx->grow(ctx->s2psi, 2 * (size_t)P.s2_walks * s2psi_n * 4));
+      CK(ctx->grow(ctx->s2c, s2c_b));
+    }
     if (basis_b) {
       CK(ctx->grow(ctx->basis, basis_b));
-      // Building the next instance's bases ahead measured within 1% (the
-      // walks already keep the GPU busy), so it is opt-in: MQW_BASIS_AHEAD=1.
-      static const bool ahead = getenv("MQW_BASIS_AHEAD") && atoi(getenv("MQW_BASIS_AHEAD")) != 0;
-      if (ahead && 2 * basis_b <= budget) {  // a second buffer to build ahead into
+      if (ahead) {  // a second buffer to build ahead into
         CK(ctx->grow(ctx->basis2, basis_b));
         CK(ctx->ensure_basis_stream());
         P.basis_buffers = 2;

@@ -225,6 +225,74 @@ cudaError_t launch_unit_eloc(void* psi, int n, const DiagOut* diag, cudaStream_t
 cudaError_t launch_combine(int precision, const CombineParams& p,
                            cudaStream_t stream);
 
+// Stage-2 product basis (FP32; mqw_stage2.cu). The vectors
+// Y_jk = U_k(H~_2) w_j (j < Kb stage-1 basis vectors, k < K2) are stored in
+// two parity classes, (j + k) even first, then odd; within a class in
+// row-major (j, k) order. S2Layout maps between (j, k) and the row q of its
+// class.
+struct S2Layout {
+  int Kb, K2;
+  // First k of class h for stage-1 index j (k = h - j mod 2).
+  __host__ __device__ int k0(int h, int j) const { return (h ^ j) & 1; }
+  // Number of k < K2 with k = first (mod 2).
+  __host__ __device__ int cnt(int first) const { return first == 0 ? (K2 + 1) / 2 : K2 / 2; }
+  __host__ __device__ int rows(int h) const {
+    return ((Kb + 1) / 2) * cnt(k0(h, 0)) + (Kb / 2) * cnt(k0(h, 1));
+  }
+  __host__ __device__ int index(int j, int k) const {
+    const int h = (j + k) & 1;
+    return ((j + 1) / 2) * cnt(k0(h, 0)) + (j / 2) * cnt(k0(h, 1)) + (k - k0(h, j)) / 2;
+  }
+  __host__ __device__ void pair(int h, int q, int* j, int* k) const {
+    const int ce = cnt(k0(h, 0));  // a pair of j (even, odd) spans ce + co = K2 rows
+    const int jp = q / K2, rem = q - jp * K2;
+    if (rem < ce) {
+      *j = 2 * jp;
+      *k = k0(h, *j) + 2 * rem;
+    } else {
+      *j = 2 * jp + 1;
+      *k = k0(h, *j) + 2 * (rem - ce);
+    }
+  }
+};
+// Coefficient matrices of one instance's walks: walk `col` (< walks) has its
+// stage-s job at job0 + col * m + s.
+struct S2CoefParams {
+  const StageDesc* stages;
+  const float* coef;
+  int job0, m, walks;
+  int col_stride;      // columns per row (a multiple of 128)
+  S2Layout lay;
+  int rows_pad[2];     // rows of C0 / C1 (zero-padded to multiples of 8)
+  float* C0;           // class 0 (real part): [rows_pad[0]][col_stride]
+  float* C1;           // class 1 (imaginary part)
+};
+struct S2GemmParams {
+  const float* Y;      // class-0 rows, then class-1 rows, 2^n floats each
+  const float* C0;
+  const float* C1;
+  int rows[2], rows_pad[2];
+  int col_stride;
+  int n, walks;
+  int out_walks;       // walk capacity of `out`
+  float* out;          // planar: Re of walk w at out + w 2^n, Im at
+                       // out + (out_walks + w) 2^n
+};
+struct UnpackWalk {
+  const float* re;
+  const float* im;
+  void* out;           // interleaved complex state
+  double* norm_part;   // per-block |psi|^2 partials
+};
+struct UnpackParams {
+  int n, L, count;
+  UnpackWalk walk[kMaxGroup];
+};
+cudaError_t launch_real_to_complex(void* dst, const float* src, int n, cudaStream_t stream);
+cudaError_t launch_s2_coef(const S2CoefParams& p, cudaStream_t stream);
+cudaError_t launch_s2_gemm(const S2GemmParams& p, cudaStream_t stream);
+cudaError_t launch_unpack(const UnpackParams& p, cudaStream_t stream);
+
 // Finalisation after a stage: kappa[g] = 1/sqrt(sum of partials); when
 // record != 0 also p_out[g] = |out[e_loc]|^2 * kappa^2.
 struct FinalTraj {

@@ -437,6 +437,34 @@ def test_basis_groups_give_identical_results(ctx, orc, mqw, monkeypatch, n, m, s
     assert np.all(grouped > 0.0) and np.all(grouped <= 1.0)
 
 
+@pytest.mark.parametrize("n,m,samples", [(16, 3, 24), (20, 4, 12), (18, 5, 16)])
+def test_stage2_basis_matches_per_walk(ctx, orc, mqw, monkeypatch, n, m, samples):
+    """Stage 2 from the product basis Y_jk = U_k(H~_2) w_j and one GEMM over
+    the instance's walks (MQW_STAGE2_BASIS=1, read at every plan) against
+    every walk running its own stage-1 recombination and stage-2 recurrence
+    (=0): per-sample P within FP32 rounding, the mean within 1e-5 of FP64, and
+    a captured graph replays it unchanged."""
+    raw = orc.sk_instances(n, 1, 4400 + n)
+
+    def run(mode, graph):
+        monkeypatch.setenv("MQW_STAGE2_BASIS", mode)
+        plan = mqw.Plan(ctx, n, m, raw, samples=samples, graph=graph)
+        plan.execute()
+        first = plan.results(per_sample=True)["p_sample"]
+        plan.execute()
+        again = plan.results(per_sample=True)["p_sample"]
+        plan.close()
+        return first, again
+
+    on, on_replay = run("1", 1)
+    off, _ = run("0", 0)
+    assert np.array_equal(on, on_replay)
+    np.testing.assert_allclose(on, off, rtol=5e-6, atol=1e-9)
+    assert np.all(on > 0.0) and np.all(on <= 1.0)
+    r64 = ctx.run_problems(n, m, raw, samples=samples, precision="fp64", graph=0)
+    assert abs(float(np.mean(on)) - r64["p"][0]) <= 1e-5
+
+
 def test_tier_peaks(ctx):
     """The bandwidth probes: shared memory above L2 above HBM, HBM within
     reach of the B200's nominal 7.7 TB/s."""
