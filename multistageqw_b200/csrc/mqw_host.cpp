@@ -861,7 +861,8 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
     if (s != MQW_OK) return s;
   }
   CK(ctx->join(stream, lanes));
-  const int col_stride = ((nw + 127) / 128) * 128;
+  const int bn = s2_tile_cols(nw);
+  const int col_stride = (nw + bn - 1) / bn * bn;
   S2CoefParams cp{};
   cp.stages = P.d_stages.as<StageDesc>();
   cp.coef = P.d_coef.as<float>();

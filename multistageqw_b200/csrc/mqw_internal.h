@@ -261,7 +261,7 @@ struct S2CoefParams {
   const StageDesc* stages;
   const float* coef;
   int job0, m, walks;
-  int col_stride;      // columns per row (a multiple of 128)
+  int col_stride;      // columns per row (a multiple of s2_tile_cols(walks))
   S2Layout lay;
   int rows_pad[2];     // rows of C0 / C1 (zero-padded to multiples of 8)
   float* C0;           // class 0 (real part): [rows_pad[0]][col_stride]
@@ -290,6 +290,8 @@ struct UnpackParams {
 };
 cudaError_t launch_real_to_complex(void* dst, const float* src, int n, cudaStream_t stream);
 cudaError_t launch_s2_coef(const S2CoefParams& p, cudaStream_t stream);
+// Columns of one GEMM tile for `walks` walks (C's row stride is a multiple).
+int s2_tile_cols(int walks);
 cudaError_t launch_s2_gemm(const S2GemmParams& p, cudaStream_t stream);
 cudaError_t launch_unpack(const UnpackParams& p, cudaStream_t stream);
 

@@ -63,12 +63,14 @@ __global__ void s2_coef_kernel(S2CoefParams p) {
 }
 
 // out_h (rows: amplitudes, columns: walks) = Y_h (amplitudes x K_h) C_h
-// (K_h x walks), FP32. A block computes a 128 x 128 tile over k in steps of
-// 8 with double-buffered shared-memory tiles; a thread holds an 8 x 8
-// sub-tile (rows tm*4 + {0..3} and 64 + tm*4 + {0..3}, likewise columns), so
-// its shared-memory reads are float4 and its stores are float4 runs of four
-// amplitudes of one walk.
-constexpr int kBM = 128, kBN = 128, kBK = 8;
+// (K_h x walks), FP32. A block of 16 TN threads computes a 128 x 8 TN tile
+// over k in steps of 8 with double-buffered shared-memory tiles; a thread
+// holds an 8 x 8 sub-tile (rows tm*4 + {0..3} and 64 + tm*4 + {0..3},
+// columns tn*4 + {0..3} and 4 TN + tn*4 + {0..3}), so its shared-memory
+// reads are float4 and its stores float4 runs of four amplitudes of one
+// walk. TN is chosen from the walk count so that few columns are padding
+// (100 walks: TN = 13, 104 columns).
+constexpr int kBM = 128, kBK = 8;
 __device__ __forceinline__ void fma_row(float (&r)[8], float a, const float4& b0,
                                         const float4& b1) {
   r[0] = fmaf(a, b0.x, r[0]);
@@ -80,50 +82,68 @@ __device__ __forceinline__ void fma_row(float (&r)[8], float a, const float4& b0
   r[6] = fmaf(a, b1.z, r[6]);
   r[7] = fmaf(a, b1.w, r[7]);
 }
-__global__ void __launch_bounds__(256, 2) s2_gemm_kernel(S2GemmParams p) {
+template <int TN>
+__global__ void __launch_bounds__(16 * TN, 2) s2_gemm_kernel(S2GemmParams p) {
+  constexpr int T = 16 * TN, BN = 8 * TN;
+  constexpr int kALoads = (kBM * kBK / 4 + T - 1) / T;  // float4 of the A tile per thread
   __shared__ __align__(16) float As[2][kBK][kBM];
-  __shared__ __align__(16) float Bs[2][kBK][kBN];
+  __shared__ __align__(16) float Bs[2][kBK][BN];
   const int h = blockIdx.z;
   const size_t N = (size_t)1 << p.n;
   const size_t m0 = (size_t)blockIdx.x * kBM;
-  const int c0 = blockIdx.y * kBN;
+  const int c0 = blockIdx.y * BN;
   const int K = h ? p.rows[1] : p.rows[0];
   const int Kp = h ? p.rows_pad[1] : p.rows_pad[0];
   const float* __restrict__ Y = p.Y + (h ? (size_t)p.rows[0] * N : 0);
   const float* __restrict__ C = h ? p.C1 : p.C0;
   float* __restrict__ out = p.out + (size_t)h * p.out_walks * N;
   const int t = threadIdx.x;
-  const int lr = t >> 5, lc = (t & 31) * 4;  // this thread's load: row lr, 4 columns at lc
+  const int br = t / (2 * TN), bc = (t % (2 * TN)) * 4;  // this thread's B-tile float4
   const int tm = t & 15, tn = t >> 4;
-  auto load_a = [&](int q) -> float4 {
-    return q < K ? __ldcs(reinterpret_cast<const float4*>(Y + (size_t)q * N + m0 + lc))
+  float4 a[kALoads];
+  auto load_a = [&](int k0) {
+#pragma unroll
+    for (int u = 0; u < kALoads; u++) {
+      const int e = t + u * T;
+      const int q = k0 + (e >> 5);
+      a[u] = e < kBM * kBK / 4 && q < K
+                 ? __ldcs(reinterpret_cast<const float4*>(Y + (size_t)q * N + m0 + (e & 31) * 4))
                  : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
   };
-  auto load_b = [&](int q) -> float4 {
-    return *reinterpret_cast<const float4*>(C + (size_t)q * p.col_stride + c0 + lc);
+  auto store_a = [&](int buf) {
+#pragma unroll
+    for (int u = 0; u < kALoads; u++) {
+      const int e = t + u * T;
+      if (e < kBM * kBK / 4) *reinterpret_cast<float4*>(&As[buf][e >> 5][(e & 31) * 4]) = a[u];
+    }
+  };
+  auto load_b = [&](int k0) -> float4 {
+    return *reinterpret_cast<const float4*>(C + (size_t)(k0 + br) * p.col_stride + c0 + bc);
   };
   float acc[8][8];
 #pragma unroll
   for (int i = 0; i < 8; i++)
 #pragma unroll
     for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
-  float4 a = load_a(lr), b = load_b(lr);
-  *reinterpret_cast<float4*>(&As[0][lr][lc]) = a;
-  *reinterpret_cast<float4*>(&Bs[0][lr][lc]) = b;
+  load_a(0);
+  float4 b = load_b(0);
+  store_a(0);
+  *reinterpret_cast<float4*>(&Bs[0][br][bc]) = b;
   __syncthreads();
   for (int k0 = 0; k0 < Kp; k0 += kBK) {
     const int cur = (k0 / kBK) & 1;
     const bool more = k0 + kBK < Kp;
     if (more) {
-      a = load_a(k0 + kBK + lr);
-      b = load_b(k0 + kBK + lr);
+      load_a(k0 + kBK);
+      b = load_b(k0 + kBK);
     }
 #pragma unroll
     for (int kk = 0; kk < kBK; kk++) {
       const float4 a0 = *reinterpret_cast<const float4*>(&As[cur][kk][tm * 4]);
       const float4 a1 = *reinterpret_cast<const float4*>(&As[cur][kk][64 + tm * 4]);
       const float4 b0 = *reinterpret_cast<const float4*>(&Bs[cur][kk][tn * 4]);
-      const float4 b1 = *reinterpret_cast<const float4*>(&Bs[cur][kk][64 + tn * 4]);
+      const float4 b1 = *reinterpret_cast<const float4*>(&Bs[cur][kk][4 * TN + tn * 4]);
       fma_row(acc[0], a0.x, b0, b1);
       fma_row(acc[1], a0.y, b0, b1);
       fma_row(acc[2], a0.z, b0, b1);
@@ -134,14 +154,14 @@ __global__ void __launch_bounds__(256, 2) s2_gemm_kernel(S2GemmParams p) {
       fma_row(acc[7], a1.w, b0, b1);
     }
     if (more) {
-      *reinterpret_cast<float4*>(&As[cur ^ 1][lr][lc]) = a;
-      *reinterpret_cast<float4*>(&Bs[cur ^ 1][lr][lc]) = b;
+      store_a(cur ^ 1);
+      *reinterpret_cast<float4*>(&Bs[cur ^ 1][br][bc]) = b;
     }
     __syncthreads();
   }
 #pragma unroll
   for (int j = 0; j < 8; j++) {
-    const int col = c0 + (j < 4 ? tn * 4 + j : 64 + tn * 4 + (j - 4));
+    const int col = c0 + (j < 4 ? tn * 4 + j : 4 * TN + tn * 4 + (j - 4));
     if (col >= p.walks) continue;
     float* o = out + (size_t)col * N + m0 + tm * 4;
     *reinterpret_cast<float4*>(o) = make_float4(acc[0][j], acc[1][j], acc[2][j], acc[3][j]);
@@ -197,9 +217,13 @@ cudaError_t launch_real_to_complex(void* dst, const float* src, int n, cudaStrea
   return cudaGetLastError();
 }
 
+int s2_tile_cols(int walks) {
+  return walks <= 32 ? 32 : walks <= 64 ? 64 : walks <= 96 ? 96 : walks <= 104 ? 104 : 128;
+}
+
 cudaError_t launch_s2_coef(const S2CoefParams& p, cudaStream_t stream) {
   if (!p.stages || !p.coef || !p.C0 || !p.C1 || p.walks < 1 || p.col_stride < p.walks ||
-      p.col_stride % kBN != 0 || p.m < 3 || p.lay.Kb < 1 || p.lay.K2 < 1 ||
+      p.col_stride % 8 != 0 || p.m < 3 || p.lay.Kb < 1 || p.lay.K2 < 1 ||
       p.rows_pad[0] < p.lay.rows(0) || p.rows_pad[1] < p.lay.rows(1))
     return cudaErrorInvalidValue;
   const size_t total = ((size_t)p.rows_pad[0] + p.rows_pad[1]) * p.col_stride;
@@ -210,15 +234,22 @@ cudaError_t launch_s2_coef(const S2CoefParams& p, cudaStream_t stream) {
 }
 
 cudaError_t launch_s2_gemm(const S2GemmParams& p, cudaStream_t stream) {
+  const int bn = s2_tile_cols(p.walks);
   if (p.n < 7 || p.n > kMaxN || !p.Y || !p.C0 || !p.C1 || !p.out || p.walks < 1 ||
-      p.out_walks < p.walks || p.col_stride % kBN != 0 || p.col_stride < p.walks ||
+      p.out_walks < p.walks || p.col_stride % bn != 0 || p.col_stride < p.walks ||
       p.rows[0] < 1 || p.rows[1] < 0)
     return cudaErrorInvalidValue;
   for (int h = 0; h < 2; h++)
     if (p.rows_pad[h] < p.rows[h] || p.rows_pad[h] % kBK != 0) return cudaErrorInvalidValue;
   const size_t N = (size_t)1 << p.n;
-  const dim3 grid((unsigned)(N / kBM), (unsigned)(p.col_stride / kBN), p.rows[1] > 0 ? 2 : 1);
-  s2_gemm_kernel<<<grid, 256, 0, stream>>>(p);
+  const dim3 grid((unsigned)(N / kBM), (unsigned)(p.col_stride / bn), p.rows[1] > 0 ? 2 : 1);
+  switch (bn) {
+    case 32: s2_gemm_kernel<4><<<grid, 64, 0, stream>>>(p); break;
+    case 64: s2_gemm_kernel<8><<<grid, 128, 0, stream>>>(p); break;
+    case 96: s2_gemm_kernel<12><<<grid, 192, 0, stream>>>(p); break;
+    case 104: s2_gemm_kernel<13><<<grid, 208, 0, stream>>>(p); break;
+    default: s2_gemm_kernel<16><<<grid, 256, 0, stream>>>(p); break;
+  }
   return cudaGetLastError();
 }
 
