@@ -495,6 +495,21 @@ def main():
         "bytes_per_launch": BYTES_PER_TERM_AMP[a.precision] * per_launch_amps,
         "avg_launch_us": 1000.0 * kms / max(1, term_launches),
     }
+    # FP32 arithmetic of the passes: (2n + 8) FLOP per term·amp (the
+    # diagonal product, the n partner sums and the Clenshaw update, complex),
+    # against the SIMT FP32 peak of this GPU at its maximum SM clock (the
+    # path is memory-bound; this is the compute roof it stays far below).
+    # Single-n workloads only; the stage-2 GEMM's FLOPs are not included.
+    if len(set(ns)) == 1 and kms > 0:
+        n0 = int(ns[0])
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = float((clk or {}).get("sm_max_mhz") or 1965.0)
+        peak_tf = sms * 128 * 2 * mhz * 1e6 / 1e12
+        ex_tf = (2 * n0 + 8) * pass_amps / (kms / 1000.0) / 1e12
+        roofline["fp32_flops"] = {
+            "per_term_amp": 2 * n0 + 8, "executed_tflops": ex_tf,
+            "reference_equivalent_tflops": (2 * n0 + 8) * term_amps / (kms / 1000.0) / 1e12,
+            "peak_tflops": peak_tf, "frac": ex_tf / peak_tf}
     if tiers:
         # The tier that holds the walks' working set (n <= 20: L2-resident):
         # the same achieved bytes against the measured L2 copy bandwidth.
@@ -522,7 +537,10 @@ def main():
                        "precision": a.precision, "group": a.group or "autotuned",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": "flushed between timed steps (256 MB write)",
-                       "graph": "CUDA graph replay of the whole device pipeline"})
+                       "graph": "CUDA graph replay of the whole device pipeline",
+                       "stage2_product_basis": {"0": "off", "1": "forced"}.get(
+                           os.environ.get("MQW_STAGE2_BASIS", ""),
+                           "auto (when 2 x stage-1 basis size <= walks per instance)")})
         line = {
             "metric": METRIC, "value": value, "unit": "instances/s", "n_gpus": world,
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps,
