@@ -793,8 +793,11 @@ mqw_status issue_chain(mqw_plan& P, const ResidentWalk& w0, int stage, int K,
     W.scale = P.onenorm[job];
     W.r = R - j;
     W.K = R + 1;
-    W.psi_uniform = S.uniform ? 1 : 0;
-    W.psi0 = (float)(1.0 / std::sqrt((double)N));
+    // Only the first pass (b_R = v) uses the start vector: every later
+    // coefficient is 0, so those passes take psi as a uniform zero state and
+    // do not read it.
+    W.psi_uniform = (S.uniform || j > 0) ? 1 : 0;
+    W.psi0 = S.uniform ? (float)(1.0 / std::sqrt((double)N)) : 0.0f;
     W.real_out = out_of(j);
     CK(launch_pass(P.precision, pp, stream));
     if (P.counting) {
