@@ -23,6 +23,7 @@
 #include <cstdlib>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <numeric>
@@ -832,10 +833,14 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
 // the Kb stage-1 basis vectors w_j (in `basis`) and k < K2, one chain of K2
 // passes per w_j, dealt round-robin to `lanes` lanes (each on its own walk
 // slots of the shared state), then the coefficient matrices and the GEMM
-// that leave every walk's stage-2 output, planar, in ctx->s2psi.
+// that leave every walk's stage-2 output, planar, in ctx->s2psi. `extra`
+// (if set) is issued beside the chains on one more lane (the last lane when
+// all four are in use): the instance's last-stage basis build.
 mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size_t b1,
                         const float* basis, int Kb, int K2, const PassGeomHost& geo,
-                        int lanes, int gmax, cudaStream_t stream) {
+                        int lanes, int gmax,
+                        const std::function<mqw_status(cudaStream_t)>& extra,
+                        cudaStream_t stream) {
   mqw_ctx* ctx = P.ctx;
   const ResidentWalk& w0 = P.walks[ws[b0]];
   const int n = w0.n;
@@ -844,7 +849,13 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
   const S2Layout lay{Kb, K2};
   float* Y = ctx->s2y.as<float>();
   const int slots = walk_slots(geo);
-  CK(ctx->fork(stream, lanes));
+  const int all = extra ? std::min(lanes + 1, kMaxLanes) : lanes;
+  CK(ctx->fork(stream, all));
+  if (extra) {
+    const int xl = all - 1;
+    mqw_status s = extra(xl == 0 ? stream : ctx->lane_stream[xl]);
+    if (s != MQW_OK) return s;
+  }
   for (int j = 0; j < Kb; j++) {
     const int lane = j % lanes;
     cudaStream_t st = lane == 0 ? stream : ctx->lane_stream[lane];
@@ -863,7 +874,7 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
     mqw_status s = issue_chain(P, w0, 1, K2, S, geo, out_of, st);
     if (s != MQW_OK) return s;
   }
-  CK(ctx->join(stream, lanes));
+  CK(ctx->join(stream, all));
   const int bn = s2_tile_cols(nw);
   const int col_stride = (nw + bn - 1) / bn * bn;
   S2CoefParams cp{};
@@ -1018,7 +1029,17 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
       const Block& bk = blocks[bi];
       const int buf = overlap ? (int)(bi & 1) : 0;
       const bool has = bk.Kb || bk.Kl;
-      if (has) {
+      // The stage-2 product basis of this instance (then no stage-1
+      // recombination: the walks start from their stage-2 outputs). Its
+      // last-stage basis is built beside the stage-2 chains.
+      const ResidentWalk& wb = P.walks[ws[bk.b0]];
+      const int nwb = (int)(bk.b1 - bk.b0);
+      const bool s2 = !overlap && bk.Kb > 0 && P.s2_k2.count(n) && wb.stages >= 3 &&
+                      nwb <= P.s2_walks && (P.s2_mode > 0 || 2 * bk.Kb <= nwb);
+      if (s2) {
+        mqw_status s = issue_basis(P, wb, 0, bk.Kb, Bs[0], geo, Bs[0].real1(), stream);
+        if (s != MQW_OK) return s;
+      } else if (has) {
         if (overlap) {
           if (!built_next) {
             CK(cudaStreamWaitEvent(bst, ctx->basis_free[buf], 0));
@@ -1036,18 +1057,17 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
       const BasisLayout& B = Bs[buf];
       const float* basis = bk.Kb ? B.real1() : nullptr;
       const float* lastb = bk.Kl ? B.real2() : nullptr;
-      // The stage-2 product basis of this instance (then no stage-1
-      // recombination: the walks start from their stage-2 outputs).
-      const ResidentWalk& wb = P.walks[ws[bk.b0]];
-      const int nwb = (int)(bk.b1 - bk.b0);
-      const bool s2 = !overlap && bk.Kb > 0 && P.s2_k2.count(n) && wb.stages >= 3 &&
-                      nwb <= P.s2_walks && (P.s2_mode > 0 || 2 * bk.Kb <= nwb);
       if (s2) {
         int K2b = 0;
         for (size_t k = bk.b0; k < bk.b1; k++)
           K2b = std::max(K2b, P.degree[P.walks[ws[k]].stage_desc_off + 1]);
+        std::function<mqw_status(cudaStream_t)> last_build;
+        if (bk.Kl)
+          last_build = [&](cudaStream_t st) {
+            return issue_basis(P, wb, wb.stages - 1, bk.Kl, B, geo, B.real2(), st);
+          };
         mqw_status s = issue_stage2(P, ws, bk.b0, bk.b1, basis, bk.Kb, K2b, geo,
-                                    std::min(gs.lanes, bk.Kb), gs.bgroup, stream);
+                                    std::min(gs.lanes, bk.Kb), gs.bgroup, last_build, stream);
         if (s != MQW_OK) return s;
       }
       // Groups are dealt round-robin to the lanes, which run concurrently.
@@ -1320,6 +1340,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       }
     }
     if (!P.s2_k2.empty()) {
+      CK(ctx->ensure_lanes(kMaxLanes));  // the last-stage basis beside the chains
       CK(ctx->grow(ctx->s2y, s2y_b));
       CK(ctx->grow(ctx->s2psi, 2 * (size_t)P.s2_walks * s2psi_n * 4));
       CK(ctx->grow(ctx->s2c, s2c_b));
