@@ -12,7 +12,11 @@
 //   4. propagation: walks with n <= resident_max_n run in one launch of the
 //                   resident kernel (a CTA per walk); larger n run on the
 //                   grid path, one launch per Clenshaw term over groups of up
-//                   to 8 walks of the same n;
+//                   to 8 walks of the same n, instance by instance with the
+//                   instance's shared bases: the stage-1 basis (recombined
+//                   per basis group), the stage-2 product basis (chains and
+//                   one GEMM for all walks, when it pays) and the last-stage
+//                   basis (projected per basis group);
 //   5. means      : mean ground-state probability per instance.
 #include <cuda_runtime.h>
 
