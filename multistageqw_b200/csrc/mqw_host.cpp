@@ -110,6 +110,7 @@ struct mqw_ctx {
   // Stage-2 product basis: the Y vectors, every walk's planar stage-2
   // output, and the coefficient matrices (one instance at a time).
   DevMem s2y, s2psi, s2c;
+  DevMem s2chain;  // chain slots of the build-ahead (4 complex vectors)
   // Bumped whenever a shared scratch buffer is reallocated: a plan's captured
   // graph holds the old addresses and is re-captured when this changes.
   unsigned long long scratch_gen = 1;
@@ -244,6 +245,9 @@ struct mqw_plan {
   std::map<int, int> s2_k2;
   int s2_walks = 0;
   int s2_mode = -1;  // MQW_STAGE2_BASIS: -1 auto, 0 off, 1 whenever it fits
+  // Per-buffer sizes (floats) of ctx->s2y / s2psi / s2c: one buffer set, two
+  // with the build-ahead.
+  size_t s2y_floats = 0, s2psi_floats = 0, s2c_floats = 0;
   DevMem d_unit;
   int unit_len = 0;
   // CUDA graph of the whole device pipeline, replayed by later executes.
@@ -840,20 +844,24 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
 // that leave every walk's stage-2 output, planar, in ctx->s2psi. `extra`
 // (if set) is issued beside the chains on one more lane (the last lane when
 // all four are in use): the instance's last-stage basis build.
+// `buf` selects one of the plan's stage-2 buffer sets (two with the
+// build-ahead, which calls this on its side stream with solo set: all chains
+// on `stream`, on the context's own chain slots instead of the lanes').
 mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size_t b1,
                         const float* basis, int Kb, int K2, const PassGeomHost& geo,
                         int lanes, int gmax,
                         const std::function<mqw_status(cudaStream_t)>& extra,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, int buf = 0, bool solo = false) {
   mqw_ctx* ctx = P.ctx;
   const ResidentWalk& w0 = P.walks[ws[b0]];
   const int n = w0.n;
   const size_t N = (size_t)1 << n;
   const int nw = (int)(b1 - b0);
   const S2Layout lay{Kb, K2};
-  float* Y = ctx->s2y.as<float>();
+  float* Y = ctx->s2y.as<float>() + (size_t)buf * P.s2y_floats;
   const int slots = walk_slots(geo);
-  const int all = extra ? std::min(lanes + 1, kMaxLanes) : lanes;
+  if (solo) lanes = 1;
+  const int all = extra && !solo ? std::min(lanes + 1, kMaxLanes) : lanes;
   CK(ctx->fork(stream, all));
   if (extra) {
     const int xl = all - 1;
@@ -863,7 +871,8 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
   for (int j = 0; j < Kb; j++) {
     const int lane = j % lanes;
     cudaStream_t st = lane == 0 ? stream : ctx->lane_stream[lane];
-    char* base = ctx->state.as<char>() + (size_t)lane * gmax * slots * N * 8;
+    char* base = solo ? ctx->s2chain.as<char>()
+                      : ctx->state.as<char>() + (size_t)lane * gmax * slots * N * 8;
     auto slot = [&](int k) -> void* { return base + (size_t)k * N * 8; };
     const ChainSlots S{slot(0), {slot(1), slot(2)}, slot(slots - 1), false};
     CK(launch_real_to_complex(slot(slots - 1), basis + (size_t)j * N, n, st));
@@ -891,7 +900,7 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
   cp.lay = lay;
   cp.rows_pad[0] = (lay.rows(0) + 7) / 8 * 8;
   cp.rows_pad[1] = (lay.rows(1) + 7) / 8 * 8;
-  cp.C0 = ctx->s2c.as<float>();
+  cp.C0 = ctx->s2c.as<float>() + (size_t)buf * P.s2c_floats;
   cp.C1 = cp.C0 + (size_t)cp.rows_pad[0] * col_stride;
   CK(launch_s2_coef(cp, stream));
   S2GemmParams gp{};
@@ -906,7 +915,7 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
   gp.n = n;
   gp.walks = nw;
   gp.out_walks = P.s2_walks;
-  gp.out = ctx->s2psi.as<float>();
+  gp.out = ctx->s2psi.as<float>() + (size_t)buf * P.s2psi_floats;
   CK(launch_s2_gemm(gp, stream));
   if (P.counting) {
     P.stats.launches += 2;
@@ -1008,6 +1017,22 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
     const int nbuf = P.basis_buffers;
     const BasisLayout Bs[2] = {{ctx->basis.as<char>(), (size_t)1 << n, kb1, kb2},
                                {ctx->basis2.as<char>(), (size_t)1 << n, kb1, kb2}};
+    // The stage-2 product basis of a block (instance), and its largest
+    // stage-2 degree.
+    auto use_s2 = [&](const Block& bk) {
+      const ResidentWalk& wb = P.walks[ws[bk.b0]];
+      const int nwb = (int)(bk.b1 - bk.b0);
+      return bk.Kb > 0 && P.s2_k2.count(n) && wb.stages >= 3 && nwb <= P.s2_walks &&
+             (P.s2_mode > 0 || 2 * bk.Kb <= nwb);
+    };
+    auto s2_degree = [&](const Block& bk) {
+      int K2b = 0;
+      for (size_t k = bk.b0; k < bk.b1; k++)
+        K2b = std::max(K2b, P.degree[P.walks[ws[k]].stage_desc_off + 1]);
+      return K2b;
+    };
+    // A block's bases on one stream (the build-ahead's side stream): stage 1,
+    // last stage, then the stage-2 product basis and its GEMM.
     auto build = [&](const Block& bk, int buf, cudaStream_t st) -> mqw_status {
       const ResidentWalk& w0 = P.walks[ws[bk.b0]];
       const BasisLayout& B = Bs[buf];
@@ -1017,6 +1042,11 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
       }
       if (bk.Kl) {
         mqw_status s = issue_basis(P, w0, w0.stages - 1, bk.Kl, B, geo, B.real2(), st);
+        if (s != MQW_OK) return s;
+      }
+      if (use_s2(bk)) {
+        mqw_status s = issue_stage2(P, ws, bk.b0, bk.b1, B.real1(), bk.Kb, s2_degree(bk), geo,
+                                    1, gs.bgroup, {}, st, buf, true);
         if (s != MQW_OK) return s;
       }
       return MQW_OK;
@@ -1034,13 +1064,12 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
       const int buf = overlap ? (int)(bi & 1) : 0;
       const bool has = bk.Kb || bk.Kl;
       // The stage-2 product basis of this instance (then no stage-1
-      // recombination: the walks start from their stage-2 outputs). Its
-      // last-stage basis is built beside the stage-2 chains.
+      // recombination: the walks start from their stage-2 outputs). In order
+      // (no build-ahead) its chains run on the lanes with the last-stage
+      // basis beside them.
       const ResidentWalk& wb = P.walks[ws[bk.b0]];
-      const int nwb = (int)(bk.b1 - bk.b0);
-      const bool s2 = !overlap && bk.Kb > 0 && P.s2_k2.count(n) && wb.stages >= 3 &&
-                      nwb <= P.s2_walks && (P.s2_mode > 0 || 2 * bk.Kb <= nwb);
-      if (s2) {
+      const bool s2 = use_s2(bk);
+      if (s2 && !overlap) {
         mqw_status s = issue_basis(P, wb, 0, bk.Kb, Bs[0], geo, Bs[0].real1(), stream);
         if (s != MQW_OK) return s;
       } else if (has) {
@@ -1061,10 +1090,8 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
       const BasisLayout& B = Bs[buf];
       const float* basis = bk.Kb ? B.real1() : nullptr;
       const float* lastb = bk.Kl ? B.real2() : nullptr;
-      if (s2) {
-        int K2b = 0;
-        for (size_t k = bk.b0; k < bk.b1; k++)
-          K2b = std::max(K2b, P.degree[P.walks[ws[k]].stage_desc_off + 1]);
+      if (s2 && !overlap) {
+        const int K2b = s2_degree(bk);
         std::function<mqw_status(cudaStream_t)> last_build;
         if (bk.Kl)
           last_build = [&](cudaStream_t st) {
@@ -1104,8 +1131,9 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
         const float* ext_im = nullptr;
         if (s2) {
           const size_t N = (size_t)1 << n;
-          ext_re = ctx->s2psi.as<float>() + (a - bk.b0) * N;
-          ext_im = ctx->s2psi.as<float>() + (P.s2_walks + (a - bk.b0)) * N;
+          const float* set = ctx->s2psi.as<float>() + (size_t)buf * P.s2psi_floats;
+          ext_re = set + (a - bk.b0) * N;
+          ext_im = set + (P.s2_walks + (a - bk.b0)) * N;
         }
         a += size;
         if (grp.empty()) continue;
@@ -1317,8 +1345,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     // Stage-2 product basis (walks of m >= 3 with the stage-1 basis): worth
     // it when its chains (one per stage-1 basis vector) are fewer than half
     // of the instance's walks (MQW_STAGE2_BASIS=0 turns it off, =1 uses it
-    // whenever it fits); not with the build-ahead (its chains use the lanes'
-    // walk slots).
+    // whenever it fits). With the build-ahead its buffers are doubled.
     P.s2_k2.clear();
     P.s2_walks = 0;
     size_t s2y_b = 0, s2psi_n = 0, s2c_b = 0;
@@ -1328,13 +1355,13 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       P.s2_mode = mode;
       for (auto& e : s2k) {
         const int n = e.first, K2 = e.second;
-        if (mode == 0 || ahead || !P.basis_kb1.count(n) || P.basis_kb1.at(n) == 0) continue;
+        if (mode == 0 || !P.basis_kb1.count(n) || P.basis_kb1.at(n) == 0) continue;
         const int k1 = P.basis_kb1.at(n), wpi = inst_walks[n];
         if (mode < 0 && 2 * k1 > wpi) continue;
         const size_t N = (size_t)1 << n;
         const size_t yb = std::max(s2y_b, (size_t)k1 * K2 * N * 4);
         const size_t pb = 2 * (size_t)std::max(P.s2_walks, wpi) * std::max(s2psi_n, N) * 4;
-        if (basis_b + yb + pb > budget) continue;
+        if ((ahead ? 2 : 1) * (basis_b + yb + pb) > budget) continue;
         P.s2_k2[n] = K2;
         P.s2_walks = std::max(P.s2_walks, wpi);
         s2y_b = yb;
@@ -1344,10 +1371,15 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       }
     }
     if (!P.s2_k2.empty()) {
+      const size_t nb = ahead ? 2 : 1;
       CK(ctx->ensure_lanes(kMaxLanes));  // the last-stage basis beside the chains
-      CK(ctx->grow(ctx->s2y, s2y_b));
-      CK(ctx->grow(ctx->s2psi, 2 * (size_t)P.s2_walks * s2psi_n * 4));
-      CK(ctx->grow(ctx->s2c, s2c_b));
+      P.s2y_floats = s2y_b / 4;
+      P.s2psi_floats = 2 * (size_t)P.s2_walks * s2psi_n;
+      P.s2c_floats = s2c_b / 4;
+      CK(ctx->grow(ctx->s2y, nb * s2y_b));
+      CK(ctx->grow(ctx->s2psi, nb * P.s2psi_floats * 4));
+      CK(ctx->grow(ctx->s2c, nb * s2c_b));
+      if (ahead) CK(ctx->grow(ctx->s2chain, 4 * s2psi_n * 8));
     }
     if (basis_b) {
       CK(ctx->grow(ctx->basis, basis_b));

@@ -468,6 +468,35 @@ def test_stage2_basis_matches_per_walk(ctx, orc, mqw, monkeypatch, n, m, samples
     assert abs(float(np.mean(on)) - r64["p"][0]) <= 1e-5
 
 
+def test_stage2_basis_built_ahead_gives_identical_results(ctx, orc, mqw, monkeypatch):
+    """The stage-2 product basis built on the build-ahead's side stream (its
+    own chain slots, double-buffered Y and outputs; MQW_BASIS_AHEAD=1 is read
+    once per process, so a child process) against the in-order build, over
+    three instances: per-sample P equal to FP64 rounding."""
+    import json
+    import sys
+    raws = np.concatenate([orc.sk_instances(16, 1, 4500 + i) for i in range(3)])
+    monkeypatch.setenv("MQW_STAGE2_BASIS", "1")
+    plan = mqw.Plan(ctx, 16, 3, raws, samples=12, group=1, lanes=2)
+    plan.execute()
+    plan.execute()
+    ref = plan.results(per_sample=True)["p_sample"]
+    plan.close()
+    code = (
+        "import json, numpy as np, multistageqw_b200 as M\n"
+        "raws = np.concatenate([M.sk_instances(16, 1, 4500 + i) for i in range(3)])\n"
+        "c = M.Context(0)\n"
+        "pl = M.Plan(c, 16, 3, raws, samples=12, group=1, lanes=2)\n"
+        "pl.execute(); pl.execute()\n"
+        "print(json.dumps(pl.results(per_sample=True)['p_sample'].tolist()))\n")
+    env = dict(os.environ, MQW_BASIS_AHEAD="1", MQW_STAGE2_BASIS="1")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env,
+                       cwd=os.path.dirname(os.path.dirname(os.path.abspath(__file__))), timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = np.array(json.loads(r.stdout.strip().splitlines()[-1]))
+    np.testing.assert_allclose(got, ref, rtol=1e-12, atol=0.0)
+
+
 def test_tier_peaks(ctx):
     """The bandwidth probes: shared memory above L2 above HBM, HBM within
     reach of the B200's nominal 7.7 TB/s."""
