@@ -96,6 +96,11 @@ struct mqw_ctx {
   // instance's walks run; events order the two buffers' uses.
   cudaStream_t basis_stream = nullptr;
   cudaEvent_t basis_built[2] = {}, basis_free[2] = {};
+  // The basis stream's own lanes (1..): its stage-2 chains run on the basis
+  // stream and these, forked and joined like the walk lanes.
+  cudaStream_t bld_stream[kMaxLanes] = {};
+  cudaEvent_t bld_fork_ev = nullptr;
+  cudaEvent_t bld_join_ev[kMaxLanes] = {};
   cudaError_t ensure_basis_stream() {
     cudaError_t e = cudaSuccess;
     if (!basis_stream) e = cudaStreamCreateWithFlags(&basis_stream, cudaStreamNonBlocking);
@@ -103,6 +108,13 @@ struct mqw_ctx {
       if (!basis_built[k]) e = cudaEventCreateWithFlags(&basis_built[k], cudaEventDisableTiming);
       if (e == cudaSuccess && !basis_free[k])
         e = cudaEventCreateWithFlags(&basis_free[k], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess && !bld_fork_ev)
+      e = cudaEventCreateWithFlags(&bld_fork_ev, cudaEventDisableTiming);
+    for (int k = 1; k < kMaxLanes && e == cudaSuccess; k++) {
+      if (!bld_stream[k]) e = cudaStreamCreateWithFlags(&bld_stream[k], cudaStreamNonBlocking);
+      if (e == cudaSuccess && !bld_join_ev[k])
+        e = cudaEventCreateWithFlags(&bld_join_ev[k], cudaEventDisableTiming);
     }
     return e;
   }
@@ -845,13 +857,14 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
 // (if set) is issued beside the chains on one more lane (the last lane when
 // all four are in use): the instance's last-stage basis build.
 // `buf` selects one of the plan's stage-2 buffer sets (two with the
-// build-ahead, which calls this on its side stream with solo set: all chains
-// on `stream`, on the context's own chain slots instead of the lanes').
+// build-ahead, which calls this on the basis stream with `builder` set: the
+// chains then run on the basis stream's own lanes and on the context's chain
+// slots, one set per lane, instead of the walk lanes and their slots).
 mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size_t b1,
                         const float* basis, int Kb, int K2, const PassGeomHost& geo,
                         int lanes, int gmax,
                         const std::function<mqw_status(cudaStream_t)>& extra,
-                        cudaStream_t stream, int buf = 0, bool solo = false) {
+                        cudaStream_t stream, int buf = 0, bool builder = false) {
   mqw_ctx* ctx = P.ctx;
   const ResidentWalk& w0 = P.walks[ws[b0]];
   const int n = w0.n;
@@ -860,19 +873,24 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
   const S2Layout lay{Kb, K2};
   float* Y = ctx->s2y.as<float>() + (size_t)buf * P.s2y_floats;
   const int slots = walk_slots(geo);
-  if (solo) lanes = 1;
-  const int all = extra && !solo ? std::min(lanes + 1, kMaxLanes) : lanes;
-  CK(ctx->fork(stream, all));
+  const int all = extra ? std::min(lanes + 1, kMaxLanes) : lanes;
+  cudaStream_t* lane_st = builder ? ctx->bld_stream : ctx->lane_stream;
+  if (builder) {  // fork the basis stream's lanes
+    CK(cudaEventRecord(ctx->bld_fork_ev, stream));
+    for (int k = 1; k < all; k++) CK(cudaStreamWaitEvent(ctx->bld_stream[k], ctx->bld_fork_ev, 0));
+  } else {
+    CK(ctx->fork(stream, all));
+  }
   if (extra) {
     const int xl = all - 1;
-    mqw_status s = extra(xl == 0 ? stream : ctx->lane_stream[xl]);
+    mqw_status s = extra(xl == 0 ? stream : lane_st[xl]);
     if (s != MQW_OK) return s;
   }
   for (int j = 0; j < Kb; j++) {
     const int lane = j % lanes;
-    cudaStream_t st = lane == 0 ? stream : ctx->lane_stream[lane];
-    char* base = solo ? ctx->s2chain.as<char>()
-                      : ctx->state.as<char>() + (size_t)lane * gmax * slots * N * 8;
+    cudaStream_t st = lane == 0 ? stream : lane_st[lane];
+    char* base = builder ? ctx->s2chain.as<char>() + (size_t)lane * 4 * N * 8
+                         : ctx->state.as<char>() + (size_t)lane * gmax * slots * N * 8;
     auto slot = [&](int k) -> void* { return base + (size_t)k * N * 8; };
     const ChainSlots S{slot(0), {slot(1), slot(2)}, slot(slots - 1), false};
     CK(launch_real_to_complex(slot(slots - 1), basis + (size_t)j * N, n, st));
@@ -887,7 +905,14 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
     mqw_status s = issue_chain(P, w0, 1, K2, S, geo, out_of, st);
     if (s != MQW_OK) return s;
   }
-  CK(ctx->join(stream, all));
+  if (builder) {
+    for (int k = 1; k < all; k++) {
+      CK(cudaEventRecord(ctx->bld_join_ev[k], ctx->bld_stream[k]));
+      CK(cudaStreamWaitEvent(stream, ctx->bld_join_ev[k], 0));
+    }
+  } else {
+    CK(ctx->join(stream, all));
+  }
   const int bn = s2_tile_cols(nw);
   const int col_stride = (nw + bn - 1) / bn * bn;
   S2CoefParams cp{};
@@ -1040,13 +1065,17 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
         mqw_status s = issue_basis(P, w0, 0, bk.Kb, B, geo, B.real1(), st);
         if (s != MQW_OK) return s;
       }
+      if (use_s2(bk)) {  // the last-stage basis beside the chains
+        std::function<mqw_status(cudaStream_t)> last_build;
+        if (bk.Kl)
+          last_build = [&](cudaStream_t ls) {
+            return issue_basis(P, w0, w0.stages - 1, bk.Kl, B, geo, B.real2(), ls);
+          };
+        return issue_stage2(P, ws, bk.b0, bk.b1, B.real1(), bk.Kb, s2_degree(bk), geo,
+                            std::min(gs.lanes, bk.Kb), gs.bgroup, last_build, st, buf, true);
+      }
       if (bk.Kl) {
         mqw_status s = issue_basis(P, w0, w0.stages - 1, bk.Kl, B, geo, B.real2(), st);
-        if (s != MQW_OK) return s;
-      }
-      if (use_s2(bk)) {
-        mqw_status s = issue_stage2(P, ws, bk.b0, bk.b1, B.real1(), bk.Kb, s2_degree(bk), geo,
-                                    1, gs.bgroup, {}, st, buf, true);
         if (s != MQW_OK) return s;
       }
       return MQW_OK;
@@ -1379,7 +1408,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       CK(ctx->grow(ctx->s2y, nb * s2y_b));
       CK(ctx->grow(ctx->s2psi, nb * P.s2psi_floats * 4));
       CK(ctx->grow(ctx->s2c, nb * s2c_b));
-      if (ahead) CK(ctx->grow(ctx->s2chain, 4 * s2psi_n * 8));
+      if (ahead) CK(ctx->grow(ctx->s2chain, (size_t)kMaxLanes * 4 * s2psi_n * 8));
     }
     if (basis_b) {
       CK(ctx->grow(ctx->basis, basis_b));
@@ -1511,6 +1540,11 @@ void mqw_destroy(mqw_ctx* ctx) {
   }
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   if (ctx->basis_stream) cudaStreamDestroy(ctx->basis_stream);
+  for (int k = 1; k < kMaxLanes; k++) {
+    if (ctx->bld_stream[k]) cudaStreamDestroy(ctx->bld_stream[k]);
+    if (ctx->bld_join_ev[k]) cudaEventDestroy(ctx->bld_join_ev[k]);
+  }
+  if (ctx->bld_fork_ev) cudaEventDestroy(ctx->bld_fork_ev);
   for (int k = 0; k < 2; k++) {
     if (ctx->basis_built[k]) cudaEventDestroy(ctx->basis_built[k]);
     if (ctx->basis_free[k]) cudaEventDestroy(ctx->basis_free[k]);
