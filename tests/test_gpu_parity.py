@@ -468,6 +468,33 @@ def test_stage2_basis_matches_per_walk(ctx, orc, mqw, monkeypatch, n, m, samples
     assert abs(float(np.mean(on)) - r64["p"][0]) <= 1e-5
 
 
+def test_stage2_basis_in_a_mixed_m_plan(ctx, orc, mqw, monkeypatch):
+    """One plan of instances of the same n with m = 3, 2, 4, 5 (the product
+    basis used instance by instance where m >= 3, its buffers reused) and the
+    learned-schedule hook (per-stage gamma/t multipliers) against the same
+    plan with every walk running its own stage 2: per-sample P within FP32
+    rounding."""
+    ms = [3, 2, 4, 5]
+    raws = np.concatenate([orc.sk_instances(16, 1, 4600 + i) for i in range(len(ms))])
+    rng = np.random.default_rng(11)
+    scale = rng.uniform(0.8, 1.25, (sum(ms), 2)).astype(np.float32).ravel()
+
+    def run(mode):
+        monkeypatch.setenv("MQW_STAGE2_BASIS", mode)
+        plan = mqw.Plan(ctx, [16] * len(ms), ms, raws, samples=20, stage_scale=scale)
+        plan.execute()
+        plan.execute()
+        ps = plan.results(per_sample=True)["p_sample"]
+        st = plan.stats()
+        plan.close()
+        return ps, st
+
+    on, st_on = run("1")
+    off, st_off = run("0")
+    np.testing.assert_allclose(on, off, rtol=5e-6, atol=1e-9)
+    assert st_on["pass_amps"] != st_off["pass_amps"]
+
+
 def test_stage2_basis_built_ahead_gives_identical_results(ctx, orc, mqw, monkeypatch):
     """The stage-2 product basis built on the build-ahead's side stream (its
     own chain slots, double-buffered Y and outputs; MQW_BASIS_AHEAD=1 is read
