@@ -437,14 +437,16 @@ def test_basis_groups_give_identical_results(ctx, orc, mqw, monkeypatch, n, m, s
     assert np.all(grouped > 0.0) and np.all(grouped <= 1.0)
 
 
-@pytest.mark.parametrize("n,m,samples", [(16, 3, 24), (20, 4, 12), (18, 5, 16), (21, 3, 6)])
+@pytest.mark.parametrize("n,m,samples", [(16, 3, 24), (20, 4, 12), (18, 5, 16), (21, 3, 6),
+                                          (14, 3, 100)])
 def test_stage2_basis_matches_per_walk(ctx, orc, mqw, monkeypatch, n, m, samples):
     """Stage 2 from the product basis Y_jk = U_k(H~_2) w_j and one GEMM over
     the instance's walks (MQW_STAGE2_BASIS=1, read at every plan) against
     every walk running its own stage-1 recombination and stage-2 recurrence
     (=0): per-sample P within FP32 rounding, the mean within 1e-5 of FP64, and
     a captured graph replays it unchanged. n = 21 runs the chains with an
-    axis read from global memory (double-buffered b, four walk slots)."""
+    axis read from global memory (double-buffered b, four walk slots); 100
+    walks (the most an instance has) take the 128-column GEMM tile."""
     raw = orc.sk_instances(n, 1, 4400 + n)
 
     shape = {"tile_log": 12} if n > 20 else {}  # 2^12 tiles leave an axis to global memory
