@@ -83,12 +83,33 @@ def parse():
     return ap.parse_args()
 
 
+def find_key(d, key):
+    """The first value stored under `key` anywhere in a nested dict/list."""
+    if isinstance(d, dict):
+        if key in d:
+            return d[key]
+        d = list(d.values())
+    if isinstance(d, list):
+        for v in d:
+            r = find_key(v, key)
+            if r is not None:
+                return r
+    return None
+
+
 def peaks():
+    """HBM copy bandwidth for the roofline: the measured figure of this pool's
+    B200s (MEASURED_PEAKS.json, written beside this file by the pool), else
+    the pool's earlier measurement."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
-        with open(p) as f:
-            d = json.load(f)
-        return d, "measured"
+        try:
+            with open(p) as f:
+                v = find_key(json.load(f), "hbm_gbs")
+            if isinstance(v, (int, float)) and v > 0:
+                return {"hbm_gbs": float(v)}, "measured"
+        except (OSError, ValueError):
+            pass
     return PEAKS_FALLBACK, "fallback"
 
 
@@ -118,6 +139,12 @@ class ClockSampler:
         except subprocess.TimeoutExpired:
             self.proc.kill()
             out, _ = self.proc.communicate()
+        return self.summarize(out)
+
+    @staticmethod
+    def summarize(out: str):
+        """Median SM clock under load, the maximum, and every throttle reason
+        seen active, from nvidia-smi's CSV lines (FIELDS order, no units)."""
         rows = []
         for line in out.strip().splitlines():
             parts = [x.strip() for x in line.split(",")]

@@ -51,3 +51,37 @@ def test_single_rank_is_identity():
     assert bench.max_over_ranks(3.5, 1) == 3.5
     assert bench.replica_seed(20, 0) == 20
     assert np.isfinite(bench.replica_seed(20, 7))
+
+
+def test_clock_summary_flags_throttling():
+    """The clocks record of the bench line: median SM clock over the samples
+    under load, the maximum clock, and every throttle reason seen active."""
+    import bench
+    lines = "\n".join([
+        "1965, 1965, 700.1, 0x0, Not Active, Not Active, Not Active, Not Active",
+        "1950, 1965, 990.5, 0x4, Not Active, Not Active, Not Active, Active",
+        "1845, 1965, 1001.0, 0x4, Not Active, Not Active, Not Active, Active",
+        "345, 1965, 90.0, 0x0, Not Active, Not Active, Not Active, Not Active",  # idle
+        "garbage line",
+    ])
+    c = bench.ClockSampler.summarize(lines)
+    assert c["sm_mhz"] == 1950.0 and c["sm_max_mhz"] == 1965.0
+    assert c["reasons"] == ["sw_power_cap"] and c["samples"] == 4
+    hot = bench.ClockSampler.summarize(
+        "1500, 1965, 900, 0x40, Not Active, Active, Not Active, Not Active")
+    assert hot["reasons"] == ["hw_thermal_slowdown"]
+    assert bench.ClockSampler.summarize("") is None
+
+
+def test_peaks_reads_nested_measured_file(tmp_path, monkeypatch):
+    """The roofline denominator: `hbm_gbs` wherever the measured-peaks file
+    keeps it, else the fallback figure."""
+    import json
+
+    import bench
+    monkeypatch.setattr(bench, "ROOT", str(tmp_path))
+    assert bench.peaks() == (bench.PEAKS_FALLBACK, "fallback")
+    (tmp_path / "MEASURED_PEAKS.json").write_text(json.dumps({"b200": {"hbm_gbs": 6544.7}}))
+    assert bench.peaks() == ({"hbm_gbs": 6544.7}, "measured")
+    (tmp_path / "MEASURED_PEAKS.json").write_text("{not json")
+    assert bench.peaks()[1] == "fallback"
