@@ -497,6 +497,29 @@ def test_stage2_basis_in_a_mixed_m_plan(ctx, orc, mqw, monkeypatch):
     assert st_on["pass_amps"] != st_off["pass_amps"]
 
 
+def test_stage2_basis_on_near_degenerate_instances(ctx, mqw, monkeypatch):
+    """The stage-2 product basis where precision matters most: n = 20
+    instances whose two lowest energies lie within 2e-2 (screened on the GPU
+    from the precision study's seeded draws), per-sample P against FP64
+    within the 1e-5 target and the mean far inside it."""
+    from multistageqw_b200 import studies
+    kept, seen, _ = studies.screen(ctx, 20, 2, 2e-2, 1500)
+    assert len(kept) == 2, seen
+    monkeypatch.setenv("MQW_STAGE2_BASIS", "1")
+    for k in kept:
+        raw = k["raw"][None, :]
+        plan = mqw.Plan(ctx, 20, 4, raw, samples=24, graph=0)
+        plan.execute()
+        on = plan.results(per_sample=True)["p_sample"][0]
+        plan.close()
+        p64 = mqw.Plan(ctx, 20, 4, raw, samples=24, graph=0, precision="fp64")
+        p64.execute()
+        ref = p64.results(per_sample=True)["p_sample"][0]
+        p64.close()
+        assert np.max(np.abs(on - ref)) <= 1e-5, (k["gap"], np.max(np.abs(on - ref)))
+        assert abs(on.mean() - ref.mean()) <= 1e-6
+
+
 def test_stage2_basis_built_ahead_gives_identical_results(ctx, orc, mqw, monkeypatch):
     """The stage-2 product basis built on the build-ahead's side stream (its
     own chain slots, double-buffered Y and outputs; MQW_BASIS_AHEAD=1 is read
