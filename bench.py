@@ -23,7 +23,17 @@ precision (the n=24 near-degenerate FP32/FP64/CPU study; one JSON report).
 With --impl reference the line times the reference's own CPU hot loop
 (Clenshaw_step, compiled from the reference source into oracle/_ref) driven
 by the oracle's restatement of its problem loop, run-script style (one
-process per core), on a bounded sample of the same workload.
+process per core): every timed step is one whole instance of the workload
+(its 100 samples split into contiguous ranges over the processes); n = 28
+times terms of the reference's step and scales them (a whole instance takes
+hours per core); the mixed workload runs the first samples of every
+instance.
+
+roofline: the dominant kernel, pass_kernel, timed alone (CUDA events around
+a pass-only replay in the plan's tuned shape) against the tier that holds
+its working set — L2 (the library's own L2 copy probe) when the walks in
+flight fit, else HBM (MEASURED_PEAKS.json); frac = bytes_per_launch /
+avg_launch_us / peak.
 """
 from __future__ import annotations
 
@@ -78,7 +88,6 @@ def parse():
     ap.add_argument("--seed", type=int, default=20)
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 |dP| check")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
-    ap.add_argument("--cpu-samples", type=int, default=1, help="samples per CPU worker")
     ap.add_argument("--cpu-walks", type=int, default=4, help="precision: CPU-checked instances")
     return ap.parse_args()
 
@@ -175,38 +184,110 @@ def gpu_selector(torch, dev):
 
 # ---- CPU baselines (reference hot loop, one process per core) ------------------
 
-def _cpu_worker(args):
-    n, m, seed, samples = args
+def _cpu_range_worker(args):
+    """Samples [s0, s1) of one instance through the reference pipeline (the
+    reference's own Clenshaw_step when the partial build is present)."""
+    n, m, raw, s0, s1 = args
     sys.path.insert(0, ROOT)
     from oracle import oracle as O
-    raw = O.sk_instances(n, 1, seed)
     use_ref = O.ref_lib() is not None
     t0 = time.perf_counter()
-    O.run_problems(n, m, raw, 1, samples, "f32", use_ref_step=use_ref)
-    return time.perf_counter() - t0, use_ref
+    ps, _ = O.run_sample_range(n, m, raw, s0, s1, "f32", use_ref_step=use_ref)
+    return ps, time.perf_counter() - t0, use_ref
 
 
-def cpu_baseline(n, m, seed, samples_per_worker):
-    """Whole samples of the reference pipeline (n <= 22): every process runs
-    `samples_per_worker` samples of its own instance."""
-    cores = len(os.sched_getaffinity(0))
-    workers = max(1, min(cores, CPU_MEM_BUDGET // (44 << n)))
-    jobs = [(n, m, seed + i, samples_per_worker) for i in range(workers)]
-    t0 = time.perf_counter()
-    with mp.get_context("spawn").Pool(workers) as pool:
-        res = pool.map(_cpu_worker, jobs)
-    wall = time.perf_counter() - t0
-    busy = max(r[0] for r in res)
-    kind = "reference" if all(r[1] for r in res) else "port"
-    inst = workers * samples_per_worker / 100.0
+def sample_ranges(samples: int, workers: int):
+    """run.sh's split of a problem range over processes (run.sh:27-38),
+    applied to one instance's samples: contiguous ranges, the first
+    `samples % workers` one longer."""
+    base, extra = divmod(samples, workers)
+    out, s = [], 0
+    for t in range(workers):
+        c = base + (1 if t < extra else 0)
+        if c:
+            out.append((s, s + c))
+            s += c
+    return out
+
+
+class CpuInstances:
+    """Whole instances of the reference pipeline on the host cores: one
+    process per core (as many as CPU_MEM_BUDGET allows), each running a
+    contiguous range of the instance's samples — run.sh's process split
+    applied to the samples of one instance, so that one instance is one
+    step. The pool is started once."""
+
+    def __init__(self, n: int):
+        cores = len(os.sched_getaffinity(0))
+        self.workers = max(1, min(cores, CPU_MEM_BUDGET // (44 << n), 100))
+        self.pool = mp.get_context("spawn").Pool(self.workers)
+
+    def run(self, n: int, m: int, raw, samples: int = 100):
+        """(mean P over the samples, wall seconds, kind)."""
+        ranges = [(0, samples)] if m == 1 else sample_ranges(samples, self.workers)
+        jobs = [(n, m, raw, s0, s1) for s0, s1 in ranges]
+        t0 = time.perf_counter()
+        res = self.pool.map(_cpu_range_worker, jobs, chunksize=1)
+        wall = time.perf_counter() - t0
+        kind = "reference" if all(r[2] for r in res) else "port"
+        return sum(r[0] for r in res) / samples, wall, kind
+
+    def close(self):
+        self.pool.close()
+        self.pool.join()
+
+
+def _step_desc(kind: str) -> str:
+    return ("reference Clenshaw_step, MultiQW.cpp:88-173, AVX-512 build" if kind == "reference"
+            else "oracle restatement")
+
+
+def cpu_baseline(n, m, seed):
+    """One whole seeded n, m instance (all 100 samples) of the reference
+    pipeline, timed on the host cores (about 10 s at n = 20, m = 4 on 16
+    cores)."""
+    import multistageqw_b200 as M
+    cpu = CpuInstances(n)
+    try:
+        raw = M.sk_instances(n, 1, seed)[0]
+        cpu.run(n, m, raw, samples=cpu.workers)  # warm-up: one sample per process
+        _, wall, kind = cpu.run(n, m, raw)
+    finally:
+        cpu.close()
     return {
-        "value": inst / busy, "unit": "instances/s", "cores": workers, "kind": kind,
-        "sample": (f"{workers} processes x {samples_per_worker} of the 100 samples of one "
-                   f"n={n}, m={m} instance each (FP32; "
-                   + ("reference Clenshaw_step, MultiQW.cpp:88-173, AVX-512 build" if kind == "reference"
-                      else "oracle restatement") + "); instances/s = samples/100 / slowest worker"),
+        "value": 1.0 / wall, "unit": "instances/s", "cores": cpu.workers, "kind": kind,
+        "sample": (f"one whole n={n}, m={m} instance (100 samples x {m} stages; FP32, "
+                   f"{_step_desc(kind)}), its samples split into {cpu.workers} contiguous ranges, "
+                   "one process per core"),
         "wall_s": wall,
     }
+
+
+def cpu_baseline_mixed(ns, ms, raw, samples: int = 4):
+    """Bounded sample of a mixed batch: the first `samples` of the 100
+    samples of every instance, one (instance, samples) job per process slot,
+    one process per core; instances/s = instances x samples/100 / wall."""
+    import multistageqw_b200 as M
+    cores = len(os.sched_getaffinity(0))
+    workers = max(1, min(cores, CPU_MEM_BUDGET // (44 << max(ns))))
+    offs = np.cumsum([0] + [M.params_per_instance(n) for n in ns])
+    jobs = [(n, m, raw[offs[i]:offs[i + 1]], 0, samples if m > 1 else 100)
+            for i, (n, m) in enumerate(zip(ns, ms))]
+    # longest first, so that the pool ends together
+    jobs.sort(key=lambda j: -(j[4] * j[1] * (1 << j[0])))
+    with mp.get_context("spawn").Pool(workers) as pool:
+        pool.map(_cpu_range_worker, jobs[:workers], chunksize=1)  # warm-up
+        t0 = time.perf_counter()
+        res = pool.map(_cpu_range_worker, jobs, chunksize=1)
+        wall = time.perf_counter() - t0
+    kind = "reference" if all(r[2] for r in res) else "port"
+    units = sum((j[4] - j[3]) / 100.0 for j in jobs)
+    return {"value": units / wall, "unit": "instances/s", "cores": workers, "kind": kind,
+            "sample": (f"the first {samples} of the 100 samples of each of the {len(ns)} "
+                       f"instances (m = 1 instances whole; FP32, {_step_desc(kind)}), one "
+                       "(instance, samples) job per process, one process per core; "
+                       "instances/s = instances x samples/100 / wall"),
+            "wall_s": wall}
 
 
 def _cpu_term_worker(args):
@@ -329,26 +410,60 @@ def instance_units(a, count: int) -> float:
 
 
 def reference_arm(a):
+    """The reference's own CPU pipeline on the host cores, on this arm's
+    workload and metric. n <= 22: every timed step is one whole seeded
+    instance (100 samples, split over one process per core; warm-up steps run
+    one sample per process). n28: seconds per term of the reference's step,
+    scaled to the instance's term count (a whole instance is hours per
+    core)."""
     n, m = (28, 3) if a.workload == "n28" else (a.n, a.m)
     times, base = [], None
-    for step in range(a.warmup + a.steps):
-        if n > 22:
+    import multistageqw_b200 as M
+    if a.workload == "mixed":
+        from multistageqw_b200 import studies
+        ns, ms_, raw = studies.mixed_batch(a.batch, replica_seed(a.seed, 0))
+        for step in range(a.warmup + a.steps):
+            b = cpu_baseline_mixed(ns, ms_, raw)
+            if step >= a.warmup:
+                times.append(1.0 / b["value"])
+            base = b
+        config = {"workload": "sk_mixed_n12-20_m2-5", "n": "12..20 (even)", "m": "2..5"}
+    elif n > 22:
+        for step in range(a.warmup + a.steps):
             # ~1 s per term per core at n = 28: time terms, scale by the
             # instance's term count (3 stages x ~190 terms x 100 samples).
             b = cpu_baseline_per_term(n, 57000, reps=1)
-        else:
-            b = cpu_baseline(n, m, a.seed + 1000 * step, 1)
-        if step >= a.warmup:
-            times.append(b)
-        base = b
-    val = sum(t["value"] for t in times) / len(times)
+            if step >= a.warmup:
+                times.append(1.0 / b["value"])
+            base = b
+        config = {"workload": f"sk_n{n}_m{m}", "n": n, "m": m, "samples": 100}
+    else:
+        cpu = CpuInstances(n)
+        try:
+            for step in range(a.warmup + a.steps):
+                raw = M.sk_instances(n, 1, a.seed + 1000 * step)[0]
+                if step < a.warmup:
+                    cpu.run(n, m, raw, samples=cpu.workers)
+                    continue
+                _, wall, kind = cpu.run(n, m, raw)
+                times.append(wall)
+        finally:
+            cpu.close()
+        base = {"kind": kind, "cores": cpu.workers,
+                "sample": (f"every timed step one whole seeded n={n}, m={m} instance (100 samples "
+                           f"x {m} stages; FP32, {_step_desc(kind)}), its samples split into "
+                           f"{cpu.workers} contiguous ranges, one process per core; warm-up steps "
+                           "one sample per process")}
+        config = {"workload": f"sk_n{n}_m{m}", "n": n, "m": m, "samples": 100}
+    sec = sum(times)
+    val = len(times) / sec
     return {
         "metric": METRIC, "value": val, "unit": "instances/s", "n_gpus": a.gpus,
-        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 / val,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 * sec / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic seeded SK instances (J,h ~ N(0,1))",
         "impl": "reference",
-        "config": {"workload": f"sk_n{n}_m{m}", "n": n, "m": m, "samples": 100},
+        "config": config,
         "cpu_baseline": {k: base[k] for k in ("kind", "cores", "sample")} | {"value": val, "unit": "instances/s"},
         "e2e": {"value": val, "unit": "instances/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -486,72 +601,107 @@ def main():
     e2e_total = max_over_ranks(sum(e2e_ms), world, dist, dev)
     e2e_val = world * instance_units(a, count) * len(e2e_ms) / (e2e_total / 1000.0)
 
-    # |dP| of the timed FP32 results against the FP64 path (first instance).
+    # |dP| of every timed FP32 result against the FP64 path (same instances,
+    # same samples), and the state-vector error of one walk (instance 0,
+    # sample 0) after its last stage, FP32 against FP64.
     check = None
     res = plan.results()
     if not a.no_check and a.precision != "fp64":
-        n0, m0 = ns[0], ms[0]
-        per0 = n0 * (n0 + 1) // 2
-        r64 = M.Plan(ctx, [n0], [m0], raw[:per0], samples=a.samples, precision="fp64", graph=0)
-        r64.execute()
-        p64 = r64.results()["p"][0]
-        r64.close()
-        check = {"max_abs_dP_vs_fp64": float(abs(res["p"][0] - p64)),
-                 "instances_checked": 1, "p_fp32": float(res["p"][0]), "p_fp64": float(p64)}
+        r64p = M.Plan(ctx, ns, ms, raw, samples=a.samples, precision="fp64", graph=0)
+        r64p.execute()
+        r64 = r64p.results()
+        r64p.close()
+        dP = np.abs(res["p"] - r64["p"])
+        check = {"max_abs_dP_vs_fp64": float(dP.max()), "mean_abs_dP_vs_fp64": float(dP.mean()),
+                 "instances_checked": len(ns), "tolerance": 1e-5,
+                 "e_loc_equal": bool(np.array_equal(res["e_loc"], r64["e_loc"])),
+                 "p_fp32": [float(x) for x in res["p"][:8]],
+                 "p_fp64": [float(x) for x in r64["p"][:8]]}
+        if max(ns) <= 24:
+            from multistageqw_b200 import studies
+            per0 = M.params_per_instance(ns[0])
+            s32, _, eloc = studies.stage_states(ctx, ns[0], ms[0], raw[:per0], 0, "fp32")
+            s64, _, _ = studies.stage_states(ctx, ns[0], ms[0], raw[:per0], 0, "fp64")
+            check["state_rel_l2_vs_fp64"] = float(np.linalg.norm(s32[-1] - s64[-1]) /
+                                                  np.linalg.norm(s64[-1]))
+            check["state_rel_l2_per_stage"] = [float(np.linalg.norm(x - y) / np.linalg.norm(y))
+                                               for x, y in zip(s32, s64)]
+            check["state_walk"] = "instance 0, sample 0, stage by stage through mqw_clenshaw"
 
     pk, pk_kind = peaks()
     tiers = ctx.measure_peaks() if rank == 0 else None
     kms = sum(kern_ms)
-    # Algorithmic bytes the propagation phase moved — the Clenshaw passes
-    # actually executed (36 B per term·amp) plus the shared-basis kernels'
-    # reads and writes (the bases replace most first- and last-stage passes;
-    # term_amps counts the reference's work) — over its device time.
-    moved = BYTES_PER_TERM_AMP[a.precision] * pass_amps + aux_bytes
-    achieved = moved / (kms / 1000.0) / 1e9 if kms > 0 else None
-    peak = pk["hbm_gbs"]
-    per_launch_amps = pass_amps / max(1, term_launches)
+    # The dominant kernel, pass_kernel (one fused Clenshaw pass), timed alone:
+    # CUDA events on the launching stream around a pass-only replay in the
+    # plan's own autotuned shape (walks per launch, concurrent lanes) for the
+    # workload's largest n. Its algorithmic bytes per launch are 36 B per
+    # term·amp (FP32; 72 B in FP64) x 2^n x walks per launch.
+    n_dom = int(max(ns))
+    pt = ctx.pass_timing(n_dom, a.precision if a.precision != "fp32c" else "fp32", reps=64)
+    bytes_per_launch = BYTES_PER_TERM_AMP[a.precision] * float(1 << n_dom) * pt["walks_per_launch"]
+    achieved = bytes_per_launch / (pt["us_per_launch"] * 1e-6) / 1e9
+    # Bound tier: the memory tier that holds the concurrent walks' working
+    # set (3 state vectors of 8 B and the 4 B diagonal per amplitude, per
+    # walk in flight): L2 (126 MB; the library's own L2 copy probe is the
+    # denominator) when it fits in 96 MB, else HBM (MEASURED_PEAKS.json).
+    ws = (3 * (8 if a.precision != "fp64" else 16) + 4) * float(1 << n_dom) * \
+        pt["walks_per_launch"] * pt["lanes"]
+    l2_resident = ws <= 96e6 and tiers is not None
+    if l2_resident:
+        bound, peak, peak_src = "l2", tiers["l2_copy_gbs"], "l2_copy_gbs of the library's own probe"
+    else:
+        bound, peak, peak_src = "hbm", pk["hbm_gbs"], f"hbm_gbs of {pk_kind}"
     dram = DRAM_BYTES_PER_TERM_AMP.get(desc["workload"])
+    # Propagation phase as a whole (every pass plus the shared-basis kernels'
+    # reads and writes, over the plan's device time): context for the
+    # kernel figure above.
+    moved = BYTES_PER_TERM_AMP[a.precision] * pass_amps + aux_bytes
+    phase_gbs = moved / (kms / 1000.0) / 1e9 if kms > 0 else None
     roofline = {
-        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-        "frac": achieved / peak if achieved else None,
-        "traffic": dram * per_launch_amps if dram else None,
-        "peak_source": f"hbm_gbs of {pk_kind}",
-        "kernel": ("propagation phase: pass_kernel (the dominant kernel, fused Clenshaw pass; "
-                   "bytes_per_launch and traffic are its per-launch figures) plus the "
-                   "shared-basis kernels (their bytes are in achieved)"),
-        "bytes_per_launch": BYTES_PER_TERM_AMP[a.precision] * per_launch_amps,
-        "avg_launch_us": 1000.0 * kms / max(1, term_launches),
+        "bound": bound, "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": achieved / peak, "traffic": dram * float(1 << n_dom) * pt["walks_per_launch"] if dram else None,
+        "peak_source": peak_src,
+        "kernel": (f"pass_kernel at n={n_dom}: frac = bytes_per_launch / avg_launch_us / peak; "
+                   "avg_launch_us from CUDA events around a pass-only replay in the plan's tuned "
+                   f"shape ({pt['walks_per_launch']} walk(s) per launch, {pt['lanes']} lane(s) "
+                   "in flight, so it is the launch-to-launch time); traffic = cold-cache DRAM "
+                   "bytes per launch from ncu"),
+        "bytes_per_launch": bytes_per_launch,
+        "avg_launch_us": pt["us_per_launch"],
+        "walks_per_launch": pt["walks_per_launch"], "lanes": pt["lanes"],
+        "working_set_bytes": ws,
+        "phase": {"achieved_gbs": phase_gbs, "device_ms_per_step": kms / max(1, a.steps),
+                  "algorithmic_bytes_per_step": moved / max(1, a.steps),
+                  "note": "whole propagation phase: executed passes at 36 B per term·amp plus "
+                          "the shared-basis kernels' reads and writes, over the phase's device time"},
     }
-    # FP32 arithmetic of the passes: (2n + 8) FLOP per term·amp (the
-    # diagonal product, the n partner sums and the Clenshaw update, complex),
-    # against the SIMT FP32 peak of this GPU at its maximum SM clock (the
-    # path is memory-bound; this is the compute roof it stays far below).
-    # Single-n workloads only; the stage-2 GEMM's FLOPs are not included.
-    if len(set(ns)) == 1 and kms > 0:
-        n0 = int(ns[0])
+    # FP32 arithmetic of the pass kernel: (2n + 8) FLOP per term·amp (the
+    # diagonal product, the n partner sums and the Clenshaw update, complex)
+    # per launch over its launch-to-launch time, against the SIMT FP32 peak
+    # at the maximum SM clock (the kernel is memory-bound; this is the
+    # compute roof it stays far below).
+    if a.precision != "fp64":
         sms = torch.cuda.get_device_properties(dev).multi_processor_count
         mhz = float((clk or {}).get("sm_max_mhz") or 1965.0)
         peak_tf = sms * 128 * 2 * mhz * 1e6 / 1e12
-        ex_tf = (2 * n0 + 8) * pass_amps / (kms / 1000.0) / 1e12
-        roofline["fp32_flops"] = {
-            "per_term_amp": 2 * n0 + 8, "executed_tflops": ex_tf,
-            "reference_equivalent_tflops": (2 * n0 + 8) * term_amps / (kms / 1000.0) / 1e12,
-            "peak_tflops": peak_tf, "frac": ex_tf / peak_tf}
+        ex_tf = (2 * n_dom + 8) * float(1 << n_dom) * pt["walks_per_launch"] / \
+            (pt["us_per_launch"] * 1e-6) / 1e12
+        roofline["fp32_flops"] = {"per_term_amp": 2 * n_dom + 8, "achieved_tflops": ex_tf,
+                                  "peak_tflops": peak_tf, "frac": ex_tf / peak_tf}
     if tiers:
-        # The tier that holds the walks' working set (n <= 20: L2-resident):
-        # the same achieved bytes against the measured L2 copy bandwidth.
         roofline["tiers_gbs"] = {k: round(v, 1) for k, v in tiers.items()}
-        if achieved:
-            roofline["frac_of_l2_copy"] = achieved / tiers["l2_copy_gbs"]
+        roofline["frac_of_hbm"] = achieved / pk["hbm_gbs"]
 
     if rank == 0:
         cpu = None
-        if world == 1 and not a.no_cpu and a.workload != "mixed":
+        if world == 1 and not a.no_cpu:
             try:
                 if a.workload == "n28":
                     cpu = cpu_baseline_per_term(28, int(terms * 100.0 / a.samples))
+                elif a.workload == "mixed":
+                    cpu = cpu_baseline_mixed(ns, ms, raw)
                 else:
-                    cpu = cpu_baseline(a.n, a.m, 4242, a.cpu_samples)
+                    cpu = cpu_baseline(a.n, a.m, 4242)
             except Exception as ex:  # the baseline is reported, not required
                 cpu = {"value": None, "error": str(ex)}
         config = dict(desc)

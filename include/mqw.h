@@ -208,8 +208,8 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
 
 /* No counterpart in the reference (which has no library API). The same
  * propagation as mqw_clenshaw, for callers that cannot allocate device
- * memory — for example code running during CUDA graph capture, code that must
- * not synchronise the device, or hosts whose own allocator owns all device
+ * memory — code that must not synchronise the device (cudaMalloc and cudaFree
+ * can), or hosts whose own allocator or fixed memory budget owns all device
  * memory. All pointers are DEVICE pointers owned by the caller: d_coeffs[K],
  * d_hp[2^n], d_psi[2^n] and d_out[2^n] complex (float for MQW_FP32, double
  * for MQW_FP64); d_out must not alias d_psi and receives the result. Work is
@@ -218,9 +218,13 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
  * Working space is a fixed device array of about 1 MiB inside the library
  * (held by every GPU that loads it until exit); n > MQW_NOALLOC_MAX_N returns
  * MQW_ERR_UNSUPPORTED and 6 <= n is required. The first call on each device
- * looks up that array's device address and must precede any stream capture.
- * Calls that overlap on the GPU share the array and race: order them on one
- * stream. Calls no cudaMalloc, cudaFree or other allocating routine. */
+ * looks up that array's device address (and makes the kernels' shared-memory
+ * opt-in on that device); make it before any stream capture. The address is
+ * kept for the life of the process: after a cudaDeviceReset of a device this
+ * entry point must not be called on it again. Calls that overlap on the GPU
+ * share the array and race: order them on one stream. After any status other
+ * than MQW_OK the contents of d_out are undefined. Calls no cudaMalloc,
+ * cudaFree or other allocating routine. */
 mqw_status mqw_clenshaw_noalloc(int precision, int n, int K,
                                 const float* d_coeffs, const float* d_hp,
                                 float gamma, float scale, const void* d_psi,
@@ -286,6 +290,18 @@ typedef struct mqw_grid_shape {
 } mqw_grid_shape;
 mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,
                               mqw_grid_shape* out);
+
+/* Device time of the grid-path pass kernel alone, in the autotuned shape for
+ * (precision, n): `reps` passes (alternating tilings) over zero-filled walks,
+ * the shape's walks per launch on each of its concurrent lanes, bracketed by
+ * CUDA events on the context's stream. us_per_launch = elapsed / (reps x
+ * lanes) — with several lanes in flight this is the launch-to-launch time,
+ * not one launch's latency; us_per_walk_pass = us_per_launch / walks per
+ * launch. Any output pointer may be NULL. No counterpart in the reference
+ * (the measurement behind the roofline of Clenshaw_step, MultiQW.cpp:88). */
+mqw_status mqw_pass_timing(mqw_ctx* ctx, int precision, int n, int reps,
+                           double* us_per_launch, double* us_per_walk_pass,
+                           int* walks_per_launch, int* lanes);
 
 /* ---- learned stage schedule (no counterpart in the reference) ---------- */
 /* Building blocks of the MLP that proposes per-stage (gamma, t) multipliers

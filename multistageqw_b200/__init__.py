@@ -153,6 +153,7 @@ def _bind(L):
         "mqw_multiqw": (i, [_vp, i, i, ctypes.c_char_p, ll, ll, ctypes.c_char_p, i]),
         "mqw_clenshaw_noalloc": (i, [i, i, i, _vp, _vp, f, f, _vp, _vp, _vp]),
         "mqw_grid_shape_for": (i, [_vp, i, i, _P(GridShape)]),
+        "mqw_pass_timing": (i, [_vp, i, i, i, _P(d), _P(d), _P(i), _P(i)]),
         "mqw_diag_moments": (i, [_vp, i, _P(d), _P(d), _P(DiagInfo)]),
         "mqw_selftest_wait_timeout": (i, [_vp]),
         "mqw_measure_peaks": (i, [_vp, _P(TierPeaks)]),
@@ -371,6 +372,18 @@ class Context:
         _check(self.h, lib().mqw_grid_shape_for(self.h, prec, n, ctypes.byref(g)))
         return g.as_dict()
 
+    def pass_timing(self, n: int, precision="fp32", reps: int = 64) -> dict:
+        """Device time of the pass kernel alone in the autotuned shape for n
+        (mqw_pass_timing): microseconds per launch (launch-to-launch, with the
+        shape's lanes in flight) and per walk-pass."""
+        prec = FP32 if precision == "fp32" else FP64
+        ul, uw = ctypes.c_double(), ctypes.c_double()
+        g, ln = ctypes.c_int(), ctypes.c_int()
+        _check(self.h, lib().mqw_pass_timing(self.h, prec, n, reps, ctypes.byref(ul),
+                                             ctypes.byref(uw), ctypes.byref(g), ctypes.byref(ln)))
+        return {"us_per_launch": ul.value, "us_per_walk_pass": uw.value,
+                "walks_per_launch": g.value, "lanes": ln.value, "reps": reps}
+
     def multiqw(self, n: int, m: int, filename: str, start: int = 0, problems: int = 2000,
                 out_dir: str | None = None, print_: bool = True):
         _check(self.h, lib().mqw_multiqw(self.h, n, m, filename.encode(), start, problems,
@@ -384,11 +397,12 @@ def clenshaw_noalloc(precision: int, n: int, K: int, d_coeffs: int, d_hp: int, g
                      scale: float, d_psi: int, d_out: int, stream: int | None = None) -> None:
     """Propagation without any device allocation (device pointers in and out).
 
-    For callers that cannot allocate device memory (e.g. while a CUDA graph is
-    captured, or when their own allocator owns the device): the library keeps
-    its working space in a fixed ~1 MiB device array, so n is limited to
-    NOALLOC_MAX_N, and calls that overlap on the GPU race on that array.
-    The first call on a device must come before any stream capture."""
+    For callers that cannot allocate device memory (code that must not
+    synchronise the device, or whose own allocator or memory budget owns the
+    device): the library keeps its working space in a fixed ~1 MiB device
+    array, so n is limited to NOALLOC_MAX_N, and calls that overlap on the GPU
+    race on that array. The first call on a device must come before any
+    stream capture; after an error the output buffer is undefined."""
     st = lib().mqw_clenshaw_noalloc(precision, n, K, _vp(d_coeffs), _vp(d_hp), gamma, scale,
                                     _vp(d_psi), _vp(d_out), _vp(stream) if stream else None)
     if st != 0:

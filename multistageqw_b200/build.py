@@ -28,7 +28,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CXX = os.environ.get("CXX", "g++")
 
 CU_SOURCES = ["mqw_diag.cu", "mqw_coeffs.cu", "mqw_propagate.cu", "mqw_noalloc.cu",
-              "mqw_mlp.cu", "mqw_peaks.cu", "mqw_stage2.cu"]
+              "mqw_mlp.cu", "mqw_peaks.cu", "mqw_stage2.cu", "mqw_stage2_tc.cu"]
 CPP_SOURCES = ["mqw_host.cpp", "mqw_schedule.cpp"]
 HEADERS = ["mqw_internal.h", "mqw_cheb.h"]
 

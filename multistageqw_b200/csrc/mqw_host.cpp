@@ -304,7 +304,8 @@ mqw_status take_device_error(mqw_ctx* ctx) {
   if (v == 0) return MQW_OK;
   CK(cudaMemset(ctx->dev_err.p, 0, sizeof v));
   return fail(ctx, MQW_ERR_TIMEOUT,
-              "a grid-path pass gave up waiting for its tile's bulk copies (error word %#x)", v);
+              "a kernel's bounded wait expired (error word %#x: bit 0 a grid-path pass's bulk "
+              "copies, bit 1 the tensor-core GEMM's pipeline)", v);
 }
 
 int walk_slots(const PassGeomHost& geo) { return geo.nu > 0 ? 4 : 3; }
@@ -330,7 +331,7 @@ int default_group(int precision, const PassGeomHost& geo, int n) {
 // Returns microseconds per walk-pass.
 mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
                             int G, int lanes, int threads, int lane_smem, int tma,
-                            double* us_per_walk) {
+                            double* us_per_walk, int reps = 12) {
   const PassGeomHost geo = pass_geom(precision, n, lmax, threads, lane_smem, tma);
   const size_t N = (size_t)1 << n;
   const size_t amp = precision == 0 ? 8 : 16;
@@ -386,7 +387,6 @@ mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  const int reps = 12;
   CK(cudaEventRecord(e0, st));
   CK(ctx->fork(st, lanes));
   for (int r = reps; r >= 1; r--)
@@ -927,7 +927,6 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
   cp.rows_pad[1] = (lay.rows(1) + 7) / 8 * 8;
   cp.C0 = ctx->s2c.as<float>() + (size_t)buf * P.s2c_floats;
   cp.C1 = cp.C0 + (size_t)cp.rows_pad[0] * col_stride;
-  CK(launch_s2_coef(cp, stream));
   S2GemmParams gp{};
   gp.Y = Y;
   gp.C0 = cp.C0;
@@ -941,7 +940,16 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
   gp.walks = nw;
   gp.out_walks = P.s2_walks;
   gp.out = ctx->s2psi.as<float>() + (size_t)buf * P.s2psi_floats;
-  CK(launch_s2_gemm(gp, stream));
+  // The GEMM on the tensor cores (tcgen05, three-product TF32 split) unless
+  // MQW_S2_GEMM=simt selects the FP32 SIMT kernel.
+  const char* gemm_env = getenv("MQW_S2_GEMM");
+  const bool simt_env = gemm_env && std::string(gemm_env) == "simt";
+  if (!simt_env && s2_tc_np(nw) <= 128 && n >= 8 && lay.rows(1) >= 1) {
+    CK(launch_s2_gemm_tc(cp, cp.C0, gp, ctx->dev_err.as<unsigned>(), stream));
+  } else {
+    CK(launch_s2_coef(cp, stream));
+    CK(launch_s2_gemm(gp, stream));
+  }
   if (P.counting) {
     P.stats.launches += 2;
     // the product basis once, every walk's planar state written
@@ -1395,7 +1403,10 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
         P.s2_walks = std::max(P.s2_walks, wpi);
         s2y_b = yb;
         s2psi_n = std::max(s2psi_n, N);
+        // coefficient matrices: the SIMT GEMM's row-major pair, or the
+        // tensor-core GEMM's K-major hi/lo copies, whichever is larger
         s2c_b = std::max(s2c_b, ((size_t)k1 * K2 + 16) * (size_t)((wpi + 127) / 128 * 128) * 4);
+        s2c_b = std::max(s2c_b, s2_tc_coef_floats(wpi, S2Layout{k1, K2}) * 4);
         rmax = std::max(rmax, K2 + (K2 & 1));
       }
     }
@@ -1840,6 +1851,31 @@ mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,
   out->group = gs.group;
   out->lanes = gs.lanes;
   out->us_per_walk_pass = gs.us;
+  return MQW_OK;
+}
+
+mqw_status mqw_pass_timing(mqw_ctx* ctx, int precision, int n, int reps,
+                           double* us_per_launch, double* us_per_walk_pass,
+                           int* walks_per_launch, int* lanes) {
+  mqw_status st = check_ctx(ctx);
+  if (st != MQW_OK) return st;
+  if ((precision != MQW_FP32 && precision != MQW_FP64) || n < 6 || n > kMaxN || reps < 1 ||
+      reps > 100000)
+    return fail(ctx, MQW_ERR_INVALID, "mqw_pass_timing: bad arguments");
+  GridShape want, gs;
+  want.group = want.lanes = 0;
+  st = tune_grid(ctx, precision, n, want, &gs);
+  if (st != MQW_OK) return st;
+  double us = 0.0;
+  st = time_grid_config(ctx, precision, n, gs.lmax, gs.group, gs.lanes, gs.threads,
+                        gs.lane_smem > 0, gs.tma > 0, &us, reps);
+  if (st != MQW_OK) return st;
+  // time_grid_config returns the elapsed time per walk-pass: launches carry
+  // `group` walks and `lanes` launches are in flight at a time.
+  if (us_per_walk_pass) *us_per_walk_pass = us;
+  if (us_per_launch) *us_per_launch = us * gs.group;
+  if (walks_per_launch) *walks_per_launch = gs.group;
+  if (lanes) *lanes = gs.lanes;
   return MQW_OK;
 }
 

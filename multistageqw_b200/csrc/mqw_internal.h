@@ -293,6 +293,16 @@ cudaError_t launch_s2_coef(const S2CoefParams& p, cudaStream_t stream);
 // Columns of one GEMM tile for `walks` walks (C's row stride is a multiple).
 int s2_tile_cols(int walks);
 cudaError_t launch_s2_gemm(const S2GemmParams& p, cudaStream_t stream);
+// The same GEMM on the tensor cores (tcgen05 kind::tf32, three-product TF32
+// split, mqw_stage2_tc.cu): writes the K-major hi/lo coefficient copies into
+// Ct (s2_tc_coef_floats floats; cp gives the coefficients, its C0/C1 are not
+// used) and then the planar outputs g.out. Walks <= 128, n >= 8. err: the
+// device error word (bit 1 set when a bounded wait expired).
+int s2_tc_np(int walks);
+int s2_tc_kp(const S2Layout& lay);
+size_t s2_tc_coef_floats(int walks, const S2Layout& lay);
+cudaError_t launch_s2_gemm_tc(const S2CoefParams& cp, float* Ct, const S2GemmParams& g,
+                              unsigned* err, cudaStream_t stream);
 cudaError_t launch_unpack(const UnpackParams& p, cudaStream_t stream);
 
 // Finalisation after a stage: kappa[g] = 1/sqrt(sum of partials); when

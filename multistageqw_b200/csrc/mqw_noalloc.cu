@@ -1,14 +1,12 @@
 // mqw_clenshaw_noalloc: the grid-path Clenshaw propagation for callers that
 // cannot allocate device memory.
 //
-// Some callers cannot call cudaMalloc: code running while a CUDA graph is
-// being captured (an allocation would break or end the capture), code that
-// must not synchronise the device (cudaMalloc/cudaFree can), and hosts whose
-// own allocator owns all device memory (a framework memory pool, an
-// embedded/real-time process with a fixed memory budget). For them this entry
-// point takes only caller-owned device buffers and keeps its own working
-// space in a fixed file-scope device array, so it calls no allocating CUDA or
-// library routine.
+// Some callers cannot call cudaMalloc: code that must not synchronise the
+// device (cudaMalloc/cudaFree can), and hosts whose own allocator owns all
+// device memory (a framework memory pool, an embedded/real-time process with
+// a fixed memory budget). For them this entry point takes only caller-owned
+// device buffers and keeps its own working space in a fixed file-scope
+// device array, so it calls no allocating CUDA or library routine.
 //
 // The working space is the partial sum P (2^n amplitudes) and one norm
 // partial per tile. Its size is fixed at MQW_NOALLOC_MAX_N = 16: 2^16
@@ -24,7 +22,12 @@
 //
 // Set-up: the device address of the array is looked up once per device with
 // cudaGetSymbolAddress, with that device current, on the first call made on
-// that device. Make that first call before starting any stream capture.
+// that device. Make that first call before starting any stream capture. The
+// address is kept for the life of the process, so a device that has been
+// reset (cudaDeviceReset) must not be used with this entry point again.
+//
+// On any status other than MQW_OK, passes may already be queued: the
+// contents of the caller's output buffer are then undefined.
 #include <mutex>
 
 #include "../../include/mqw.h"

@@ -26,10 +26,40 @@
 //    its vectors once as coalesced tile rows (see the grid-path section).
 #include <stdlib.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "mqw_internal.h"
 
 namespace mqw {
 namespace {
+
+// Dynamic shared-memory opt-ins. cudaFuncSetAttribute applies to the current
+// device only, so the size a kernel has been opted in to is recorded per
+// (device, kernel); contexts on several devices and several host threads may
+// launch concurrently, hence the lock. The first launch of a kernel on a
+// device makes the call (before any stream capture that uses it).
+std::mutex g_optin_mu;
+std::map<std::pair<int, const void*>, size_t> g_optin;
+
+cudaError_t ensure_smem_optin(const void* fn, size_t bytes, bool nonportable_cluster) {
+  if (bytes <= 48 * 1024 && !nonportable_cluster) return cudaSuccess;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(g_optin_mu);
+  size_t& done = g_optin[std::make_pair(dev, fn)];
+  if (bytes <= done) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e != cudaSuccess) return e;
+  if (nonportable_cluster) {
+    e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    if (e != cudaSuccess) return e;
+  }
+  done = bytes;
+  return cudaSuccess;
+}
 
 template <typename R> struct Cplx;
 template <> struct Cplx<float> { using T = float2; };
@@ -903,26 +933,18 @@ cudaError_t launch_resident(int precision, const ResidentWalk* walks,
   ResidentArgs a{walks, stages, coef, hp, diag, p_sample};
   const int T = (1 << max_n) < 512 ? (1 << max_n) : 512;
   const int threads = T < 32 ? 32 : T;
-  // The shared-memory opt-in is set once per size (never while a stream is
-  // being captured after the first eager launch).
-  static size_t configured[2] = {0, 0};
+  // The shared-memory opt-in is made per device on the first launch of each
+  // size (never while a stream is being captured after the first eager
+  // launch).
   if (precision == 0) {
     const size_t sm = resident_smem<float>(max_n);
-    if (sm > configured[0]) {
-      cudaError_t e = cudaFuncSetAttribute(resident_kernel<float>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      if (e != cudaSuccess) return e;
-      configured[0] = sm;
-    }
+    cudaError_t e = ensure_smem_optin((const void*)resident_kernel<float>, sm, false);
+    if (e != cudaSuccess) return e;
     resident_kernel<float><<<count, threads, sm, stream>>>(a);
   } else {
     const size_t sm = resident_smem<double>(max_n);
-    if (sm > configured[1]) {
-      cudaError_t e = cudaFuncSetAttribute(resident_kernel<double>,
-                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-      if (e != cudaSuccess) return e;
-      configured[1] = sm;
-    }
+    cudaError_t e = ensure_smem_optin((const void*)resident_kernel<double>, sm, false);
+    if (e != cudaSuccess) return e;
     resident_kernel<double><<<count, threads, sm, stream>>>(a);
   }
   return cudaGetLastError();
@@ -935,11 +957,8 @@ template <typename R, int LT, int CL>
 int cluster_fits() {
   using S = PassShape<LT>;
   const size_t smem = S::template smem<R>();
-  if (cudaFuncSetAttribute(pass_kernel<R, LT, CL, kPassThreads>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-    return 0;
-  if (CL > 3 && cudaFuncSetAttribute(pass_kernel<R, LT, CL, kPassThreads>,
-                                     cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)
+  if (ensure_smem_optin((const void*)pass_kernel<R, LT, CL, kPassThreads>, smem, CL > 3) !=
+      cudaSuccess)
     return 0;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(1u << CL, 1, 1);
@@ -963,15 +982,16 @@ int cluster_fits() {
 
 template <typename R, int LT>
 int max_cluster_log() {
-  static int cached = -1;  // per precision; one device type per process
-  if (cached < 0) {
+  // Per precision, probed once (one device type per process); the static's
+  // initialisation is thread-safe.
+  static const int cached = [] {
     int c = 0;
     if (cluster_fits<R, LT, 1>()) c = 1;
     if (c == 1 && cluster_fits<R, LT, 2>()) c = 2;
     if (c == 2 && cluster_fits<R, LT, 3>()) c = 3;
     if (c == 3 && cluster_fits<R, LT, 4>()) c = 4;
-    cached = c;
-  }
+    return c;
+  }();
   return cached;
 }
 }  // namespace
@@ -983,11 +1003,10 @@ PassGeomHost pass_geom(int precision, int n, int lmax, int threads, int lane_sme
   // tilings cover every axis when possible (2L - a >= n); above that, at the
   // widest compiled tile, a tiling's tile spans a cluster of 2^C CTAs
   // (2(L+C) - a >= n up to C = 4) before any axis is left to global memory.
-  static int env = -2;
-  if (env == -2) {
+  static const int env = [] {  // read once; thread-safe initialisation
     const char* e = getenv("MQW_PASS_TILE_LOG");
-    env = e ? atoi(e) : -1;
-  }
+    return e ? atoi(e) : -1;
+  }();
   int Lmax = precision == 0 ? 12 : 11;
   if (env >= 6 && env <= 13) Lmax = env;
   if (lmax >= 6 && lmax <= 13) Lmax = lmax;
@@ -1029,18 +1048,11 @@ template <typename R, int LT, int CL, int TB = kPassThreads, bool LS = false, bo
           bool COMP = false>
 cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
   using S = PassShape<LT, TB>;
-  static size_t configured = 0;
   const size_t smem = S::template smem<R, S::kStageP || TMA>();
-  if (smem > 48 * 1024 && smem > configured) {
-    cudaError_t e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB, LS, TMA, COMP>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  {
+    cudaError_t e = ensure_smem_optin((const void*)pass_kernel<R, LT, CL, TB, LS, TMA, COMP>,
+                                      smem, CL > 3);
     if (e != cudaSuccess) return e;
-    if (CL > 3) {
-      e = cudaFuncSetAttribute(pass_kernel<R, LT, CL, TB, LS, TMA, COMP>,
-                               cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
-      if (e != cudaSuccess) return e;
-    }
-    configured = smem;
   }
   const dim3 grid((unsigned)((size_t)1 << (p.n - LT)), p.count);
   if constexpr (CL == 0) {

@@ -1,0 +1,465 @@
+// Stage-2 product-basis GEMM on the tensor cores (tcgen05, kind::tf32) with
+// a three-product TF32 split, for FP32 accuracy.
+//
+// The product basis (mqw_stage2.cu) gives every walk's stage-2 output as one
+// column of a real GEMM per parity class h:
+//   out_h[walk][amp] = sum_q Y_h[q][amp] C_h[q][walk]
+// (q the (j, k) pairs of the class, K_h of them; Y the basis vectors, 2^n
+// floats each; C the walks' coefficient products). Here the amplitudes are
+// the MMA's M dimension (two M = 128 halves per CTA, 256 amplitudes), the
+// walks its N dimension (padded to a multiple of 16, at most 128) and the
+// pairs its K dimension, in chunks of 32.
+//
+// TF32 keeps 10 mantissa bits. Each FP32 operand is split as x = hi + lo
+// with hi = x rounded to TF32 (exact in TF32) and lo = x - hi (exact in
+// FP32, |lo| <= 2^-11 |x|), and the product is accumulated as
+//   A_hi B_hi + A_hi B_lo + A_lo B_hi
+// in the FP32 TMEM accumulator; the dropped A_lo B_lo term and the TF32
+// rounding of the lo parts are ~2^-21 relative, the level of FP32 rounding.
+// The coefficient matrix is split once (s2_coef_tc_kernel, K-major hi and lo
+// copies); the basis tile is split in shared memory as it arrives.
+//
+// Data movement: Y tiles (MN-major: 32 amplitudes x 32 pairs per box, eight
+// boxes per chunk) and the C tiles (K-major: 32 pairs x N walks) arrive by
+// TMA (cp.async.bulk.tensor, 128-byte swizzle, no multicast) on an mbarrier
+// per pipeline stage. Warp roles per CTA (192 threads):
+//   warp 0      TMA producer (one thread);
+//   warp 1      TMEM allocator and MMA issuer (one thread issues tcgen05.mma);
+//   warps 2-5   split the Y tile into hi (in place) and lo, then, after the
+//               last chunk, read the accumulators (tcgen05.ld) and store
+//               them to the planar outputs (each warp reads its TMEM lane
+//               quarter: 32 amplitudes; a store covers 32 consecutive
+//               amplitudes of one walk).
+// Every wait is bounded (%globaltimer): on expiry the CTA sets bit 1 of the
+// device error word, the other roles see the abort flag and stop, in-flight
+// copies and MMAs are waited for (bounded), the TMEM is freed and the CTA
+// returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <map>
+#include <mutex>
+
+#include "mqw_internal.h"
+
+namespace mqw {
+namespace {
+
+constexpr int kTcM = 128;            // amplitudes per MMA (TMEM lanes)
+constexpr int kTcAmps = 2 * kTcM;    // amplitudes per CTA (two M halves)
+constexpr int kTcBK = 32;            // pairs per chunk: one 128-byte row of tf32
+constexpr int kTcStages = 2;
+constexpr int kTcThreads = 192;
+constexpr int kTcMaxN = 128;         // walks (MMA N) per CTA
+constexpr unsigned kTcTmemCols = 256;  // two accumulators at columns 0 and 128
+constexpr unsigned long long kTcWaitNs = 200000000ull;  // 200 ms
+
+// Shared-memory layout (offsets from a 1024-byte aligned base).
+constexpr unsigned kTcATile = kTcAmps * kTcBK * 4;        // 32 KB: eight 4 KB boxes
+constexpr unsigned kTcBTile = kTcMaxN * kTcBK * 4;        // 16 KB
+constexpr unsigned kTcStage = 2 * kTcATile + 2 * kTcBTile;  // A(hi), A lo, B hi, B lo
+constexpr unsigned kTcBarOff = kTcStages * kTcStage;
+constexpr unsigned kTcSmem = kTcBarOff + 128 + 1024;     // barriers + alignment slack
+
+struct TcArgs {
+  float* out;          // planar outputs: class 0 at out, class 1 at out + out_walks 2^n
+  unsigned* err;       // device error word (bit 1: a bounded wait expired)
+  int n, walks, out_walks;
+  int Np;              // MMA N: walks padded to a multiple of 16
+  int chunks[2];       // K chunks of 32 per class
+  int crow[2];         // first row of the class's hi copy in the C map (lo: + Np)
+};
+
+__device__ __forceinline__ unsigned saddr(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ unsigned long long gtime() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void bar_init(unsigned bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ bool bar_try(unsigned bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ void bar_arrive(unsigned bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void bar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+// Waits for phase `parity` of `bar`; false when the CTA is aborting or the
+// wait ran out of time (which starts the abort).
+__device__ __forceinline__ bool bar_wait(unsigned bar, unsigned parity, volatile int* abort_flag,
+                                         unsigned* err) {
+  const unsigned long long t0 = gtime();
+  while (!bar_try(bar, parity)) {
+    if (*abort_flag) return false;
+    if (gtime() - t0 > kTcWaitNs) {
+      *abort_flag = 1;
+      if (err) atomicOr(err, 2u);
+      return false;
+    }
+  }
+  return true;
+}
+// The same without the abort flag, for the teardown's drains.
+__device__ __forceinline__ void bar_drain(unsigned bar, unsigned parity) {
+  const unsigned long long t0 = gtime();
+  while (!bar_try(bar, parity))
+    if (gtime() - t0 > kTcWaitNs) return;
+}
+__device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map, int x, int y,
+                                            unsigned bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+// UMMA shared-memory descriptor, 128-byte swizzle (sm_100 version bits).
+// lbo/sbo in bytes.
+__device__ __forceinline__ unsigned long long umma_desc(unsigned addr, unsigned lbo, unsigned sbo) {
+  unsigned long long d = 0;
+  d |= (unsigned long long)((addr >> 4) & 0x3FFFu);
+  d |= (unsigned long long)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (unsigned long long)((sbo >> 4) & 0x3FFFu) << 32;
+  d |= 1ull << 46;  // descriptor version (sm_100)
+  d |= 2ull << 61;  // layout: 128-byte swizzle
+  return d;
+}
+// Instruction descriptor: D f32, A and B tf32, A MN-major, B K-major,
+// M = 128, N = Np.
+__device__ __forceinline__ unsigned umma_idesc(int Np) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | ((unsigned)(Np >> 3) << 17) |
+         ((unsigned)(kTcM >> 4) << 24);
+}
+__device__ __forceinline__ void umma_tf32(unsigned d_tmem, unsigned long long a,
+                                          unsigned long long b, unsigned idesc, bool acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"((unsigned)acc)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(unsigned bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+      : "memory");
+}
+
+// x = hi + lo: hi rounded to TF32 (nearest, ties away; 10 mantissa bits),
+// lo = x - hi exactly.
+__device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
+  const unsigned u = (__float_as_uint(x) + 0x1000u) & 0xFFFFE000u;
+  hi = __uint_as_float(u);
+  lo = x - hi;
+}
+
+__global__ void __launch_bounds__(kTcThreads, 1)
+    s2_gemm_tc_kernel(const __grid_constant__ CUtensorMap mapY0,
+                      const __grid_constant__ CUtensorMap mapY1,
+                      const __grid_constant__ CUtensorMap mapC, TcArgs p) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ unsigned tmem_base_sh;
+  __shared__ int abort_sh;
+  unsigned char* smem = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+  const unsigned sbase = saddr(smem);
+  const unsigned bars = sbase + kTcBarOff;
+  auto full = [&](int s) { return bars + 8u * s; };
+  auto conv = [&](int s) { return bars + 8u * (kTcStages + s); };
+  auto empty = [&](int s) { return bars + 8u * (2 * kTcStages + s); };
+  const unsigned accf = bars + 8u * (3 * kTcStages);
+  auto a_tile = [&](int s) { return sbase + s * kTcStage; };
+  auto alo_tile = [&](int s) { return sbase + s * kTcStage + kTcATile; };
+  auto bhi_tile = [&](int s) { return sbase + s * kTcStage + 2 * kTcATile; };
+  auto blo_tile = [&](int s) { return sbase + s * kTcStage + 2 * kTcATile + kTcBTile; };
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int h = blockIdx.y;
+  const int m0 = blockIdx.x * kTcAmps;
+  const int chunks = p.chunks[h];
+  volatile int* abort_flag = &abort_sh;
+
+  if (threadIdx.x == 0) {
+    abort_sh = 0;
+    for (int s = 0; s < kTcStages; s++) {
+      bar_init(full(s), 1);
+      bar_init(conv(s), 128);
+      bar_init(empty(s), 1);
+    }
+    bar_init(accf, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     saddr(&tmem_base_sh)),
+                 "r"(kTcTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const unsigned tmem = tmem_base_sh;
+  const unsigned b_bytes = (unsigned)p.Np * kTcBK * 4u;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // TMA producer.
+      const CUtensorMap* mY = h ? &mapY1 : &mapY0;
+      int issued = 0;
+      for (int c = 0; c < chunks; c++) {
+        const int s = c % kTcStages;
+        if (c >= kTcStages && !bar_wait(empty(s), ((c / kTcStages) - 1) & 1, abort_flag, p.err))
+          break;
+        bar_expect_tx(full(s), kTcATile + 2 * b_bytes);
+        const int k0 = c * kTcBK;
+        for (int b = 0; b < kTcAmps / 32; b++)
+          tma_load_2d(a_tile(s) + b * 4096u, mY, m0 + 32 * b, k0, full(s));
+        tma_load_2d(bhi_tile(s), &mapC, k0, p.crow[h], full(s));
+        tma_load_2d(blo_tile(s), &mapC, k0, p.crow[h] + p.Np, full(s));
+        issued = c + 1;
+      }
+      if (*abort_flag) {
+        // Copies issued but never consumed must land before the CTA's shared
+        // memory is released; only the last kTcStages chunks can be pending
+        // (a stage is reissued only after its previous chunk was consumed).
+        for (int c = issued > kTcStages ? issued - kTcStages : 0; c < issued; c++)
+          bar_drain(full(c % kTcStages), (c / kTcStages) & 1);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // MMA issuer.
+      const unsigned idesc = umma_idesc(p.Np);
+      int done = 0;
+      for (int c = 0; c < chunks; c++) {
+        const int s = c % kTcStages;
+        if (!bar_wait(conv(s), (c / kTcStages) & 1, abort_flag, p.err)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+        for (int kk = 0; kk < kTcBK / 8; kk++) {
+#pragma unroll
+          for (int half = 0; half < 2; half++) {
+            const unsigned long long ahi =
+                umma_desc(a_tile(s) + half * (kTcATile / 2) + kk * 1024u, 4096u, 1024u);
+            const unsigned long long alo =
+                umma_desc(alo_tile(s) + half * (kTcATile / 2) + kk * 1024u, 4096u, 1024u);
+            const unsigned long long bhi = umma_desc(bhi_tile(s) + kk * 32u, 16u, 1024u);
+            const unsigned long long blo = umma_desc(blo_tile(s) + kk * 32u, 16u, 1024u);
+            const unsigned d = tmem + (unsigned)(half * kTcM);
+            umma_tf32(d, ahi, bhi, idesc, c > 0 || kk > 0);
+            umma_tf32(d, ahi, blo, idesc, true);
+            umma_tf32(d, alo, bhi, idesc, true);
+          }
+        }
+        umma_commit(empty(s));  // the stage's tiles are free once these MMAs finish
+        done = c + 1;
+      }
+      umma_commit(accf);  // every MMA issued so far has completed when accf flips
+      if (*abort_flag || done < chunks) bar_drain(accf, 0);
+    }
+    __syncwarp();
+  } else {
+    // Warps 2-5: split each Y tile into hi (in place) and lo.
+    const int ct = threadIdx.x - 64;  // 0..127
+    bool ok = true;
+    for (int c = 0; c < chunks && ok; c++) {
+      const int s = c % kTcStages;
+      if (!bar_wait(full(s), (c / kTcStages) & 1, abort_flag, p.err)) {
+        ok = false;
+        break;
+      }
+      float4* a = reinterpret_cast<float4*>(smem + s * kTcStage);
+      float4* alo = reinterpret_cast<float4*>(smem + s * kTcStage + kTcATile);
+#pragma unroll 4
+      for (int e = ct; e < (int)(kTcATile / 16); e += 128) {
+        const float4 v = a[e];
+        float4 hi, lo;
+        split_tf32(v.x, hi.x, lo.x);
+        split_tf32(v.y, hi.y, lo.y);
+        split_tf32(v.z, hi.z, lo.z);
+        split_tf32(v.w, hi.w, lo.w);
+        a[e] = hi;
+        alo[e] = lo;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      bar_arrive(conv(s));
+    }
+    // Epilogue: this warp's TMEM lane quarter = 32 amplitudes of each half.
+    if (ok && bar_wait(accf, 0, abort_flag, p.err)) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int q = warp & 3;
+      const size_t N = (size_t)1 << p.n;
+      float* out = p.out + (size_t)h * p.out_walks * N;
+      for (int half = 0; half < 2; half++) {
+        const size_t amp = (size_t)m0 + half * kTcM + 32 * q + lane;
+        for (int c0 = 0; c0 < p.Np; c0 += 8) {
+          const unsigned ta = tmem + ((unsigned)(32 * q) << 16) + (unsigned)(half * kTcM + c0);
+          unsigned r[8];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+              : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                "=r"(r[6]), "=r"(r[7])
+              : "r"(ta)
+              : "memory");
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int j = 0; j < 8; j++)
+            if (c0 + j < p.walks) out[(size_t)(c0 + j) * N + amp] = __uint_as_float(r[j]);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(kTcTmemCols)
+                 : "memory");
+  }
+}
+
+// K-major hi/lo copies of the coefficient matrices: row (2h + part) Np + w,
+// column q (the class's pair index), Kp columns per row; zero outside the
+// class's rows and walks.
+__global__ void s2_coef_tc_kernel(S2CoefParams p, float* Ct, int Np, int Kp) {
+  const size_t total = (size_t)2 * Np * Kp;  // (class, walk, q)
+  for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (size_t)gridDim.x * blockDim.x) {
+    const int h = (int)(e / ((size_t)Np * Kp));
+    const size_t r = e - (size_t)h * Np * Kp;
+    const int w = (int)(r / Kp), q = (int)(r % Kp);
+    float v = 0.0f;
+    if (q < p.lay.rows(h) && w < p.walks) {
+      int j, k;
+      p.lay.pair(h, q, &j, &k);
+      const StageDesc s1 = p.stages[p.job0 + w * p.m];
+      const StageDesc s2 = p.stages[p.job0 + w * p.m + 1];
+      auto weight = [](const float* c, int K, int i) {
+        const double ci = i < K ? (double)c[i] : 0.0;
+        const double ci2 = i + 2 < K ? (double)c[i + 2] : 0.0;
+        return i == 0 ? ci - 0.5 * ci2 : 0.5 * (ci - ci2);
+      };
+      const double d1 = weight(p.coef + s1.coef_off, s1.K, j);
+      const double d2 = weight(p.coef + s2.coef_off, s2.K, k);
+      const double sg = (h == 0 && (j & 1) && (k & 1)) ? -1.0 : 1.0;
+      v = (float)(sg * d1 * d2);
+    }
+    float hi, lo;
+    split_tf32(v, hi, lo);
+    Ct[((size_t)(2 * h) * Np + w) * Kp + q] = hi;
+    Ct[((size_t)(2 * h + 1) * Np + w) * Kp + q] = lo;
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      f = nullptr;
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// 2-D float32 tensor map, 128-byte swizzle: dims {inner, outer}, row pitch
+// in bytes, box {bx, by}.
+bool make_map(CUtensorMap* m, const float* base, unsigned long long inner,
+              unsigned long long outer, unsigned long long pitch, unsigned bx, unsigned by) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
+  if (!enc) return false;
+  const cuuint64_t dims[2] = {inner, outer};
+  const cuuint64_t strides[1] = {pitch};
+  const cuuint32_t box[2] = {bx, by};
+  const cuuint32_t es[2] = {1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box,
+             es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
+std::mutex g_tc_mu;
+std::map<int, bool> g_tc_optin;  // per device: the kernel's shared-memory opt-in is made
+
+}  // namespace
+
+int s2_tc_np(int walks) { return (walks + 15) / 16 * 16; }
+int s2_tc_kp(const S2Layout& lay) {
+  const int r = lay.rows(0) > lay.rows(1) ? lay.rows(0) : lay.rows(1);
+  return (r + kTcBK - 1) / kTcBK * kTcBK;
+}
+size_t s2_tc_coef_floats(int walks, const S2Layout& lay) {
+  return (size_t)4 * s2_tc_np(walks) * s2_tc_kp(lay);
+}
+
+cudaError_t launch_s2_gemm_tc(const S2CoefParams& cp, float* Ct, const S2GemmParams& g,
+                              unsigned* err, cudaStream_t stream) {
+  const int Np = s2_tc_np(g.walks);
+  const int Kp = s2_tc_kp(cp.lay);
+  if (g.n < 8 || g.n > kMaxN || !g.Y || !g.out || !Ct || g.walks < 1 || Np > kTcMaxN ||
+      g.out_walks < g.walks || g.rows[0] < 1 || g.rows[1] < 1 || cp.walks != g.walks ||
+      cp.lay.rows(0) != g.rows[0] || cp.lay.rows(1) != g.rows[1] || !encode_fn())
+    return cudaErrorInvalidValue;
+  // Coefficients: K-major hi/lo copies.
+  {
+    const size_t total = (size_t)2 * Np * Kp;
+    const size_t want = (total + 255) / 256;
+    s2_coef_tc_kernel<<<(unsigned)(want < 8192 ? want : 8192), 256, 0, stream>>>(cp, Ct, Np, Kp);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  const unsigned long long N = 1ull << g.n;
+  CUtensorMap mY0, mY1, mC;
+  if (!make_map(&mY0, g.Y, N, (unsigned long long)g.rows[0], N * 4, 32, kTcBK) ||
+      !make_map(&mY1, g.Y + (size_t)g.rows[0] * N, N, (unsigned long long)g.rows[1], N * 4, 32,
+                kTcBK) ||
+      !make_map(&mC, Ct, (unsigned long long)Kp, 4ull * Np, (unsigned long long)Kp * 4, kTcBK,
+                (unsigned)Np))
+    return cudaErrorInvalidValue;
+  TcArgs a{};
+  a.out = g.out;
+  a.err = err;
+  a.n = g.n;
+  a.walks = g.walks;
+  a.out_walks = g.out_walks;
+  a.Np = Np;
+  for (int h = 0; h < 2; h++) {
+    a.chunks[h] = (g.rows[h] + kTcBK - 1) / kTcBK;
+    a.crow[h] = 2 * h * Np;
+  }
+  {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(g_tc_mu);
+    if (!g_tc_optin[dev]) {
+      e = cudaFuncSetAttribute(s2_gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)kTcSmem);
+      if (e != cudaSuccess) return e;
+      g_tc_optin[dev] = true;
+    }
+  }
+  const dim3 grid((unsigned)(N / kTcAmps), 2);
+  s2_gemm_tc_kernel<<<grid, kTcThreads, kTcSmem, stream>>>(mY0, mY1, mC, a);
+  return cudaGetLastError();
+}
+
+}  // namespace mqw

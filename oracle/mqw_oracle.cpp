@@ -456,12 +456,16 @@ void orc_clenshaw_f64(int n, int K, const float* coeffs, const double* hp,
 // with the reference's Clenshaw_step signature.
 // Outputs per instance: mean ground-state probability, total_t, E_loc and
 // the summed Chebyshev degree (work accounting).
-int orc_run_problems_ext(int n, int m, const double* raw, int count,
-                         int samples_used, int mode, double* p_out,
-                         float* total_t_out, uint32_t* e_loc_out,
-                         long long* terms_out, void* ext_step) {
+// Samples [s_begin, s_end) of each instance; p_out receives the mean over
+// them, and psum_out (nullable) their sum. With m == 1 the samples are
+// cumulative steps of one walk (MultiQW.cpp:426-430), so s_begin must be 0.
+static int run_samples(int n, int m, const double* raw, int count, int s_begin,
+                       int samples_used, int mode, double* p_out, double* psum_out,
+                       float* total_t_out, uint32_t* e_loc_out, long long* terms_out,
+                       void* ext_step) {
   if (n < 1 || n > 30 || m < 1 || count < 0) return -1;
   if (samples_used < 1 || samples_used > kSamples) return -1;
+  if (s_begin < 0 || s_begin >= samples_used || (m == 1 && s_begin != 0)) return -1;
   const size_t N = size_t(1) << n;
   const int per = n * (n + 1) / 2;
   std::vector<float> J(n * n), h(n), hp(N), psi(2 * N), out(2 * N);
@@ -499,7 +503,7 @@ int orc_run_problems_ext(int n, int m, const double* raw, int count,
     reset();
     bool psi_real = true;
     double psum = 0.0;
-    for (int j = 0; j < samples_used; j++) {
+    for (int j = s_begin; j < samples_used; j++) {
       for (int i = 0; i < m; i++) {
         float gamma = gammas[i];
         // E_abs + gamma*n (MultiQW.cpp:436), with the multiply-add fused as
@@ -546,12 +550,32 @@ int orc_run_problems_ext(int n, int m, const double* raw, int count,
       }
     }
     // Mean over samples (MultiQW.cpp:454), accumulated in double.
-    p_out[p] = psum / samples_used;
+    p_out[p] = psum / (samples_used - s_begin);
+    if (psum_out) psum_out[p] = psum;
     if (total_t_out) total_t_out[p] = total_t;
     if (e_loc_out) e_loc_out[p] = d.e_loc;
     if (terms_out) terms_out[p] = terms;
   }
   return 0;
+}
+
+int orc_run_problems_ext(int n, int m, const double* raw, int count,
+                         int samples_used, int mode, double* p_out,
+                         float* total_t_out, uint32_t* e_loc_out,
+                         long long* terms_out, void* ext_step) {
+  return run_samples(n, m, raw, count, 0, samples_used, mode, p_out, nullptr, total_t_out,
+                     e_loc_out, terms_out, ext_step);
+}
+
+// Samples [s_begin, s_end) of one instance: the sum of their ground-state
+// probabilities (so that ranges run in separate processes add up to the
+// reference's per-instance sum, MultiQW.cpp:432-454) and their summed degree.
+int orc_run_sample_range_ext(int n, int m, const double* raw, int s_begin, int s_end,
+                             int mode, double* psum_out, long long* terms_out,
+                             void* ext_step) {
+  double p = 0.0;
+  return run_samples(n, m, raw, 1, s_begin, s_end, mode, &p, psum_out, nullptr, nullptr,
+                     terms_out, ext_step);
 }
 
 int orc_run_problems(int n, int m, const double* raw, int count,

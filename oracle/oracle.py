@@ -43,13 +43,25 @@ def _ptr(a: np.ndarray | None, ctype):
     return a.ctypes.data_as(_P(ctype))
 
 
+def reference_dir() -> str | None:
+    """The reference checkout to build the partial reference from: the
+    directory named by MQW_REFERENCE_DIR, else a checkout named `reference`
+    beside this repository; None when neither holds MultiQW.cpp."""
+    env = os.environ.get("MQW_REFERENCE_DIR")
+    cands = [env] if env else [os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")]
+    for c in cands:
+        if c and os.path.exists(os.path.join(c, "MultiQW.cpp")):
+            return c
+    return None
+
+
 def build(quiet: bool = True) -> None:
     """Compile liboracle.so (and the partial reference build when the
     reference tree is present)."""
     out = subprocess.DEVNULL if quiet else None
     subprocess.check_call(["make", "-C", HERE, "liboracle.so"], stdout=out)
-    ref_src = os.environ.get("MQW_REFERENCE_DIR", "/root/reference")
-    if os.path.exists(os.path.join(ref_src, "MultiQW.cpp")):
+    ref_src = reference_dir()
+    if ref_src:
         subprocess.check_call(["make", "-C", HERE, "ref", f"REF={ref_src}"], stdout=out)
 
 
@@ -74,6 +86,7 @@ def lib():
         L.orc_clenshaw_f32_ext.argtypes = [_c_int, _c_int, _P(_c_float), _P(_c_float), _c_float, _c_float, _P(_c_float), _P(_c_float), _c_int, ctypes.c_void_p]
         L.orc_clenshaw_f64.argtypes = [_c_int, _c_int, _P(_c_float), _P(_c_double), _c_float, _c_float, _P(_c_double), _P(_c_double), _c_int]
         L.orc_run_problems_ext.argtypes = [_c_int, _c_int, _P(_c_double), _c_int, _c_int, _c_int, _P(_c_double), _P(_c_float), _P(ctypes.c_uint32), _P(ctypes.c_longlong), ctypes.c_void_p]
+        L.orc_run_sample_range_ext.argtypes = [_c_int, _c_int, _P(_c_double), _c_int, _c_int, _c_int, _P(_c_double), _P(ctypes.c_longlong), ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -223,6 +236,25 @@ def run_problems(n: int, m: int, raw: np.ndarray, count: int, samples_used: int 
     if rc != 0:
         raise RuntimeError(f"orc_run_problems failed: {rc}")
     return {"p": p, "total_t": tt, "e_loc": el, "terms": terms}
+
+
+def run_sample_range(n: int, m: int, raw: np.ndarray, s_begin: int, s_end: int,
+                     mode: str = "f32", use_ref_step: bool = False):
+    """Samples [s_begin, s_end) of one instance through the reference
+    pipeline: (sum of their ground-state probabilities, summed degree)."""
+    raw = np.ascontiguousarray(raw, dtype=np.float64).ravel()
+    assert raw.size >= params_per_instance(n)
+    ps = np.zeros(1, np.float64)
+    terms = np.zeros(1, np.int64)
+    ext = ref_step_ptr() if use_ref_step else None
+    if use_ref_step and ext is None:
+        raise RuntimeError("partial reference build not available")
+    rc = lib().orc_run_sample_range_ext(n, m, _ptr(raw, _c_double), s_begin, s_end,
+                                        0 if mode == "f32" else 1, _ptr(ps, _c_double),
+                                        _ptr(terms, ctypes.c_longlong), ext)
+    if rc != 0:
+        raise RuntimeError(f"orc_run_sample_range failed: {rc}")
+    return float(ps[0]), int(terms[0])
 
 
 def sk_instances(n: int, count: int, seed: int, j_std: float = 1.0, h_std: float = 1.0) -> np.ndarray:

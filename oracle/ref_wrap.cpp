@@ -6,8 +6,8 @@
 // extracts exactly that span from the reference source into
 // oracle/_ref/ref_span.inc; nothing of it is committed. The Eigen-dependent
 // driver (Clenshaw, main) is not buildable here because Eigen 3.4 and the
-// ApproxTools submodule are absent; its loop is restated in
-// ref_driver.cpp / mqw_oracle.cpp instead.
+// ApproxTools submodule are absent; its loop is restated in mqw_oracle.cpp
+// instead.
 #include <math.h>
 #include <stdint.h>
 #include <string.h>

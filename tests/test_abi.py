@@ -149,3 +149,40 @@ def test_struct_layouts_match_header(tmp_path):
         assert int(out[name]) == ctypes.sizeof(cls), name
         for field, _ in cls._fields_:
             assert int(out[f"{name}.{field}"]) == getattr(cls, field).offset, (name, field)
+
+
+def _ranges_like_reference(problems, threads):
+    """run.sh:27-33's split, restated: contiguous ranges, the first
+    problems % threads of them one longer."""
+    base, extra = divmod(problems, threads)
+    out = []
+    for t in range(threads):
+        start = t * base + min(t, extra)
+        count = base + (1 if t < extra else 0)
+        if count:
+            out.append((start, count))
+    return out
+
+
+@pytest.mark.parametrize("threads,problems", [(1, 2000), (3, 10), (7, 2000), (16, 30), (5, 3)])
+def test_run_driver_splits_like_the_reference(mqw, tmp_path, threads, problems):
+    """The run.sh-compatible driver issues exactly the reference script's
+    ranges for every (n, m) of its lists, devices dealt round-robin."""
+    script = os.path.join(os.path.dirname(mqw.LIB_PATH), "..", "run.sh")
+    (tmp_path / "x_6n").write_bytes(b"")
+    env = dict(os.environ, MQW_DRY_RUN="1", MQW_N_VALUES="6", MQW_M_VALUES="1 2",
+               MQW_PROBLEMS=str(problems), MQW_DEVICES="0 1")
+    r = subprocess.run(["bash", script, str(threads), "x"], cwd=tmp_path, env=env,
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.strip().splitlines()
+    want = []
+    for m in (1, 2):
+        for k, (s, c) in enumerate(_ranges_like_reference(problems, threads)):
+            want.append((f"MQW_DEVICE={k % 2}", "6", str(m), str(s), str(c)))
+    got = []
+    for ln in lines:
+        f = ln.split()
+        got.append((f[0], f[2], f[3], f[5], f[6]))
+    # ranges with no problems are not launched (the reference starts them anyway)
+    assert got == [w for w in want]

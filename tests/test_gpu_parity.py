@@ -556,3 +556,89 @@ def test_tier_peaks(ctx):
     assert 2000 < t["hbm_copy_gbs"] < 9000, t
     assert t["l2_read_gbs"] > t["hbm_copy_gbs"], t
     assert t["smem_gbs"] > t["l2_read_gbs"], t
+
+
+def test_mixed_batch_per_instance_fp32_vs_fp64(ctx, mqw):
+    """The mixed batch's first 16 instances (n in {12..20}, m in {2..5},
+    drawn like the 4096-instance batch) as one FP32 plan at the full 100
+    samples, every instance within 1e-5 of the same plan in FP64, with the
+    same ground-state index; the draw covers n = 18 and 20 and m = 5."""
+    from multistageqw_b200 import studies
+    ns, ms, raw = studies.mixed_batch(16, 0)
+    assert {18, 20} <= set(ns) and max(ms) == 5
+    out = {}
+    for prec in ("fp32", "fp64"):
+        plan = mqw.Plan(ctx, ns, ms, raw, samples=100, precision=prec, graph=0)
+        plan.execute()
+        out[prec] = plan.results()
+        plan.close()
+    dP = np.abs(out["fp32"]["p"] - out["fp64"]["p"])
+    assert dP.max() <= 1e-5, dP
+    assert out["fp32"]["e_loc"].tolist() == out["fp64"]["e_loc"].tolist()
+
+
+def test_n28_m3_fp32_vs_fp64(ctx, orc):
+    """The largest size, n = 28 (2^28 amplitudes, tiles over clusters or
+    with global-memory axes), m = 3, one sample of the seed-7 instance: FP32
+    within 1e-5 of FP64 and the reference-arithmetic ground-state index."""
+    raw = orc.sk_instances(28, 1, 7)
+    r32 = ctx.run_problems(28, 3, raw, samples=1, precision="fp32")
+    r64 = ctx.run_problems(28, 3, raw, samples=1, precision="fp64")
+    assert 0.0 <= r32["p"][0] <= 1.0
+    assert abs(r32["p"][0] - r64["p"][0]) <= 1e-5
+    assert r32["e_loc"][0] == r64["e_loc"][0]
+
+
+def test_run_driver_output_is_in_problem_order(mqw, orc, tmp_path):
+    """The run.sh-compatible driver over 4 concurrent ranges writes
+    output_<n>_<m> byte-identical to one MultiQW run over the whole range
+    (problem order, not completion order), for every (n, m) of its lists,
+    and appends like the reference."""
+    import os
+    raw = orc.sk_instances(7, 23, 5)
+    (tmp_path / "SK_7n").write_bytes(raw.tobytes())
+    single = tmp_path / "single"
+    single.mkdir()
+    for m in (1, 3):
+        r = subprocess.run([mqw.CLI_PATH, "7", str(m), str(tmp_path / "SK_7n"), "0", "23"],
+                           cwd=single, capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+    script = os.path.join(os.path.dirname(mqw.LIB_PATH), "..", "run.sh")
+    env = dict(os.environ, MQW_N_VALUES="7", MQW_M_VALUES="1 3", MQW_PROBLEMS="23")
+    for _ in range(2):  # the second run appends
+        r = subprocess.run(["bash", script, "4", "SK"], cwd=tmp_path, env=env,
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        assert len(r.stdout.strip().splitlines()) == 46
+    for m in (1, 3):
+        a = (single / f"output_7_{m}").read_bytes()
+        assert len(a) == 23 * 4
+        assert (tmp_path / f"output_7_{m}").read_bytes() == a + a
+
+
+@pytest.mark.parametrize("n,m,samples", [(16, 3, 24), (20, 4, 100), (14, 5, 7)])
+def test_stage2_tensor_core_gemm_matches_simt(ctx, orc, mqw, monkeypatch, n, m, samples):
+    """The stage-2 product-basis GEMM on the tensor cores (tcgen05 kind::tf32
+    with the three-product TF32 split, the default) against the FP32 SIMT
+    GEMM (MQW_S2_GEMM=simt) on the same product basis: per-sample P within
+    FP32-level rounding (5e-6 relative), the mean within 1e-5 of FP64; 7
+    walks take a 16-column MMA, 100 walks a 112-column one."""
+    raw = orc.sk_instances(n, 1, 5100 + n)
+    monkeypatch.setenv("MQW_STAGE2_BASIS", "1")
+
+    def run(gemm):
+        if gemm:
+            monkeypatch.setenv("MQW_S2_GEMM", gemm)
+        else:
+            monkeypatch.delenv("MQW_S2_GEMM", raising=False)
+        plan = mqw.Plan(ctx, n, m, raw, samples=samples, graph=0)
+        plan.execute()
+        out = plan.results(per_sample=True)["p_sample"]
+        plan.close()
+        return out
+
+    tc = run(None)
+    simt = run("simt")
+    np.testing.assert_allclose(tc, simt, rtol=5e-6, atol=1e-9)
+    r64 = ctx.run_problems(n, m, raw, samples=samples, precision="fp64", graph=0)
+    assert abs(float(np.mean(tc)) - r64["p"][0]) <= 1e-5

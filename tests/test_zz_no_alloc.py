@@ -1,8 +1,8 @@
 """The allocation-free propagation entry point (mqw_clenshaw_noalloc).
 
-It serves callers that cannot allocate device memory — code running while a
-CUDA graph is captured, code that must not synchronise the device, hosts whose
-own allocator owns all device memory. It must give the same result as the
+It serves callers that cannot allocate device memory — code that must not
+synchronise the device, hosts whose own allocator or fixed memory budget owns
+all device memory. It must give the same result as the
 ordinary entry point (mqw_clenshaw), including on a second call that reuses
 the working space the first call left behind, and it must refuse sizes beyond
 its fixed working space with an error instead of touching memory.
