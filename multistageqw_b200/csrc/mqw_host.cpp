@@ -70,7 +70,8 @@ struct GridShape {
   int lmax = 0, group = 1, lanes = 1;
   int threads = 0;  // CTA threads at the widest tile (0: 512)
   int lane_smem = 0;  // lane axes: 1 shared memory, -1 shuffles, 0 (want): any
-  int tma = 0;        // staging: 1 bulk copies, -1 cp.async, 0 (want): any
+  int tma = 0;        // staging: 1 bulk copies, 2 psi straight into registers,
+                      // -1 cp.async, 0 (want): any
   double us = 0.0;  // timed microseconds per walk-pass (0: not timed)
   int bgroup = 1;   // walks per shared-basis group (>= group; set by the plan)
 };
@@ -425,9 +426,9 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
     return g <= kMaxGroup && (size_t)g * lanes * walk_bytes(precision, geo, n) <= budget;
   };
   auto time = [&](const GridShape& c, double* us) -> mqw_status {
-    const PassGeomHost geo = pass_geom(precision, n, c.lmax, c.threads, c.lane_smem > 0, c.tma > 0);
+    const PassGeomHost geo = pass_geom(precision, n, c.lmax, c.threads, c.lane_smem > 0, std::max(0, c.tma));
     mqw_status s = time_grid_config(ctx, precision, n, c.lmax, c.group, c.lanes, c.threads,
-                                    c.lane_smem > 0, c.tma > 0, us);
+                                    c.lane_smem > 0, std::max(0, c.tma), us);
     if (s == MQW_OK && log)
       fprintf(stderr,
               "mqw tune: precision %d n %d tile %d cluster %d global %d threads %d lane_smem %d "
@@ -454,17 +455,17 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
     if (want.lmax && l != want.lmax) continue;
     for (int threads : {0, 256})
       for (int ls : {0, 1})
-        for (int tma : {0, 1}) {
+        for (int tma : {0, 1, 2}) {
           if (want.threads && (want.threads == 256) != (threads == 256)) continue;
           if (want.lane_smem && (want.lane_smem > 0) != (ls == 1)) continue;
-          if (want.tma && (want.tma > 0) != (tma == 1)) continue;
+          if (want.tma && std::max(0, want.tma) != tma) continue;
           const PassGeomHost geo = pass_geom(precision, n, l, threads, ls, tma);
           if (geo.threads != threads || geo.lane_smem != ls || geo.tma != tma) continue;
           GridShape c;
           c.lmax = l;
           c.threads = threads;
           c.lane_smem = ls ? 1 : -1;
-          c.tma = tma ? 1 : -1;
+          c.tma = tma ? tma : -1;
           c.group = want.group ? want.group : 1;
           c.lanes = want.lanes ? want.lanes : (fits(geo, c.group, 2) ? 2 : 1);
           if (!fits(geo, c.group, c.lanes)) continue;
@@ -482,7 +483,7 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
   }
   // Stage 2: walks per launch and lanes for that shape.
   if (best < 1e300 && (!want.group || !want.lanes)) {
-    const PassGeomHost geo = pass_geom(precision, n, b.lmax, b.threads, b.lane_smem > 0, b.tma > 0);
+    const PassGeomHost geo = pass_geom(precision, n, b.lmax, b.threads, b.lane_smem > 0, std::max(0, b.tma));
     const int g0 = default_group(precision, geo, n);
     std::vector<int> groups = {1, 2, 4};
     if (g0 != 1 && g0 != 2 && g0 != 4) groups.push_back(g0);
@@ -1011,7 +1012,7 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
   for (auto& kv : grid_by_n) {
     const int n = kv.first;
     const GridShape gs = P.grid_geo.at(n);
-    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, gs.tma > 0);
+    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, std::max(0, gs.tma));
     const int G = gs.group;
     const std::vector<int>& ws = kv.second;
     const int kb1 = P.basis_kb1.count(n) ? P.basis_kb1.at(n) : 0;
@@ -1255,7 +1256,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     gs.group = std::min(std::min(gs.group, kMaxGroup), kv.second);
     const int ngroups = (kv.second + gs.group - 1) / gs.group;
     gs.lanes = std::max(1, std::min(gs.lanes, ngroups));
-    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, gs.tma > 0);
+    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, std::max(0, gs.tma));
     // Walks per shared-basis group: the stage-1 recombination and the
     // last-stage projection read each basis vector once per group, so the
     // group is as large as the launch structures allow (kMaxGroup) within a
@@ -1358,7 +1359,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       const int n = e.first;
       const GridShape& gs = P.grid_geo.at(n);
       const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads,
-                                         gs.lane_smem > 0, gs.tma > 0);
+                                         gs.lane_smem > 0, std::max(0, gs.tma));
       int k1 = want1 && e.second.first <= kMaxBasis ? e.second.first : 0;
       int k2 = want2 && e.second.second <= kMaxBasis ? e.second.second : 0;
       if (BasisLayout::bytes(n, k1, k2) > budget) k2 = 0;
@@ -1841,7 +1842,7 @@ mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,
   want.group = want.lanes = 0;  // nothing fixed
   st = tune_grid(ctx, precision, n, want, &gs);
   if (st != MQW_OK) return st;
-  const PassGeomHost geo = pass_geom(precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, gs.tma > 0);
+  const PassGeomHost geo = pass_geom(precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, std::max(0, gs.tma));
   out->tile_log = geo.L;
   out->threads = geo.threads ? geo.threads : 512;
   out->lane_smem = geo.lane_smem;
@@ -1868,7 +1869,7 @@ mqw_status mqw_pass_timing(mqw_ctx* ctx, int precision, int n, int reps,
   if (st != MQW_OK) return st;
   double us = 0.0;
   st = time_grid_config(ctx, precision, n, gs.lmax, gs.group, gs.lanes, gs.threads,
-                        gs.lane_smem > 0, gs.tma > 0, &us, reps);
+                        gs.lane_smem > 0, std::max(0, gs.tma), &us, reps);
   if (st != MQW_OK) return st;
   // time_grid_config returns the elapsed time per walk-pass: launches carry
   // `group` walks and `lanes` launches are in flight at a time.

@@ -507,8 +507,14 @@ constexpr int pass_min_blocks() {
 // slower than cp.async.
 // COMP: the partner sums are compensated (PartnerSum<float, true>): the
 // FP32-compensated precision mode.
+// DR: psi goes straight from global memory into registers instead of
+// through cp.async staging, which saves its shared-memory write and read;
+// the freed space holds a second exchange tile, so b_r is written to it
+// without first waiting for every reader of b_{r+1}'s tile (one block
+// barrier fewer per pass). Shapes with P in registers (8 pairs per thread)
+// only.
 template <typename R, int LT, int CL, int TB, bool LS = false, bool TMA = false,
-          bool COMP = false>
+          bool COMP = false, bool DR = false>
 __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
                                   pass_min_blocks<LT, TB, sizeof(R) == 4, CL>())
     pass_kernel(PassParams p) {
@@ -516,6 +522,8 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   constexpr int RP = S::kRP, LOGT = S::kLogT, T = S::kThreads;
   constexpr bool kStageP = S::kStageP || TMA;
   static_assert(!TMA || CL == 0, "bulk-copy staging is for single-CTA tiles");
+  static_assert(!DR || (!kStageP && CL == 0 && !TMA && !LS),
+                "direct loads need P in registers and a single-CTA tile");
   constexpr int LL = LT + CL;  // tile bits of the tiling
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[32];
@@ -528,6 +536,7 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   R* sp = sx + 4 * S::kPairs;              // staged P_r, [j][tid] pairs
   R* ss = kStageP ? sp + 4 * S::kPairs : sp;  // staged psi
   float2* sd = reinterpret_cast<float2*>(ss + 4 * S::kPairs);  // staged D
+  R* sx2 = DR ? ss : sx;  // DR: b_r's exchange tile (where psi would be staged)
   // Global amplitude index of register pair j: g0 + j * gstride (32-bit: n <= 30).
   // For a 1-D cluster the cluster rank is blockIdx.x mod 2^CL.
   const unsigned rank = CL > 0 ? (blockIdx.x & ((1u << CL) - 1u)) : 0u;
@@ -639,7 +648,7 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
       const unsigned gi = g0 + j * gstride;
       const int o = j * T + tid;
       if (kStageP && !first) cp_async_pair<R>(sp + 4 * o, part + 2 * (size_t)gi);
-      if (!uni) cp_async_pair<R>(ss + 4 * o, psi + 2 * (size_t)gi);
+      if (!uni && !DR) cp_async_pair<R>(ss + 4 * o, psi + 2 * (size_t)gi);
       cp_async8(sd + o, hp + gi);
     }
 #pragma unroll
@@ -648,6 +657,17 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
       if constexpr (!kStageP) pv[j] = first ? pzero<R>() : pld(part + 2 * (size_t)(g0 + j * gstride));
     }
   }
+  // DR: psi of this thread's pairs straight into registers; issued once b_r
+  // is formed (when P_r's registers are free), before the barrier and the
+  // exchange-tile store that cover part of its latency.
+  Pair<R> psv[DR ? RP : 1];
+  auto load_direct = [&]() {
+    if constexpr (DR) {
+#pragma unroll
+      for (int j = 0; j < RP; j++)
+        psv[j] = uni ? pzero<R>() : pld(psi + 2 * (size_t)(g0 + j * gstride));
+    }
+  };
   const double kap = W.kappa ? *W.kappa : 1.0;
   const R scale = (R)W.scale;
   const R gamma = (R)W.gamma;
@@ -657,9 +677,12 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   if (first) {
     const R cr = (R)((double)W.coef[r] * kap);
     if (!bulk) cp_async_wait_all();
+    load_direct();
 #pragma unroll
     for (int j = 0; j < RP; j++) {
-      const V4<R> pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * (j * T + tid));
+      V4<R> pv;
+      if constexpr (DR) pv = uni ? V4<R>{psi0, 0, psi0, 0} : to4(psv[DR ? j : 0]);
+      else pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * (j * T + tid));
       vb[j] = from4(cpsi4<R>(cr, r & 1, pv));
     }
   } else {
@@ -692,6 +715,7 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
       vb[j] = from4(V4<R>{fma(-ag, acc.x, pr.x), fma(-ag, acc.y, pr.y),
                           fma(-ag, acc.z, pr.z), fma(-ag, acc.w, pr.w)});
     }
+    if (r > 0) load_direct();
   }
 #pragma unroll
   for (int j = 0; j < RP; j++) pst(bout + 2 * (size_t)(g0 + j * gstride), vb[j]);
@@ -717,9 +741,11 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
     return;
   }
   // Start P_{r-1} = c psi + a (D b_r - gamma X_Z b_r) - b_{r+1} over all tile axes.
-  tile_barrier<CL>();  // every reader of sx (this CTA and its peers) is done
+  // (DR: b_r goes to its own exchange tile, so no reader of b_{r+1}'s tile
+  // has to be waited for.)
+  if constexpr (!DR) tile_barrier<CL>();  // every reader of sx (this CTA and its peers) is done
 #pragma unroll
-  for (int j = 0; j < RP; j++) pst(sx + 4 * (tid | (j << LOGT)), vb[j]);
+  for (int j = 0; j < RP; j++) pst(sx2 + 4 * (tid | (j << LOGT)), vb[j]);
   tile_barrier<CL>();
   const int rm = r - 1;
   const R am = rm == 0 ? a_fin : a_mid;
@@ -727,11 +753,13 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
 #pragma unroll
   for (int j = 0; j < RP; j++) {
     const Remote rv = cluster_load(j, 0, LL);
-    PartnerSum<R, COMP> accp = axis_sum<R, LT, LOGT, RP, LS, COMP>(vb, j, sx, 0, LT, tid);
+    PartnerSum<R, COMP> accp = axis_sum<R, LT, LOGT, RP, LS, COMP>(vb, j, sx2, 0, LT, tid);
     cluster_add(accp, rv, 0, LL);
     const V4<R> acc = to4(accp.value());
     const int o = j * T + tid;
-    const V4<R> pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * o);
+    V4<R> pv;
+    if constexpr (DR) pv = uni ? V4<R>{psi0, 0, psi0, 0} : to4(psv[DR ? j : 0]);
+    else pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * o);
     const float2 d = sd[o];
     const V4<R> b = to4(vb[j]);
     const V4<R> b1 = to4(va[j]);
@@ -1038,25 +1066,31 @@ PassGeomHost pass_geom(int precision, int n, int lmax, int threads, int lane_sme
   g.threads = (threads == 256 && L == cap && g.C == 0) ? 256 : 0;
   // Lane axes through shared memory: FP32 single-CTA tiles of 2^12 or 2^13.
   g.lane_smem = (lane_smem && precision == 0 && g.C == 0 && L >= cap) ? 1 : 0;
-  // Bulk-copy staging: FP32 single-CTA tiles.
-  g.tma = (tma && precision == 0 && g.C == 0) ? 1 : 0;
+  // Staging: bulk copies (1) on FP32 single-CTA tiles; psi straight into
+  // registers (2) on FP32 single-CTA tiles with 8 pairs per thread (the
+  // 256-thread 2^12 tile or the 2^13 tile) and shuffled lane axes.
+  g.tma = 0;
+  if (tma == 1 && precision == 0 && g.C == 0) g.tma = 1;
+  if (tma == 2 && precision == 0 && g.C == 0 && !g.lane_smem &&
+      ((L == cap && g.threads == 256) || L == 13))
+    g.tma = 2;
   return g;
 }
 
 namespace {
 template <typename R, int LT, int CL, int TB = kPassThreads, bool LS = false, bool TMA = false,
-          bool COMP = false>
+          bool COMP = false, bool DR = false>
 cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
   using S = PassShape<LT, TB>;
   const size_t smem = S::template smem<R, S::kStageP || TMA>();
   {
-    cudaError_t e = ensure_smem_optin((const void*)pass_kernel<R, LT, CL, TB, LS, TMA, COMP>,
+    cudaError_t e = ensure_smem_optin((const void*)pass_kernel<R, LT, CL, TB, LS, TMA, COMP, DR>,
                                       smem, CL > 3);
     if (e != cudaSuccess) return e;
   }
   const dim3 grid((unsigned)((size_t)1 << (p.n - LT)), p.count);
   if constexpr (CL == 0) {
-    pass_kernel<R, LT, 0, TB, LS, TMA, COMP><<<grid, S::kThreads, smem, stream>>>(p);
+    pass_kernel<R, LT, 0, TB, LS, TMA, COMP, DR><<<grid, S::kThreads, smem, stream>>>(p);
     return cudaGetLastError();
   } else {
     cudaLaunchConfig_t cfg = {};
@@ -1077,8 +1111,17 @@ cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
 
 // FP32 single-CTA tile variants: threads (512/256), lane axes (shuffles or
 // shared memory) and staging (cp.async or bulk copies).
+// p.tma: 0 cp.async staging, 1 bulk copies, 2 psi straight into registers
+// (shapes with 8 pairs per thread, shuffled lane axes).
 template <typename R, int LT, int TB>
 cudaError_t launch_pass_variant(const PassParams& p, cudaStream_t stream) {
+  if (p.tma == 2) {
+    if constexpr (!PassShape<LT, TB>::kStageP) {
+      if (p.lane_smem) return cudaErrorInvalidValue;
+      return launch_pass_lt<R, LT, 0, TB, false, false, false, true>(p, stream);
+    }
+    return cudaErrorInvalidValue;
+  }
   if (p.lane_smem) {
     if (p.tma) return launch_pass_lt<R, LT, 0, TB, true, true>(p, stream);
     return launch_pass_lt<R, LT, 0, TB, true, false>(p, stream);
@@ -1130,6 +1173,7 @@ cudaError_t launch_pass_t(const PassParams& p, cudaStream_t stream) {
   if (p.threads == 256 && p.L != cap) return cudaErrorInvalidValue;
   if (p.lane_smem && (sizeof(R) != 4 || p.C != 0 || p.L < cap)) return cudaErrorInvalidValue;
   if (p.tma && (sizeof(R) != 4 || p.C != 0)) return cudaErrorInvalidValue;
+  if (p.tma == 2 && p.L < cap) return cudaErrorInvalidValue;  // 8 pairs per thread only
   if constexpr (sizeof(R) == 4) {
     if (p.tma && p.L < cap) {
       switch (p.L) {

@@ -642,3 +642,21 @@ def test_stage2_tensor_core_gemm_matches_simt(ctx, orc, mqw, monkeypatch, n, m, 
     np.testing.assert_allclose(tc, simt, rtol=5e-6, atol=1e-9)
     r64 = ctx.run_problems(n, m, raw, samples=samples, precision="fp64", graph=0)
     assert abs(float(np.mean(tc)) - r64["p"][0]) <= 1e-5
+
+
+@pytest.mark.parametrize("n,tile,threads", [(19, 12, 256), (20, 12, 256), (22, 13, 512),
+                                            (24, 13, 512)])
+def test_direct_register_staging_matches_cp_async(ctx, orc, n, tile, threads):
+    """psi loaded straight into registers with a second exchange tile (tma=2,
+    shapes with 8 pairs per thread: the 256-thread 2^12 tile and the 2^13
+    tile) against cp.async staging: the same arithmetic, so bit-identical
+    per-sample values, including n = 24 (2^13 tiles, two axes read from
+    global memory), and within FP32 of FP64."""
+    raw = orc.sk_instances(n, 1, 2700 + n)
+    kw = dict(samples=3, graph=0, group=1, lanes=1, tile_log=tile, threads=threads, lane_smem=-1,
+              stage1_basis=0)
+    r_d = ctx.run_problems(n, 3, raw, precision="fp32", tma=2, **kw)
+    r_c = ctx.run_problems(n, 3, raw, precision="fp32", tma=-1, **kw)
+    assert r_d["p"][0] == r_c["p"][0]
+    r64 = ctx.run_problems(n, 3, raw, precision="fp64", samples=3, graph=0)
+    assert abs(r_d["p"][0] - r64["p"][0]) <= 1e-5
