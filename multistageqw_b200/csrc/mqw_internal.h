@@ -306,6 +306,11 @@ int s2_tc_kp(const S2Layout& lay);
 size_t s2_tc_coef_floats(int walks, const S2Layout& lay);
 cudaError_t launch_s2_gemm_tc(const S2CoefParams& cp, float* Ct, const S2GemmParams& g,
                               unsigned* err, cudaStream_t stream);
+// The GEMM alone, on given K-major hi/lo coefficient copies Ct ([4 Np][Kp]:
+// class-0 hi, class-0 lo, class-1 hi, class-1 lo rows of Np walks each).
+cudaError_t launch_s2_gemm_tc_raw(const float* Y, const int rows[2], const float* Ct, int Np,
+                                  int Kp, int n, int walks, int out_walks, float* out,
+                                  unsigned* err, cudaStream_t stream);
 cudaError_t launch_unpack(const UnpackParams& p, cudaStream_t stream);
 
 // Finalisation after a stage: kappa[g] = 1/sqrt(sum of partials); when

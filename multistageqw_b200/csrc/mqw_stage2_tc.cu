@@ -21,8 +21,11 @@
 //
 // Data movement: Y tiles (MN-major: 32 amplitudes x 32 pairs per box, eight
 // boxes per chunk) and the C tiles (K-major: 32 pairs x N walks) arrive by
-// TMA (cp.async.bulk.tensor, 128-byte swizzle, no multicast) on an mbarrier
-// per pipeline stage. Warp roles per CTA (192 threads):
+// TMA (cp.async.bulk.tensor, no multicast) on an mbarrier per pipeline
+// stage. An MN-major tf32 operand has one shared-memory layout the MMA
+// accepts: 128-byte rows along M with the swizzle applied to 32-byte units
+// (atoms of 4 rows; the TMA's 128B_ATOM_32B swizzle writes it); the K-major
+// C tiles use the ordinary 128-byte swizzle. Warp roles per CTA (192 threads):
 //   warp 0      TMA producer (one thread);
 //   warp 1      TMEM allocator and MMA issuer (one thread issues tcgen05.mma);
 //   warps 2-5   split the Y tile into hi (in place) and lo, then, after the
@@ -128,15 +131,16 @@ __device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map
       : "memory");
 }
 
-// UMMA shared-memory descriptor, 128-byte swizzle (sm_100 version bits).
-// lbo/sbo in bytes.
-__device__ __forceinline__ unsigned long long umma_desc(unsigned addr, unsigned lbo, unsigned sbo) {
+// UMMA shared-memory descriptor (sm_100 version bits); lbo/sbo in bytes;
+// layout 2 = 128-byte swizzle, 1 = 128-byte swizzle with 32-byte atoms.
+__device__ __forceinline__ unsigned long long umma_desc(unsigned addr, unsigned lbo, unsigned sbo,
+                                                        unsigned layout) {
   unsigned long long d = 0;
   d |= (unsigned long long)((addr >> 4) & 0x3FFFu);
   d |= (unsigned long long)((lbo >> 4) & 0x3FFFu) << 16;
   d |= (unsigned long long)((sbo >> 4) & 0x3FFFu) << 32;
   d |= 1ull << 46;  // descriptor version (sm_100)
-  d |= 2ull << 61;  // layout: 128-byte swizzle
+  d |= (unsigned long long)layout << 61;
   return d;
 }
 // Instruction descriptor: D f32, A and B tf32, A MN-major, B K-major,
@@ -254,12 +258,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         for (int kk = 0; kk < kTcBK / 8; kk++) {
 #pragma unroll
           for (int half = 0; half < 2; half++) {
+            // A (MN-major, 32-byte-atom swizzle): blocks of 32 amplitudes
+            // 4 KB apart (LBO), groups of 4 pair rows 512 B apart (SBO); the
+            // MMA's 8 pairs start 1 KB further per step. B (K-major, 128-byte
+            // swizzle): groups of 8 walk rows 1 KB apart (SBO); the MMA's 8
+            // pairs start 32 B further per step.
             const unsigned long long ahi =
-                umma_desc(a_tile(s) + half * (kTcATile / 2) + kk * 1024u, 4096u, 1024u);
+                umma_desc(a_tile(s) + half * (kTcATile / 2) + kk * 1024u, 4096u, 512u, 1u);
             const unsigned long long alo =
-                umma_desc(alo_tile(s) + half * (kTcATile / 2) + kk * 1024u, 4096u, 1024u);
-            const unsigned long long bhi = umma_desc(bhi_tile(s) + kk * 32u, 16u, 1024u);
-            const unsigned long long blo = umma_desc(blo_tile(s) + kk * 32u, 16u, 1024u);
+                umma_desc(alo_tile(s) + half * (kTcATile / 2) + kk * 1024u, 4096u, 512u, 1u);
+            const unsigned long long bhi = umma_desc(bhi_tile(s) + kk * 32u, 16u, 1024u, 2u);
+            const unsigned long long blo = umma_desc(blo_tile(s) + kk * 32u, 16u, 1024u, 2u);
             const unsigned d = tmem + (unsigned)(half * kTcM);
             umma_tf32(d, ahi, bhi, idesc, c > 0 || kk > 0);
             umma_tf32(d, ahi, blo, idesc, true);
@@ -380,10 +389,11 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// 2-D float32 tensor map, 128-byte swizzle: dims {inner, outer}, row pitch
-// in bytes, box {bx, by}.
+// 2-D float32 tensor map: dims {inner, outer}, row pitch in bytes, box
+// {bx, by}, the given swizzle.
 bool make_map(CUtensorMap* m, const float* base, unsigned long long inner,
-              unsigned long long outer, unsigned long long pitch, unsigned bx, unsigned by) {
+              unsigned long long outer, unsigned long long pitch, unsigned bx, unsigned by,
+              CUtensorMapSwizzle swz) {
   PFN_cuTensorMapEncodeTiled_v12000 enc = encode_fn();
   if (!enc) return false;
   const cuuint64_t dims[2] = {inner, outer};
@@ -391,7 +401,7 @@ bool make_map(CUtensorMap* m, const float* base, unsigned long long inner,
   const cuuint32_t box[2] = {bx, by};
   const cuuint32_t es[2] = {1, 1};
   return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box,
-             es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+             es, CU_TENSOR_MAP_INTERLEAVE_NONE, swz,
              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
          CUDA_SUCCESS;
 }
@@ -410,39 +420,31 @@ size_t s2_tc_coef_floats(int walks, const S2Layout& lay) {
   return (size_t)4 * s2_tc_np(walks) * s2_tc_kp(lay);
 }
 
-cudaError_t launch_s2_gemm_tc(const S2CoefParams& cp, float* Ct, const S2GemmParams& g,
-                              unsigned* err, cudaStream_t stream) {
-  const int Np = s2_tc_np(g.walks);
-  const int Kp = s2_tc_kp(cp.lay);
-  if (g.n < 8 || g.n > kMaxN || !g.Y || !g.out || !Ct || g.walks < 1 || Np > kTcMaxN ||
-      g.out_walks < g.walks || g.rows[0] < 1 || g.rows[1] < 1 || cp.walks != g.walks ||
-      cp.lay.rows(0) != g.rows[0] || cp.lay.rows(1) != g.rows[1] || !encode_fn())
+cudaError_t launch_s2_gemm_tc_raw(const float* Y, const int rows[2], const float* Ct, int Np,
+                                  int Kp, int n, int walks, int out_walks, float* out,
+                                  unsigned* err, cudaStream_t stream) {
+  if (n < 8 || n > kMaxN || !Y || !out || !Ct || walks < 1 || Np != s2_tc_np(walks) ||
+      Np > kTcMaxN || out_walks < walks || rows[0] < 1 || rows[1] < 1 || Kp % kTcBK != 0 ||
+      Kp < rows[0] || Kp < rows[1] || !encode_fn())
     return cudaErrorInvalidValue;
-  // Coefficients: K-major hi/lo copies.
-  {
-    const size_t total = (size_t)2 * Np * Kp;
-    const size_t want = (total + 255) / 256;
-    s2_coef_tc_kernel<<<(unsigned)(want < 8192 ? want : 8192), 256, 0, stream>>>(cp, Ct, Np, Kp);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-  }
-  const unsigned long long N = 1ull << g.n;
+  const unsigned long long N = 1ull << n;
   CUtensorMap mY0, mY1, mC;
-  if (!make_map(&mY0, g.Y, N, (unsigned long long)g.rows[0], N * 4, 32, kTcBK) ||
-      !make_map(&mY1, g.Y + (size_t)g.rows[0] * N, N, (unsigned long long)g.rows[1], N * 4, 32,
-                kTcBK) ||
+  if (!make_map(&mY0, Y, N, (unsigned long long)rows[0], N * 4, 32, kTcBK,
+                CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B) ||
+      !make_map(&mY1, Y + (size_t)rows[0] * N, N, (unsigned long long)rows[1], N * 4, 32, kTcBK,
+                CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B) ||
       !make_map(&mC, Ct, (unsigned long long)Kp, 4ull * Np, (unsigned long long)Kp * 4, kTcBK,
-                (unsigned)Np))
+                (unsigned)Np, CU_TENSOR_MAP_SWIZZLE_128B))
     return cudaErrorInvalidValue;
   TcArgs a{};
-  a.out = g.out;
+  a.out = out;
   a.err = err;
-  a.n = g.n;
-  a.walks = g.walks;
-  a.out_walks = g.out_walks;
+  a.n = n;
+  a.walks = walks;
+  a.out_walks = out_walks;
   a.Np = Np;
   for (int h = 0; h < 2; h++) {
-    a.chunks[h] = (g.rows[h] + kTcBK - 1) / kTcBK;
+    a.chunks[h] = (rows[h] + kTcBK - 1) / kTcBK;
     a.crow[h] = 2 * h * Np;
   }
   {
@@ -460,6 +462,25 @@ cudaError_t launch_s2_gemm_tc(const S2CoefParams& cp, float* Ct, const S2GemmPar
   const dim3 grid((unsigned)(N / kTcAmps), 2);
   s2_gemm_tc_kernel<<<grid, kTcThreads, kTcSmem, stream>>>(mY0, mY1, mC, a);
   return cudaGetLastError();
+}
+
+cudaError_t launch_s2_gemm_tc(const S2CoefParams& cp, float* Ct, const S2GemmParams& g,
+                              unsigned* err, cudaStream_t stream) {
+  const int Np = s2_tc_np(g.walks);
+  const int Kp = s2_tc_kp(cp.lay);
+  if (g.walks < 1 || Np > kTcMaxN || !Ct || cp.walks != g.walks ||
+      cp.lay.rows(0) != g.rows[0] || cp.lay.rows(1) != g.rows[1])
+    return cudaErrorInvalidValue;
+  // Coefficients: K-major hi/lo copies.
+  {
+    const size_t total = (size_t)2 * Np * Kp;
+    const size_t want = (total + 255) / 256;
+    s2_coef_tc_kernel<<<(unsigned)(want < 8192 ? want : 8192), 256, 0, stream>>>(cp, Ct, Np, Kp);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return launch_s2_gemm_tc_raw(g.Y, g.rows, Ct, Np, Kp, g.n, g.walks, g.out_walks, g.out, err,
+                               stream);
 }
 
 }  // namespace mqw

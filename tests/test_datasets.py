@@ -57,7 +57,7 @@ def test_readme_example_adam_sk10n_through_the_drop_in(mqw, tmp_path):
     """`MultiQW 10 2 <file>` on the first 200 AdamData SK_10n instances: one
     float32 per instance appended to output_10_2, each within 1e-5 of the
     reference pipeline run with the reference's own step; stdout's total_t
-    per instance equals the reference schedule's."""
+    per instance is the reference schedule's, as printed."""
     name = "adam_sk10n_first200.bin"
     run = EXPECT["files"][name]["runs"]["2"]
     f = tmp_path / "SK_10n"
@@ -70,8 +70,9 @@ def test_readme_example_adam_sk10n_through_the_drop_in(mqw, tmp_path):
     assert np.abs(out.astype(np.float64) - np.array(run["p_ref_step_f32"])).max() <= 1e-5
     lines = r.stdout.strip().splitlines()
     assert len(lines) == 200
-    tt = [float(x.split()[0]) for x in lines]
-    assert tt == pytest.approx(run["total_t"], rel=1e-6)
+    # stdout prints total_t with "%g" (MultiQW.cpp:423 streams a float with
+    # six significant digits): the same text as the reference's value
+    assert [x.split()[0] for x in lines] == ["%g" % t for t in run["total_t"]]
 
 
 @pytest.mark.gpu
