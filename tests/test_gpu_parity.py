@@ -660,3 +660,22 @@ def test_direct_register_staging_matches_cp_async(ctx, orc, n, tile, threads):
     assert r_d["p"][0] == r_c["p"][0]
     r64 = ctx.run_problems(n, 3, raw, precision="fp64", samples=3, graph=0)
     assert abs(r_d["p"][0] - r64["p"][0]) <= 1e-5
+
+
+def test_each_device_gets_its_own_shared_memory_opt_in(mqw, orc):
+    """Kernels above 48 KB of shared memory are opted in per device: after
+    FP32 and FP64 runs on device 0 the same runs on device 1 (a second
+    context in the same process) must launch too and agree. Needs two GPUs;
+    skipped otherwise."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    n = 16
+    raw = orc.sk_instances(n, 1, 77)
+    out = []
+    for dev in (0, 1):
+        c = mqw.Context(dev)
+        out.append([c.run_problems(n, 3, raw, samples=4, precision=p)["p"][0]
+                    for p in ("fp32", "fp64")])
+        c.close()
+    assert out[0] == out[1]
