@@ -87,6 +87,19 @@ float inv_norm_upper(float pf) {
   return (float)x;
 }
 
+// The inverse normal the schedule uses: this restatement's (default) or an
+// external one with the reference's my_normcdfinvf signature (float ->
+// float) — the reference's own, from the partial build in oracle/_ref — so
+// that a whole run can be driven by the reference's schedule arithmetic.
+typedef float (*InvNormFn)(float);
+InvNormFn g_inv_norm = nullptr;
+// Not inlined: the schedule then sees an opaque call either way, as the
+// CUDA path's host code does (its inverse normal lives in another
+// translation unit), so the compiler fuses the same multiply-add around it.
+__attribute__((noinline)) float sched_inv_norm(float p) {
+  return g_inv_norm ? g_inv_norm(p) : inv_norm_upper(p);
+}
+
 struct DiagInfo {
   double e0, emax, mid;
   float e_abs;
@@ -148,10 +161,10 @@ void schedule(int n, int m, const float* J, const float* h, float* gammas,
               float* short_ts, float* times /* m * kSamples */,
               float* total_t_out) {
   const unsigned N = 1u << n;
-  float b = inv_norm_upper(1 / (float)N);
   float e_m = 0.577215664901532860;
   float e = 2.718281828459045;
-  float a = (1 - e_m) * b + e_m * inv_norm_upper(1 / (e * N));
+  float b = sched_inv_norm(1 / (float)N);
+  float a = (1 - e_m) * b + e_m * sched_inv_norm(1 / (e * N));
   float JJ = 0.0f, hh = 0.0f;
   for (int i = 0; i < n * n; i++) JJ += J[i] * J[i];
   for (int i = 0; i < n; i++) hh += h[i] * h[i];
@@ -360,6 +373,10 @@ struct orc_diag_info {
 int orc_version() { return 1; }
 
 float orc_inv_norm_upper(float p) { return inv_norm_upper(p); }
+
+// Selects the schedule's inverse normal: fn (float -> float, the
+// reference's my_normcdfinvf signature), or this restatement's when null.
+void orc_set_inv_norm(void* fn) { g_inv_norm = reinterpret_cast<InvNormFn>(fn); }
 
 void orc_load_instance(int n, const double* raw, float* J, float* h) {
   load_instance(n, raw, J, h);

@@ -77,6 +77,8 @@ def lib():
         L = ctypes.CDLL(path)
         L.orc_inv_norm_upper.restype = _c_float
         L.orc_inv_norm_upper.argtypes = [_c_float]
+        L.orc_set_inv_norm.argtypes = [ctypes.c_void_p]
+        L.orc_set_inv_norm.restype = None
         L.orc_load_instance.argtypes = [_c_int, _P(_c_double), _P(_c_float), _P(_c_float)]
         L.orc_energies_ref.argtypes = [_c_int, _P(_c_double), _P(_c_double), _P(_c_float), ctypes.c_void_p]
         L.orc_energies_exact.argtypes = [_c_int, _P(_c_double), _P(_c_double)]
@@ -124,6 +126,20 @@ def ref_lib():
         R.ref_log2_of_lsb.argtypes = [_c_int]
         _ref = R
     return _ref
+
+
+def use_reference_inv_norm(on: bool) -> None:
+    """Drive the oracle's schedule with the reference's own my_normcdfinvf
+    (MultiQW.cpp:83-86, from the partial build) instead of this
+    restatement's correctly rounded inverse normal (they differ by at most
+    1 ulp at the heuristic's inputs)."""
+    if on:
+        R = ref_lib()
+        if R is None:
+            raise RuntimeError("partial reference build not available")
+        lib().orc_set_inv_norm(ctypes.cast(R.ref_my_normcdfinvf, ctypes.c_void_p).value)
+    else:
+        lib().orc_set_inv_norm(None)
 
 
 def ref_step_ptr():

@@ -16,13 +16,16 @@ them unchanged):
   tim_sk10n_first100.bin    the first 100 instances of data/TimData/SK_10n
   tim_sk12n_first100.bin    the first 100 instances of data/TimData/SK_12n
   dataset_expect.json       per file and (n, m): per-instance ground-state
-                            probability of the reference pipeline with the
+                            probability of a reference-driven run — the
                             reference's own FP32 Clenshaw_step (MultiQW.cpp:
-                            88-173, the partial build in oracle/_ref) and of
-                            the oracle in FP64, E_loc, total_t, the summed
-                            Chebyshev degree and the gap between the two
-                            lowest energies (reference arithmetic), plus the
-                            SHA-256 of each fixture file.
+                            88-173) and its own my_normcdfinvf
+                            (MultiQW.cpp:83-86) in the schedule, both from the
+                            partial build in oracle/_ref — with its total_t;
+                            the same with this project's inverse normal (the
+                            one the CUDA path uses) in FP32 and in FP64; E_loc,
+                            the summed Chebyshev degree and the gap between
+                            the two lowest energies (reference arithmetic),
+                            plus the SHA-256 of each fixture file.
 """
 from __future__ import annotations
 
@@ -75,18 +78,24 @@ def main() -> None:
                  "sha256": hashlib.sha256(data).hexdigest(),
                  "gaps": [two_lowest_gap(n, raw[i]) for i in range(count)], "runs": {}}
         for m in m_values:
+            O.use_reference_inv_norm(True)
+            rr = O.run_problems(n, m, raw, count, O.SAMPLES, "f32", use_ref_step=True)
+            O.use_reference_inv_norm(False)
             r32 = O.run_problems(n, m, raw, count, O.SAMPLES, "f32", use_ref_step=True)
             r64 = O.run_problems(n, m, raw, count, O.SAMPLES, "f64")
-            assert np.array_equal(r32["e_loc"], r64["e_loc"])
+            assert np.array_equal(rr["e_loc"], r64["e_loc"])
             entry["runs"][str(m)] = {
+                "p_reference_driven": rr["p"].tolist(),
+                "total_t_reference_driven": rr["total_t"].astype(float).tolist(),
                 "p_ref_step_f32": r32["p"].tolist(),
                 "p_oracle_f64": r64["p"].tolist(),
                 "e_loc": r32["e_loc"].astype(int).tolist(),
                 "total_t": r32["total_t"].astype(float).tolist(),
                 "terms": r32["terms"].astype(int).tolist(),
             }
-            print(f"{fixture} m={m}: max |P_ref - P_f64| = "
-                  f"{np.abs(r32['p'] - r64['p']).max():.2e}")
+            print(f"{fixture} m={m}: max |P_refdriven - P_f64| = "
+                  f"{np.abs(rr['p'] - r64['p']).max():.2e}, "
+                  f"max |P_refdriven - P_own_invnorm| = {np.abs(rr['p'] - r32['p']).max():.2e}")
         out["files"][fixture] = entry
     with open(os.path.join(HERE, "dataset_expect.json"), "w") as f:
         json.dump(out, f, indent=0)
