@@ -761,13 +761,26 @@ struct BasisLayout {
 
 // State slots of one unit-coefficient pass chain: the partial P, the
 // recurrence vector b (b[1] only when axes are read from global memory) and
-// the start vector (not read when `uniform`: the uniform state).
+// the start vector (not read when `uniform`: the uniform state), complex;
+// `start_real` is the same start vector as a real vector, for the real
+// chain kernel (nullptr when uniform).
 struct ChainSlots {
   void* part;
   void* b[2];
   const void* start;
   bool uniform;
+  const float* start_real;
 };
+
+// Whether a plan's chains run on the real chain kernel (real_pass_kernel):
+// FP32, single-CTA tiles; MQW_REAL_CHAINS=0 keeps them on the complex pass
+// kernel (the same results: the real kernel reproduces the real parts bit
+// for bit).
+bool use_real_chains(const mqw_plan& P, const PassGeomHost& geo) {
+  if (P.precision != 0 || geo.C != 0) return false;
+  const char* e = getenv("MQW_REAL_CHAINS");
+  return !(e && atoi(e) == 0);
+}
 
 // One unit-coefficient pass chain: w_j = U_j(H~) v, j < K, for the operator of
 // stage `stage` of the instance of walk w0 and the start vector v of `S`,
@@ -784,6 +797,37 @@ mqw_status issue_chain(mqw_plan& P, const ResidentWalk& w0, int stage, int K,
   const size_t N = (size_t)1 << w0.n;
   const int R = K + (K & 1);
   const int job = w0.stage_desc_off + stage;
+  if (use_real_chains(P, geo)) {
+    // Every vector of the chain is real: the real chain kernel, writing
+    // each b_r straight into its basis slot and reading b_{r+1} back from
+    // the previous one (no complex b slot, no separate real copy).
+    for (int j = 0; j < K; j++) {
+      RealChainParams rp{};
+      rp.n = w0.n;
+      rp.L = geo.L;
+      rp.a = geo.a;
+      rp.tiling = ((R - j) & 1) ? 2 : 1;
+      rp.first = j == 0;
+      rp.bin = j > 0 ? out_of(j - 1) : nullptr;
+      rp.bout = out_of(j);
+      rp.part = static_cast<float*>(S.part);
+      rp.start = S.start_real;
+      rp.start_uniform = S.uniform ? 1 : 0;
+      rp.psi0 = (float)(1.0 / std::sqrt((double)N));
+      rp.hp = P.d_hp.as<float>() + w0.hp_off;
+      rp.gamma = P.jobs[job].gamma;
+      rp.scale = P.onenorm[job];
+      CK(launch_real_pass(rp, stream));
+      if (P.counting) {
+        P.stats.launches++;
+        P.stats.term_launches++;
+        // read b_{r+1}, P, D and write b_r, P: 20 B per amplitude (the
+        // first pass reads the start vector instead of b_{r+1} and P)
+        P.stats.aux_bytes += (double)N * 20.0;
+      }
+    }
+    return MQW_OK;
+  }
   const float* unit = P.d_unit.as<float>() + (P.unit_len - 1 - R);
   for (int j = 0; j < K; j++) {
     PassParams pp{};
@@ -840,12 +884,18 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
                        cudaStream_t stream) {
   const size_t N = (size_t)1 << w0.n;
   const bool from_eloc = stage > 0;
+  const bool real_chain = use_real_chains(P, geo);
   if (from_eloc) {
     mqw_ctx* ctx = P.ctx;
-    CK(launch_unit_eloc(B.slot(3), w0.n, P.d_diag.as<DiagOut>() + w0.inst, stream));
+    if (real_chain)
+      CK(launch_unit_eloc_real(static_cast<float*>(B.slot(3)), w0.n,
+                               P.d_diag.as<DiagOut>() + w0.inst, stream));
+    else
+      CK(launch_unit_eloc(B.slot(3), w0.n, P.d_diag.as<DiagOut>() + w0.inst, stream));
     if (P.counting) P.stats.launches++;
   }
-  const ChainSlots S{B.slot(0), {B.slot(1), B.slot(2)}, B.slot(3), !from_eloc};
+  const ChainSlots S{B.slot(0), {B.slot(1), B.slot(2)}, B.slot(3), !from_eloc,
+                     from_eloc ? static_cast<const float*>(B.slot(3)) : nullptr};
   return issue_chain(P, w0, stage, Kb, S, geo, [&](int j) { return real + (size_t)j * N; },
                      stream);
 }
@@ -893,11 +943,13 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
     char* base = builder ? ctx->s2chain.as<char>() + (size_t)lane * 4 * N * 8
                          : ctx->state.as<char>() + (size_t)lane * gmax * slots * N * 8;
     auto slot = [&](int k) -> void* { return base + (size_t)k * N * 8; };
-    const ChainSlots S{slot(0), {slot(1), slot(2)}, slot(slots - 1), false};
-    CK(launch_real_to_complex(slot(slots - 1), basis + (size_t)j * N, n, st));
-    if (P.counting) {
-      P.stats.launches++;
-      P.stats.aux_bytes += (double)N * 12.0;
+    const ChainSlots S{slot(0), {slot(1), slot(2)}, slot(slots - 1), false, basis + (size_t)j * N};
+    if (!use_real_chains(P, geo)) {  // the complex kernel starts from a complex copy
+      CK(launch_real_to_complex(slot(slots - 1), basis + (size_t)j * N, n, st));
+      if (P.counting) {
+        P.stats.launches++;
+        P.stats.aux_bytes += (double)N * 12.0;
+      }
     }
     auto out_of = [&](int k) {
       const int h = (j + k) & 1;

@@ -225,6 +225,36 @@ struct ProjectParams {
 cudaError_t launch_project(const ProjectParams& p, cudaStream_t stream);
 // psi = the unit vector at E_loc of instance `inst` (complex FP32, 2^n).
 cudaError_t launch_unit_eloc(void* psi, int n, const DiagOut* diag, cudaStream_t stream);
+
+// Real unit-coefficient chains (FP32). The shared-basis chains — the
+// stage-1 basis from the uniform state, the last-stage basis from
+// e_{E_loc}, the stage-2 product basis from the real stage-1 basis vectors —
+// apply a real operator to a real start vector with real unit coefficients,
+// so every vector of the recurrence is real. real_pass_kernel runs one pass
+// of such a chain on real vectors (4 bytes per amplitude instead of a
+// complex 8) with the same tilings, thread layout and partner-sum order as
+// pass_kernel, so its outputs equal the real parts of the complex chain's
+// bit for bit. Pass j of a chain with top index R (r = R - j >= 1, a =
+// 2/scale): j == 0 writes b_R = v to bout and starts P_{R-1} = a (D v -
+// gamma X_Z v); j > 0 finishes b_r = P_r - a gamma X_F b_{r+1} (b_{r+1} in
+// bin, the previous pass's bout), writes it to bout and starts P_{r-1} =
+// a (D b_r - gamma X_Z b_r) - b_{r+1}. Single-CTA tiles (C = 0) only.
+struct RealChainParams {
+  int n, L, a;
+  int tiling;          // 1 or 2 (odd r: 2)
+  int first;           // j == 0
+  const float* bin;    // b_{r+1} (j > 0)
+  float* bout;         // b_r, written (the basis vector itself)
+  float* part;         // P, real, in place
+  const float* start;  // v (j == 0; unused when start_uniform)
+  int start_uniform;   // v is the uniform state psi0
+  float psi0;
+  const float* hp;
+  float gamma, scale;
+};
+cudaError_t launch_real_pass(const RealChainParams& p, cudaStream_t stream);
+// v = e_{E_loc} as a real vector of 2^n floats.
+cudaError_t launch_unit_eloc_real(float* v, int n, const DiagOut* diag, cudaStream_t stream);
 cudaError_t launch_combine(int precision, const CombineParams& p,
                            cudaStream_t stream);
 

@@ -941,6 +941,157 @@ __global__ void mean_kernel(const double* p_sample, const int* p_off,
   p_mean[i] = s / c;
 }
 
+// ---------------------------------------------------------------------------
+// Real unit-coefficient chains (see RealChainParams): pass_kernel's tilings,
+// thread layout and partner-sum order on real vectors. A register "pair" is
+// two neighbouring real amplitudes packed in 64 bits (summed with
+// add.rn.f32x2, exchanged with one 64-bit shuffle); the exchange tiles hold
+// 2^LT floats. 256 threads, P in registers, D staged by cp.async, two
+// exchange tiles (b_{r+1}'s and b_r's) so that no barrier separates the
+// last read of one from the first write of the other.
+template <int LT> struct RealShape {
+  static constexpr int kPairs = 1 << (LT - 1);
+  static constexpr int kThreads = kPairs < 256 ? kPairs : 256;
+  static constexpr int kRP = kPairs / kThreads;
+  static constexpr int kLogT = kThreads >= 256 ? 8 : kThreads >= 128 ? 7 : kThreads >= 64 ? 6 : 5;
+  static constexpr size_t smem() { return (size_t)kPairs * (2 * 8 + 8); }
+};
+
+__device__ __forceinline__ unsigned long long rpair_swap(unsigned long long v) {
+  return (v >> 32) | (v << 32);
+}
+__device__ __forceinline__ void rpair_add(unsigned long long& acc, unsigned long long v) {
+  asm("add.rn.f32x2 %0, %0, %1;" : "+l"(acc) : "l"(v));
+}
+
+// Partner sum over tile axes [q0, q1) of register pair j (pass_kernel's
+// axis_sum on real pairs: the same axes in the same order).
+template <int LT, int LOGT, int RP>
+__device__ __forceinline__ unsigned long long real_axis_sum(const unsigned long long (&v)[RP],
+                                                            int j, const unsigned long long* sx,
+                                                            int q0, int q1, int tid) {
+  unsigned long long acc = 0ull;
+  if (q0 <= 0) rpair_add(acc, rpair_swap(v[j]));
+  const int pp = tid | (j << LOGT);
+#pragma unroll
+  for (int q = 1; q <= 5 && q < LT; q++)
+    if (q >= q0 && q < q1) rpair_add(acc, __shfl_xor_sync(0xffffffffu, v[j], 1 << (q - 1)));
+#pragma unroll
+  for (int q = 6; q <= LOGT && q < LT; q++)
+    if (q >= q0 && q < q1) rpair_add(acc, sx[pp ^ (1 << (q - 1))]);
+#pragma unroll
+  for (int k = 0; (1 << k) < RP; k++) {
+    const int q = LOGT + 1 + k;
+    if (q >= q0 && q < q1) rpair_add(acc, v[j ^ (1 << k)]);
+  }
+  return acc;
+}
+
+__device__ __forceinline__ float2 u2f(unsigned long long v) {
+  float2 f;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(f.x), "=f"(f.y) : "l"(v));
+  return f;
+}
+__device__ __forceinline__ unsigned long long f2u(float2 f) {
+  unsigned long long v;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(v) : "f"(f.x), "f"(f.y));
+  return v;
+}
+
+template <int LT>
+__global__ void __launch_bounds__(RealShape<LT>::kThreads) real_pass_kernel(RealChainParams p) {
+  using S = RealShape<LT>;
+  constexpr int RP = S::kRP, LOGT = S::kLogT, T = S::kThreads;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  unsigned long long* sx1 = reinterpret_cast<unsigned long long*>(smem_raw);  // b_{r+1}
+  unsigned long long* sx2 = sx1 + S::kPairs;                                  // b_r
+  float2* sd = reinterpret_cast<float2*>(sx2 + S::kPairs);                    // staged D
+  const int n = p.n, a = p.a, tid = threadIdx.x;
+  const int nu = n - (2 * LT - a) > 0 ? n - (2 * LT - a) : 0;
+  unsigned tile = blockIdx.x;
+  if (p.tiling == 2 && nu > 0) {
+    const int tb = n - LT;
+    tile = ((tile & ((1u << nu) - 1u)) << (tb - nu)) | (tile >> nu);
+  }
+  const unsigned pos0 = 2u * tid;
+  unsigned g0, gstride;
+  if (p.tiling == 1) {
+    g0 = (tile << LT) | pos0;
+    gstride = 1u << (LOGT + 1);
+  } else {
+    const unsigned amask = (1u << a) - 1u;
+    g0 = (pos0 & amask) | (tile << a) | ((pos0 >> a) << (n - LT + a));
+    gstride = 1u << (LOGT + 1 + n - LT);
+  }
+  const int fb0 = p.tiling == 1 ? a : max(2 * LT - n, a);
+  const int fb1 = p.tiling == 1 ? min(LT, n - LT + a) : LT;
+  const float* __restrict__ hp = p.hp;
+  const float* __restrict__ bin = p.bin;
+  float* __restrict__ part = p.part;
+#pragma unroll
+  for (int j = 0; j < RP; j++) cp_async8(sd + (j * T + tid), hp + g0 + j * gstride);
+  unsigned long long va[RP], vb[RP];
+  const float am = 2.0f / p.scale;
+  const float gamma = p.gamma;
+  if (p.first) {
+#pragma unroll
+    for (int j = 0; j < RP; j++) {
+      va[j] = 0ull;
+      vb[j] = p.start_uniform ? f2u(make_float2(p.psi0, p.psi0))
+                              : *reinterpret_cast<const unsigned long long*>(p.start + g0 + j * gstride);
+    }
+    cp_async_wait_all();
+  } else {
+    unsigned long long pv[RP];
+#pragma unroll
+    for (int j = 0; j < RP; j++) {
+      va[j] = *reinterpret_cast<const unsigned long long*>(bin + g0 + j * gstride);
+      pv[j] = *reinterpret_cast<const unsigned long long*>(part + g0 + j * gstride);
+    }
+#pragma unroll
+    for (int j = 0; j < RP; j++) sx1[tid | (j << LOGT)] = va[j];
+    __syncthreads();
+    cp_async_wait_all();
+    const float ag = am * gamma;
+#pragma unroll
+    for (int j = 0; j < RP; j++) {
+      unsigned long long acc = real_axis_sum<LT, LOGT, RP>(va, j, sx1, fb0, fb1, tid);
+      const unsigned gi = g0 + j * gstride;
+      for (int u0 = 0; u0 < nu; u0 += 4) {
+        unsigned long long gv[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (u0 + u < nu)
+            gv[u] = *reinterpret_cast<const unsigned long long*>(bin + (gi ^ (1u << (LT + u0 + u))));
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+          if (u0 + u < nu) rpair_add(acc, gv[u]);
+      }
+      const float2 s = u2f(acc), pr = u2f(pv[j]);
+      vb[j] = f2u(make_float2(fmaf(-ag, s.x, pr.x), fmaf(-ag, s.y, pr.y)));
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < RP; j++)
+    *reinterpret_cast<unsigned long long*>(p.bout + g0 + j * gstride) = vb[j];
+  // Start P_{r-1} = a (D b_r - gamma X_Z b_r) - b_{r+1} over all tile axes.
+#pragma unroll
+  for (int j = 0; j < RP; j++) sx2[tid | (j << LOGT)] = vb[j];
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < RP; j++) {
+    const float2 s = u2f(real_axis_sum<LT, LOGT, RP>(vb, j, sx2, 0, LT, tid));
+    const float2 d = sd[j * T + tid];
+    const float2 b = u2f(vb[j]), b1 = u2f(va[j]);
+    // pass_kernel's arithmetic with a zero coefficient: (0 - b1) + a (...)
+    const float2 out = make_float2(fmaf(am, fmaf(d.x, b.x, -gamma * s.x), 0.0f - b1.x),
+                                   fmaf(am, fmaf(d.y, b.y, -gamma * s.y), 0.0f - b1.y));
+    *reinterpret_cast<unsigned long long*>(part + g0 + j * gstride) = f2u(out);
+  }
+}
+
+__global__ void unit_eloc_real_kernel(float* v, const DiagOut* diag) { v[diag->e_loc] = 1.0f; }
+
 template <typename R>
 size_t resident_smem(int n) {
   const size_t N = (size_t)1 << n;
@@ -1270,6 +1421,44 @@ cudaError_t launch_unit_eloc(void* psi, int n, const DiagOut* diag, cudaStream_t
   if (e != cudaSuccess) return e;
   unit_eloc_kernel<<<1, 1, 0, stream>>>(reinterpret_cast<float2*>(psi), diag);
   return cudaGetLastError();
+}
+
+cudaError_t launch_unit_eloc_real(float* v, int n, const DiagOut* diag, cudaStream_t stream) {
+  if (n < 1 || n > kMaxN || !v || !diag) return cudaErrorInvalidValue;
+  cudaError_t e = cudaMemsetAsync(v, 0, ((size_t)1 << n) * sizeof(float), stream);
+  if (e != cudaSuccess) return e;
+  unit_eloc_real_kernel<<<1, 1, 0, stream>>>(v, diag);
+  return cudaGetLastError();
+}
+
+namespace {
+template <int LT>
+cudaError_t launch_real_lt(const RealChainParams& p, cudaStream_t stream) {
+  using S = RealShape<LT>;
+  const size_t smem = S::smem();
+  cudaError_t e = ensure_smem_optin((const void*)real_pass_kernel<LT>, smem, false);
+  if (e != cudaSuccess) return e;
+  real_pass_kernel<LT><<<(unsigned)((size_t)1 << (p.n - LT)), S::kThreads, smem, stream>>>(p);
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_real_pass(const RealChainParams& p, cudaStream_t stream) {
+  if (p.n < 6 || p.n > kMaxN || p.L < 6 || p.L > 13 || p.L > p.n || p.a != 4 ||
+      (p.tiling != 1 && p.tiling != 2) || !p.bout || !p.part || !p.hp || !(p.scale > 0.0f) ||
+      (p.first && !p.start_uniform && !p.start) || (!p.first && !p.bin) || p.bin == p.bout)
+    return cudaErrorInvalidValue;
+  switch (p.L) {
+    case 6: return launch_real_lt<6>(p, stream);
+    case 7: return launch_real_lt<7>(p, stream);
+    case 8: return launch_real_lt<8>(p, stream);
+    case 9: return launch_real_lt<9>(p, stream);
+    case 10: return launch_real_lt<10>(p, stream);
+    case 11: return launch_real_lt<11>(p, stream);
+    case 12: return launch_real_lt<12>(p, stream);
+    case 13: return launch_real_lt<13>(p, stream);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_finalize(int precision, const FinalParams& p,

@@ -679,3 +679,30 @@ def test_each_device_gets_its_own_shared_memory_opt_in(mqw, orc):
                     for p in ("fp32", "fp64")])
         c.close()
     assert out[0] == out[1]
+
+
+@pytest.mark.parametrize("n,m,samples,tile", [(16, 3, 24, 0), (20, 4, 12, 0), (21, 3, 6, 11),
+                                              (14, 4, 9, 0)])
+def test_real_chains_match_complex_chains(ctx, orc, mqw, monkeypatch, n, m, samples, tile):
+    """The shared-basis chains on the real chain kernel (the default) against
+    the same chains on the complex pass kernel (MQW_REAL_CHAINS=0): the real
+    kernel reproduces the real parts bit for bit, so every per-sample P is
+    identical — with the stage-2 product basis forced on (its chains start
+    from the stage-1 basis vectors), and at n = 21 with 2^11 tiles, where
+    three axes of every pass are read from global memory."""
+    raw = orc.sk_instances(n, 1, 5300 + n)
+    monkeypatch.setenv("MQW_STAGE2_BASIS", "1")
+    shape = {"tile_log": tile} if tile else {}
+
+    def run(real):
+        monkeypatch.setenv("MQW_REAL_CHAINS", "1" if real else "0")
+        plan = mqw.Plan(ctx, n, m, raw, samples=samples, graph=0, **shape)
+        plan.execute()
+        out = plan.results(per_sample=True)["p_sample"]
+        plan.close()
+        return out
+
+    on, off = run(True), run(False)
+    assert np.array_equal(on, off)
+    r64 = ctx.run_problems(n, m, raw, samples=samples, precision="fp64", graph=0)
+    assert abs(float(np.mean(on)) - r64["p"][0]) <= 1e-5
