@@ -85,7 +85,7 @@ def parse():
     ap.add_argument("--threads", type=int, default=0, help="CTA threads 512/256 (0: autotuned)")
     ap.add_argument("--lane-smem", type=int, default=0, help="lane axes: 1 shared memory, -1 shuffles")
     ap.add_argument("--tma", type=int, default=0,
-                    help="tile staging: 1 bulk copies, 2 psi straight into registers, -1 cp.async")
+                    help="tile staging: 1 bulk copies, 2 second exchange tile, -1 cp.async")
     ap.add_argument("--seed", type=int, default=20)
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 |dP| check")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")

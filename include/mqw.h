@@ -81,10 +81,9 @@ typedef struct mqw_options {
   int lane_smem;   /* grid-path partners along the warp-lane axes: 1 from
                       shared memory, -1 by warp shuffles, 0 = autotuned */
   int tma;         /* grid-path tile staging (FP32): 1 bulk copies (TMA)
-                      completing on an mbarrier, 2 psi loaded straight into
-                      registers with a second exchange tile (shapes with 8
-                      amplitude pairs per thread), -1 per-thread cp.async,
-                      0 = autotuned */
+                      completing on an mbarrier, 2 per-thread cp.async with
+                      a second exchange tile (shapes with 8 amplitude pairs
+                      per thread), -1 per-thread cp.async, 0 = autotuned */
   int stage1_basis; /* 1 (default): FP32 walks of an instance share one
                        Chebyshev basis for their first stage (built once,
                        recombined per walk); 0: every walk runs its own
@@ -287,8 +286,8 @@ typedef struct mqw_grid_shape {
   int tile_log, cluster_log, global_axes, group, lanes;
   int threads;     /* threads per CTA */
   int lane_smem;   /* 1: lane-axis partners from shared memory */
-  int tma;         /* 1: tiles staged by bulk copies, 2: psi loaded straight
-                      into registers, 0: per-thread cp.async */
+  int tma;         /* 1: tiles staged by bulk copies, 2: cp.async with a
+                      second exchange tile, 0: per-thread cp.async */
   double us_per_walk_pass;
 } mqw_grid_shape;
 mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,

@@ -70,7 +70,7 @@ struct GridShape {
   int lmax = 0, group = 1, lanes = 1;
   int threads = 0;  // CTA threads at the widest tile (0: 512)
   int lane_smem = 0;  // lane axes: 1 shared memory, -1 shuffles, 0 (want): any
-  int tma = 0;        // staging: 1 bulk copies, 2 psi straight into registers,
+  int tma = 0;        // staging: 1 bulk copies, 2 a second exchange tile,
                       // -1 cp.async, 0 (want): any
   double us = 0.0;  // timed microseconds per walk-pass (0: not timed)
   int bgroup = 1;   // walks per shared-basis group (>= group; set by the plan)

@@ -148,9 +148,9 @@ struct PassParams {
                        // or 256 (more pairs per thread)
   int lane_smem;       // 1: lane-axis partners from shared memory (FP32,
                        // tiles of 2^12 and 2^13), 0: warp shuffles
-  int tma;             // 2: psi straight into registers (8 pairs per thread;
-                       // a second exchange tile). 1: the tile's b, P, psi
-                       // and D arrive by bulk copies
+  int tma;             // 2: a second exchange tile (8 pairs per thread).
+                       // 1: the tile's b, P, psi and D arrive by bulk
+                       // copies
                        // (TMA) on an mbarrier, FP32 single-CTA tiles
   int comp;            // 1: compensated partner sums (FP32-compensated mode)
   int tiling;          // 1 or 2
@@ -165,8 +165,8 @@ struct PassGeomHost {
   int C;               // cluster log (tile of 2^(L+C) amplitudes over 2^C CTAs)
   int threads;         // CTA threads (0: default 512)
   int lane_smem;       // lane axes through shared memory instead of shuffles
-  int tma;             // tile staging: 0 cp.async, 1 bulk copies (TMA), 2 psi
-                       // straight into registers
+  int tma;             // tile staging: 0 cp.async, 1 bulk copies (TMA), 2
+                       // cp.async with a second exchange tile
 };
 // Geometry for n; lmax > 0 caps the tile (log2 amplitudes), else the
 // precision's default cap (or MQW_PASS_TILE_LOG) applies.

@@ -507,14 +507,13 @@ constexpr int pass_min_blocks() {
 // slower than cp.async.
 // COMP: the partner sums are compensated (PartnerSum<float, true>): the
 // FP32-compensated precision mode.
-// DR: psi goes straight from global memory into registers instead of
-// through cp.async staging, which saves its shared-memory write and read;
-// the freed space holds a second exchange tile, so b_r is written to it
-// without first waiting for every reader of b_{r+1}'s tile (one block
-// barrier fewer per pass). Shapes with P in registers (8 pairs per thread)
-// only.
+// X2: a second exchange tile: b_r is written to its own tile without first
+// waiting for every reader of b_{r+1}'s tile (one block barrier fewer per
+// pass) at the cost of 16 B of shared memory per amplitude. Shapes with P in
+// registers (8 pairs per thread) only, where it still leaves two CTAs per
+// SM at the 2^12 tile.
 template <typename R, int LT, int CL, int TB, bool LS = false, bool TMA = false,
-          bool COMP = false, bool DR = false>
+          bool COMP = false, bool X2 = false>
 __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
                                   pass_min_blocks<LT, TB, sizeof(R) == 4, CL>())
     pass_kernel(PassParams p) {
@@ -522,8 +521,8 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   constexpr int RP = S::kRP, LOGT = S::kLogT, T = S::kThreads;
   constexpr bool kStageP = S::kStageP || TMA;
   static_assert(!TMA || CL == 0, "bulk-copy staging is for single-CTA tiles");
-  static_assert(!DR || (!kStageP && CL == 0 && !TMA && !LS),
-                "direct loads need P in registers and a single-CTA tile");
+  static_assert(!X2 || (!kStageP && CL == 0 && !TMA && !LS),
+                "the second exchange tile is for shapes with P in registers and a single-CTA tile");
   constexpr int LL = LT + CL;  // tile bits of the tiling
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[32];
@@ -536,7 +535,8 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   R* sp = sx + 4 * S::kPairs;              // staged P_r, [j][tid] pairs
   R* ss = kStageP ? sp + 4 * S::kPairs : sp;  // staged psi
   float2* sd = reinterpret_cast<float2*>(ss + 4 * S::kPairs);  // staged D
-  R* sx2 = DR ? ss : sx;  // DR: b_r's exchange tile (where psi would be staged)
+  // X2: b_r's exchange tile, after the staged D
+  R* sx2 = X2 ? reinterpret_cast<R*>(sd + S::kPairs) : sx;
   // Global amplitude index of register pair j: g0 + j * gstride (32-bit: n <= 30).
   // For a 1-D cluster the cluster rank is blockIdx.x mod 2^CL.
   const unsigned rank = CL > 0 ? (blockIdx.x & ((1u << CL) - 1u)) : 0u;
@@ -648,7 +648,7 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
       const unsigned gi = g0 + j * gstride;
       const int o = j * T + tid;
       if (kStageP && !first) cp_async_pair<R>(sp + 4 * o, part + 2 * (size_t)gi);
-      if (!uni && !DR) cp_async_pair<R>(ss + 4 * o, psi + 2 * (size_t)gi);
+      if (!uni) cp_async_pair<R>(ss + 4 * o, psi + 2 * (size_t)gi);
       cp_async8(sd + o, hp + gi);
     }
 #pragma unroll
@@ -657,17 +657,6 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
       if constexpr (!kStageP) pv[j] = first ? pzero<R>() : pld(part + 2 * (size_t)(g0 + j * gstride));
     }
   }
-  // DR: psi of this thread's pairs straight into registers; issued once b_r
-  // is formed (when P_r's registers are free), before the barrier and the
-  // exchange-tile store that cover part of its latency.
-  Pair<R> psv[DR ? RP : 1];
-  auto load_direct = [&]() {
-    if constexpr (DR) {
-#pragma unroll
-      for (int j = 0; j < RP; j++)
-        psv[j] = uni ? pzero<R>() : pld(psi + 2 * (size_t)(g0 + j * gstride));
-    }
-  };
   const double kap = W.kappa ? *W.kappa : 1.0;
   const R scale = (R)W.scale;
   const R gamma = (R)W.gamma;
@@ -677,12 +666,9 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   if (first) {
     const R cr = (R)((double)W.coef[r] * kap);
     if (!bulk) cp_async_wait_all();
-    load_direct();
 #pragma unroll
     for (int j = 0; j < RP; j++) {
-      V4<R> pv;
-      if constexpr (DR) pv = uni ? V4<R>{psi0, 0, psi0, 0} : to4(psv[DR ? j : 0]);
-      else pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * (j * T + tid));
+      const V4<R> pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * (j * T + tid));
       vb[j] = from4(cpsi4<R>(cr, r & 1, pv));
     }
   } else {
@@ -715,7 +701,6 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
       vb[j] = from4(V4<R>{fma(-ag, acc.x, pr.x), fma(-ag, acc.y, pr.y),
                           fma(-ag, acc.z, pr.z), fma(-ag, acc.w, pr.w)});
     }
-    if (r > 0) load_direct();
   }
 #pragma unroll
   for (int j = 0; j < RP; j++) pst(bout + 2 * (size_t)(g0 + j * gstride), vb[j]);
@@ -741,9 +726,9 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
     return;
   }
   // Start P_{r-1} = c psi + a (D b_r - gamma X_Z b_r) - b_{r+1} over all tile axes.
-  // (DR: b_r goes to its own exchange tile, so no reader of b_{r+1}'s tile
+  // (X2: b_r goes to its own exchange tile, so no reader of b_{r+1}'s tile
   // has to be waited for.)
-  if constexpr (!DR) tile_barrier<CL>();  // every reader of sx (this CTA and its peers) is done
+  if constexpr (!X2) tile_barrier<CL>();  // every reader of sx (this CTA and its peers) is done
 #pragma unroll
   for (int j = 0; j < RP; j++) pst(sx2 + 4 * (tid | (j << LOGT)), vb[j]);
   tile_barrier<CL>();
@@ -757,9 +742,7 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
     cluster_add(accp, rv, 0, LL);
     const V4<R> acc = to4(accp.value());
     const int o = j * T + tid;
-    V4<R> pv;
-    if constexpr (DR) pv = uni ? V4<R>{psi0, 0, psi0, 0} : to4(psv[DR ? j : 0]);
-    else pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * o);
+    const V4<R> pv = uni ? V4<R>{psi0, 0, psi0, 0} : ld4<R>(ss + 4 * o);
     const float2 d = sd[o];
     const V4<R> b = to4(vb[j]);
     const V4<R> b1 = to4(va[j]);
@@ -1217,9 +1200,9 @@ PassGeomHost pass_geom(int precision, int n, int lmax, int threads, int lane_sme
   g.threads = (threads == 256 && L == cap && g.C == 0) ? 256 : 0;
   // Lane axes through shared memory: FP32 single-CTA tiles of 2^12 or 2^13.
   g.lane_smem = (lane_smem && precision == 0 && g.C == 0 && L >= cap) ? 1 : 0;
-  // Staging: bulk copies (1) on FP32 single-CTA tiles; psi straight into
-  // registers (2) on FP32 single-CTA tiles with 8 pairs per thread (the
-  // 256-thread 2^12 tile or the 2^13 tile) and shuffled lane axes.
+  // Staging: bulk copies (1) on FP32 single-CTA tiles; cp.async with a
+  // second exchange tile (2) on FP32 single-CTA tiles with 8 pairs per thread
+  // (the 256-thread 2^12 tile or the 2^13 tile) and shuffled lane axes.
   g.tma = 0;
   if (tma == 1 && precision == 0 && g.C == 0) g.tma = 1;
   if (tma == 2 && precision == 0 && g.C == 0 && !g.lane_smem &&
@@ -1230,18 +1213,20 @@ PassGeomHost pass_geom(int precision, int n, int lmax, int threads, int lane_sme
 
 namespace {
 template <typename R, int LT, int CL, int TB = kPassThreads, bool LS = false, bool TMA = false,
-          bool COMP = false, bool DR = false>
+          bool COMP = false, bool X2 = false>
 cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
   using S = PassShape<LT, TB>;
-  const size_t smem = S::template smem<R, S::kStageP || TMA>();
+  // X2: a second exchange tile after the staged D.
+  const size_t smem = S::template smem<R, S::kStageP || TMA>() +
+                      (X2 ? (size_t)S::kPairs * 4 * sizeof(R) : 0);
   {
-    cudaError_t e = ensure_smem_optin((const void*)pass_kernel<R, LT, CL, TB, LS, TMA, COMP, DR>,
+    cudaError_t e = ensure_smem_optin((const void*)pass_kernel<R, LT, CL, TB, LS, TMA, COMP, X2>,
                                       smem, CL > 3);
     if (e != cudaSuccess) return e;
   }
   const dim3 grid((unsigned)((size_t)1 << (p.n - LT)), p.count);
   if constexpr (CL == 0) {
-    pass_kernel<R, LT, 0, TB, LS, TMA, COMP, DR><<<grid, S::kThreads, smem, stream>>>(p);
+    pass_kernel<R, LT, 0, TB, LS, TMA, COMP, X2><<<grid, S::kThreads, smem, stream>>>(p);
     return cudaGetLastError();
   } else {
     cudaLaunchConfig_t cfg = {};
@@ -1262,8 +1247,8 @@ cudaError_t launch_pass_lt(const PassParams& p, cudaStream_t stream) {
 
 // FP32 single-CTA tile variants: threads (512/256), lane axes (shuffles or
 // shared memory) and staging (cp.async or bulk copies).
-// p.tma: 0 cp.async staging, 1 bulk copies, 2 psi straight into registers
-// (shapes with 8 pairs per thread, shuffled lane axes).
+// p.tma: 0 cp.async staging, 1 bulk copies, 2 cp.async staging with a
+// second exchange tile (shapes with 8 pairs per thread, shuffled lane axes).
 template <typename R, int LT, int TB>
 cudaError_t launch_pass_variant(const PassParams& p, cudaStream_t stream) {
   if (p.tma == 2) {

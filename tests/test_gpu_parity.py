@@ -646,12 +646,11 @@ def test_stage2_tensor_core_gemm_matches_simt(ctx, orc, mqw, monkeypatch, n, m, 
 
 @pytest.mark.parametrize("n,tile,threads", [(19, 12, 256), (20, 12, 256), (22, 13, 512),
                                             (24, 13, 512)])
-def test_direct_register_staging_matches_cp_async(ctx, orc, n, tile, threads):
-    """psi loaded straight into registers with a second exchange tile (tma=2,
-    shapes with 8 pairs per thread: the 256-thread 2^12 tile and the 2^13
-    tile) against cp.async staging: the same arithmetic, so bit-identical
-    per-sample values, including n = 24 (2^13 tiles, two axes read from
-    global memory), and within FP32 of FP64."""
+def test_second_exchange_tile_matches_one(ctx, orc, n, tile, threads):
+    """A second exchange tile (tma=2, shapes with 8 pairs per thread: the
+    256-thread 2^12 tile and the 2^13 tile) against the single tile: the same
+    arithmetic, so bit-identical per-sample values, including n = 24 (2^13
+    tiles, two axes read from global memory), and within FP32 of FP64."""
     raw = orc.sk_instances(n, 1, 2700 + n)
     kw = dict(samples=3, graph=0, group=1, lanes=1, tile_log=tile, threads=threads, lane_smem=-1,
               stage1_basis=0)
