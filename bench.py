@@ -86,6 +86,8 @@ def parse():
     ap.add_argument("--lane-smem", type=int, default=0, help="lane axes: 1 shared memory, -1 shuffles")
     ap.add_argument("--tma", type=int, default=0,
                     help="tile staging: 1 bulk copies, 2 second exchange tile, -1 cp.async")
+    ap.add_argument("--cluster", type=int, default=0,
+                    help="widest tile with axes left over: 1 cluster, -1 global axes (0: autotuned)")
     ap.add_argument("--seed", type=int, default=20)
     ap.add_argument("--no-check", action="store_true", help="skip the FP64 |dP| check")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline")
@@ -532,7 +534,7 @@ def main():
     ns, ms, raw, desc = make_batch(M, a, rank)
     count = len(ns)
     shape = dict(group=a.group, tile_log=a.tile_log, lanes=a.lanes, threads=a.threads,
-                 lane_smem=a.lane_smem, tma=a.tma)
+                 lane_smem=a.lane_smem, tma=a.tma, cluster=a.cluster)
     plan = M.Plan(ctx, ns, ms, raw, samples=a.samples, precision=a.precision, **shape)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
 
@@ -706,7 +708,8 @@ def main():
             except Exception as ex:  # the baseline is reported, not required
                 cpu = {"value": None, "error": str(ex)}
         config = dict(desc)
-        if not (a.group or a.tile_log or a.lanes or a.threads or a.lane_smem or a.tma):
+        if not (a.group or a.tile_log or a.lanes or a.threads or a.lane_smem or a.tma
+                or a.cluster):
             config["grid_shape"] = ctx.grid_shape(max(ns), a.precision)
         config["reference_term_amps_per_step"] = term_amps / a.steps
         config["pass_term_amps_per_step"] = pass_amps / a.steps

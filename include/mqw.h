@@ -93,6 +93,11 @@ typedef struct mqw_options {
                        e_{E_loc} (the output norm is taken as the input norm,
                        exact up to the 1e-6 Chebyshev tail); 0: every walk
                        runs its own last-stage recurrence */
+  int cluster;     /* where the widest grid-path tile leaves axes to neither
+                      tiling (n > 20 in FP32): 1 tiles spanning a thread-block
+                      cluster, -1 single-CTA tiles with those axes read from
+                      global memory, 0 = autotuned (clusters when the other
+                      shape fields are all fixed) */
 } mqw_options;
 
 typedef struct mqw_diag_info {

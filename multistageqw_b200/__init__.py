@@ -61,6 +61,7 @@ class Options(ctypes.Structure):
         ("tma", ctypes.c_int),
         ("stage1_basis", ctypes.c_int),
         ("final_projection", ctypes.c_int),
+        ("cluster", ctypes.c_int),
     ]
 
 
@@ -198,7 +199,7 @@ def _ptr(a, ct):
 
 def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_max_n=0,
           stage_scale=None, tile_log=0, graph=1, lanes=0, threads=0, lane_smem=0,
-          tma=0, stage1_basis=1, final_projection=1):
+          tma=0, stage1_basis=1, final_projection=1, cluster=0):
     o = Options()
     lib().mqw_default_options(ctypes.byref(o))
     o.precision = {"fp32": FP32, "fp64": FP64, "fp32c": FP32C, FP32: FP32, FP64: FP64,
@@ -215,6 +216,7 @@ def _opts(precision="fp32", samples=SAMPLES, cheb_tol=1e-6, group=0, resident_ma
     o.tma = int(tma)
     o.stage1_basis = int(stage1_basis)
     o.final_projection = int(final_projection)
+    o.cluster = int(cluster)
     keep = None
     if stage_scale is not None:
         keep = np.ascontiguousarray(stage_scale, dtype=np.float32)

@@ -72,6 +72,9 @@ struct GridShape {
   int lane_smem = 0;  // lane axes: 1 shared memory, -1 shuffles, 0 (want): any
   int tma = 0;        // staging: 1 bulk copies, 2 a second exchange tile,
                       // -1 cp.async, 0 (want): any
+  int cl = 0;         // where the widest tile leaves axes over: 1 a tile
+                      // spanning a cluster, -1 single-CTA tiles with those
+                      // axes read from global memory, 0 (want): any
   double us = 0.0;  // timed microseconds per walk-pass (0: not timed)
   int bgroup = 1;   // walks per shared-basis group (>= group; set by the plan)
 };
@@ -216,6 +219,7 @@ void default_opts(mqw_options* o) {
   o->threads = 0;
   o->lane_smem = 0;
   o->tma = 0;
+  o->cluster = 0;
   o->stage1_basis = 1;
   o->final_projection = 1;
 }
@@ -332,8 +336,8 @@ int default_group(int precision, const PassGeomHost& geo, int n) {
 // Returns microseconds per walk-pass.
 mqw_status time_grid_config(mqw_ctx* ctx, int precision, int n, int lmax,
                             int G, int lanes, int threads, int lane_smem, int tma,
-                            double* us_per_walk, int reps = 12) {
-  const PassGeomHost geo = pass_geom(precision, n, lmax, threads, lane_smem, tma);
+                            double* us_per_walk, int reps = 12, int cluster = 1) {
+  const PassGeomHost geo = pass_geom(precision, n, lmax, threads, lane_smem, tma, cluster);
   const size_t N = (size_t)1 << n;
   const size_t amp = precision == 0 ? 8 : 16;
   const int slots = walk_slots(geo);
@@ -412,7 +416,7 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
   const auto key = std::make_pair(precision, n);
   auto it = ctx->tuned.find(key);
   const bool fixed_none = !want.lmax && !want.group && !want.lanes && !want.threads &&
-                          !want.lane_smem && !want.tma;
+                          !want.lane_smem && !want.tma && !want.cl;
   if (it != ctx->tuned.end() && fixed_none) {
     *out = it->second;
     return MQW_OK;
@@ -426,9 +430,9 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
     return g <= kMaxGroup && (size_t)g * lanes * walk_bytes(precision, geo, n) <= budget;
   };
   auto time = [&](const GridShape& c, double* us) -> mqw_status {
-    const PassGeomHost geo = pass_geom(precision, n, c.lmax, c.threads, c.lane_smem > 0, std::max(0, c.tma));
+    const PassGeomHost geo = pass_geom(precision, n, c.lmax, c.threads, c.lane_smem > 0, std::max(0, c.tma), c.cl < 0 ? 0 : 1);
     mqw_status s = time_grid_config(ctx, precision, n, c.lmax, c.group, c.lanes, c.threads,
-                                    c.lane_smem > 0, std::max(0, c.tma), us);
+                                    c.lane_smem > 0, std::max(0, c.tma), us, 12, c.cl < 0 ? 0 : 1);
     if (s == MQW_OK && log)
       fprintf(stderr,
               "mqw tune: precision %d n %d tile %d cluster %d global %d threads %d lane_smem %d "
@@ -451,17 +455,23 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
   b.threads = want.threads == 256 ? 256 : 0;
   b.lane_smem = want.lane_smem;
   b.tma = want.tma;
-  for (int l : caps) {
+  // At the widest tile, when axes are left over, both the cluster-spanning
+  // tile and the single-CTA tile with global-memory axes are candidates.
+  for (int l : caps)
+    for (int cl : {1, -1}) {
     if (want.lmax && l != want.lmax) continue;
+    if (want.cl && want.cl != cl) continue;
+    if (cl < 0 && (l != def_l || n <= 2 * def_l - 4)) continue;
     for (int threads : {0, 256})
       for (int ls : {0, 1})
         for (int tma : {0, 1, 2}) {
           if (want.threads && (want.threads == 256) != (threads == 256)) continue;
           if (want.lane_smem && (want.lane_smem > 0) != (ls == 1)) continue;
           if (want.tma && std::max(0, want.tma) != tma) continue;
-          const PassGeomHost geo = pass_geom(precision, n, l, threads, ls, tma);
+          const PassGeomHost geo = pass_geom(precision, n, l, threads, ls, tma, cl < 0 ? 0 : 1);
           if (geo.threads != threads || geo.lane_smem != ls || geo.tma != tma) continue;
           GridShape c;
+          c.cl = cl;
           c.lmax = l;
           c.threads = threads;
           c.lane_smem = ls ? 1 : -1;
@@ -480,10 +490,10 @@ mqw_status tune_grid(mqw_ctx* ctx, int precision, int n, GridShape want, GridSha
             b = c;
           }
         }
-  }
+    }
   // Stage 2: walks per launch and lanes for that shape.
   if (best < 1e300 && (!want.group || !want.lanes)) {
-    const PassGeomHost geo = pass_geom(precision, n, b.lmax, b.threads, b.lane_smem > 0, std::max(0, b.tma));
+    const PassGeomHost geo = pass_geom(precision, n, b.lmax, b.threads, b.lane_smem > 0, std::max(0, b.tma), b.cl < 0 ? 0 : 1);
     const int g0 = default_group(precision, geo, n);
     std::vector<int> groups = {1, 2, 4};
     if (g0 != 1 && g0 != 2 && g0 != 4) groups.push_back(g0);
@@ -1064,7 +1074,7 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
   for (auto& kv : grid_by_n) {
     const int n = kv.first;
     const GridShape gs = P.grid_geo.at(n);
-    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, std::max(0, gs.tma));
+    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, std::max(0, gs.tma), gs.cl < 0 ? 0 : 1);
     const int G = gs.group;
     const std::vector<int>& ws = kv.second;
     const int kb1 = P.basis_kb1.count(n) ? P.basis_kb1.at(n) : 0;
@@ -1289,6 +1299,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     gs.threads = P.opt.threads == 256 ? 256 : 0;
     gs.lane_smem = P.opt.lane_smem;
     gs.tma = P.opt.tma;
+    gs.cl = P.opt.cluster;  // fixed (1 / -1) or tuned (0; clusters when not tuned)
     if (!gs.lmax || !gs.group || !gs.lanes || !P.opt.threads || !P.opt.lane_smem ||
         !P.opt.tma) {
       GridShape want = gs;
@@ -1303,12 +1314,13 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       gs.lane_smem = -1;
       gs.tma = -1;
       gs.lmax = std::min(gs.lmax, 12);
-      if (pass_geom(P.precision, n, gs.lmax).C > 0) gs.lmax = 11;  // single-CTA tiles
+      if (pass_geom(P.precision, n, gs.lmax, 0, 0, 0, gs.cl < 0 ? 0 : 1).C > 0)
+        gs.lmax = 11;  // single-CTA tiles
     }
     gs.group = std::min(std::min(gs.group, kMaxGroup), kv.second);
     const int ngroups = (kv.second + gs.group - 1) / gs.group;
     gs.lanes = std::max(1, std::min(gs.lanes, ngroups));
-    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, std::max(0, gs.tma));
+    const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, std::max(0, gs.tma), gs.cl < 0 ? 0 : 1);
     // Walks per shared-basis group: the stage-1 recombination and the
     // last-stage projection read each basis vector once per group, so the
     // group is as large as the launch structures allow (kMaxGroup) within a
@@ -1411,7 +1423,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       const int n = e.first;
       const GridShape& gs = P.grid_geo.at(n);
       const PassGeomHost geo = pass_geom(P.precision, n, gs.lmax, gs.threads,
-                                         gs.lane_smem > 0, std::max(0, gs.tma));
+                                         gs.lane_smem > 0, std::max(0, gs.tma), gs.cl < 0 ? 0 : 1);
       int k1 = want1 && e.second.first <= kMaxBasis ? e.second.first : 0;
       int k2 = want2 && e.second.second <= kMaxBasis ? e.second.second : 0;
       if (BasisLayout::bytes(n, k1, k2) > budget) k2 = 0;
@@ -1894,7 +1906,7 @@ mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,
   want.group = want.lanes = 0;  // nothing fixed
   st = tune_grid(ctx, precision, n, want, &gs);
   if (st != MQW_OK) return st;
-  const PassGeomHost geo = pass_geom(precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, std::max(0, gs.tma));
+  const PassGeomHost geo = pass_geom(precision, n, gs.lmax, gs.threads, gs.lane_smem > 0, std::max(0, gs.tma), gs.cl < 0 ? 0 : 1);
   out->tile_log = geo.L;
   out->threads = geo.threads ? geo.threads : 512;
   out->lane_smem = geo.lane_smem;
@@ -1921,7 +1933,7 @@ mqw_status mqw_pass_timing(mqw_ctx* ctx, int precision, int n, int reps,
   if (st != MQW_OK) return st;
   double us = 0.0;
   st = time_grid_config(ctx, precision, n, gs.lmax, gs.group, gs.lanes, gs.threads,
-                        gs.lane_smem > 0, std::max(0, gs.tma), &us, reps);
+                        gs.lane_smem > 0, std::max(0, gs.tma), &us, reps, gs.cl < 0 ? 0 : 1);
   if (st != MQW_OK) return st;
   // time_grid_config returns the elapsed time per walk-pass: launches carry
   // `group` walks and `lanes` launches are in flight at a time.

@@ -171,7 +171,7 @@ struct PassGeomHost {
 // Geometry for n; lmax > 0 caps the tile (log2 amplitudes), else the
 // precision's default cap (or MQW_PASS_TILE_LOG) applies.
 PassGeomHost pass_geom(int precision, int n, int lmax = 0, int threads = 0,
-                        int lane_smem = 0, int tma = 0);
+                        int lane_smem = 0, int tma = 0, int cluster = 1);
 cudaError_t launch_pass(int precision, const PassParams& p,
                         cudaStream_t stream);
 

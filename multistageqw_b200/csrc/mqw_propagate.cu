@@ -1158,13 +1158,16 @@ int max_cluster_log() {
 }
 }  // namespace
 
-PassGeomHost pass_geom(int precision, int n, int lmax, int threads, int lane_smem, int tma) {
+PassGeomHost pass_geom(int precision, int n, int lmax, int threads, int lane_smem, int tma,
+                        int cluster) {
   // Tile: 2^L amplitudes of b_{r+1} and 2^L of b_r in shared memory
   // (64 KB at L = 12 in FP32, 3 CTAs per SM). Rows of 2^a = 16 amplitudes
   // (128 bytes in FP32) keep T2 loads coalesced. L is chosen so the two
   // tilings cover every axis when possible (2L - a >= n); above that, at the
   // widest compiled tile, a tiling's tile spans a cluster of 2^C CTAs
-  // (2(L+C) - a >= n up to C = 4) before any axis is left to global memory.
+  // (2(L+C) - a >= n up to C = 4) before any axis is left to global memory;
+  // cluster = 0 keeps single-CTA tiles there and reads the remaining axes
+  // from global memory.
   static const int env = [] {  // read once; thread-safe initialisation
     const char* e = getenv("MQW_PASS_TILE_LOG");
     return e ? atoi(e) : -1;
@@ -1189,7 +1192,7 @@ PassGeomHost pass_geom(int precision, int n, int lmax, int threads, int lane_sme
   if (L > n) L = n;
   g.L = L;
   g.nu = n - (2 * L - g.a);
-  if (g.nu > 0 && L == cap) {
+  if (g.nu > 0 && L == cap && cluster) {
     const int cmax = precision == 0 ? max_cluster_log<float, 12>() : max_cluster_log<double, 11>();
     g.C = (g.nu + 1) / 2;
     if (g.C > cmax) g.C = cmax;

@@ -200,6 +200,24 @@ def test_cluster_tiles_match_global_partner_path(ctx, orc, n):
     assert 0.0 < r_cl["p"][0] < 1.0
 
 
+@pytest.mark.parametrize("n", [23, 25])
+def test_single_cta_widest_tiles_match_cluster_tiles(ctx, orc, n):
+    """cluster = -1 keeps the widest tile (2^12 in FP32) on one CTA and reads
+    the axes neither tiling covers from global memory (3 at n = 23, 5 at
+    n = 25) instead of spanning a cluster; with it the shared-basis chains
+    run on the real chain kernel. Both shapes agree with each other and with
+    FP64 to the FP32 target."""
+    raw = orc.sk_instances(n, 1, 700 + n)
+    kw = dict(samples=2, graph=0, group=1, tile_log=12)
+    r_cl = ctx.run_problems(n, 2, raw, precision="fp32", cluster=1, **kw)
+    r_gl = ctx.run_problems(n, 2, raw, precision="fp32", cluster=-1, **kw)
+    r_64 = ctx.run_problems(n, 2, raw, precision="fp64", samples=2, graph=0)
+    assert r_cl["stats"]["terms"] == r_gl["stats"]["terms"] == r_64["stats"]["terms"]
+    assert abs(r_cl["p"][0] - r_gl["p"][0]) <= 1e-6
+    assert abs(r_gl["p"][0] - r_64["p"][0]) <= 1e-5
+    assert 0.0 < r_gl["p"][0] < 1.0
+
+
 def test_lanes_give_identical_results(ctx, orc, mqw):
     """Walk groups run on 1, 2 or 3 concurrent lanes (streams, and branches
     of the captured graph) produce bit-identical per-sample results."""
