@@ -663,6 +663,9 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
     mqw_status s = finalize(0, W, 0, rtiles);
     if (s != MQW_OK) return s;
   }
+  // Small n: every term of a walk-stage in one chain launch (a cluster of
+  // CTAs per walk) instead of one launch per term.
+  const int chain_L = P.comp ? 0 : chain_tile_log(P.precision, n);
   // Recurrence stages [combine, end) of each pass group.
   for (int g0 = 0; g0 < W; g0 += G) {
     const int g1 = std::min(W, g0 + G);
@@ -674,6 +677,43 @@ mqw_status run_grid_group(mqw_plan& P, const std::vector<int>& widx,
       for (int g = g0; g < g1; g++) {
         K[g - g0] = degree(g, st);
         Kmax = std::max(Kmax, K[g - g0]);
+      }
+      if (chain_L && Kmax > 0) {
+        PassParams pp{};
+        pp.n = n;
+        pp.L = chain_L;
+        pp.a = geo.a;
+        pp.tiling = 1;
+        pp.err = ctx->dev_err.as<unsigned>();
+        pp.count = g1 - g0;
+        for (int g = g0; g < g1; g++) {
+          PassWalk& Wk = pp.walk[g - g0];
+          const ResidentWalk& w = P.walks[widx[g]];
+          Wk.active = K[g - g0] > 0;
+          if (!Wk.active) continue;
+          const int job = w.stage_desc_off + st;
+          Wk.bin = Wk.bout = buf(g, xs[g]);  // no axis from global memory: in place
+          Wk.part = buf(g, ps);
+          Wk.psi = buf(g, pi[g]);
+          Wk.hp = hp + w.hp_off;
+          Wk.coef = coef + P.coef_off[job];
+          Wk.kappa = st == 0 ? nullptr : kappa + g;
+          Wk.norm_part = norm_part + (size_t)g * rtiles;
+          Wk.gamma = P.jobs[job].gamma;
+          Wk.scale = P.onenorm[job];
+          Wk.K = K[g - g0];
+          Wk.psi_uniform = st == 0;
+          Wk.psi0 = (float)(1.0 / std::sqrt((double)N));
+          if (P.counting) P.stats.pass_amps += (double)N * K[g - g0];
+        }
+        CK(launch_pass_chain(P.precision, pp, stream));
+        if (P.counting) {
+          P.stats.launches++;
+          P.stats.term_launches++;
+        }
+        mqw_status s = finalize(g0, g1, st, (int)(N >> chain_L));
+        if (s != MQW_OK) return s;
+        continue;
       }
       for (int r = Kmax - 1; r >= 0; r--) {
         PassParams pp{};
@@ -811,6 +851,43 @@ mqw_status issue_chain(mqw_plan& P, const ResidentWalk& w0, int stage, int K,
     // Every vector of the chain is real: the real chain kernel, writing
     // each b_r straight into its basis slot and reading b_{r+1} back from
     // the previous one (no complex b slot, no separate real copy).
+    // Small n: the whole chain in one launch when the outputs are laid out
+    // as two interleaved strided sequences (even and odd j), which both the
+    // stage-1/last-stage bases and the stage-2 product basis are.
+    const int cL = chain_tile_log(0, w0.n);
+    if (cL && K > 0) {
+      float* base0 = out_of(0);
+      float* base1 = K > 1 ? out_of(1) : nullptr;
+      const long long stride = K > 2 ? (long long)(out_of(2) - base0) : (long long)(2 * N);
+      bool affine = stride >= (long long)N;
+      for (int j = 0; j < K && affine; j++)
+        affine = out_of(j) == (j & 1 ? base1 : base0) + (size_t)(j >> 1) * (size_t)stride;
+      if (affine) {
+        RealChainParams rp{};
+        rp.n = w0.n;
+        rp.L = cL;
+        rp.a = geo.a;
+        rp.part = static_cast<float*>(S.part);
+        rp.start = S.start_real;
+        rp.start_uniform = S.uniform ? 1 : 0;
+        rp.psi0 = (float)(1.0 / std::sqrt((double)N));
+        rp.hp = P.d_hp.as<float>() + w0.hp_off;
+        rp.gamma = P.jobs[job].gamma;
+        rp.scale = P.onenorm[job];
+        rp.K = K;
+        rp.R = R;
+        rp.out_base[0] = base0;
+        rp.out_base[1] = base1;
+        rp.out_stride = stride;
+        CK(launch_real_chain(rp, stream));
+        if (P.counting) {
+          P.stats.launches++;
+          P.stats.term_launches++;
+          P.stats.aux_bytes += (double)N * 20.0 * K;
+        }
+        return MQW_OK;
+      }
+    }
     for (int j = 0; j < K; j++) {
       RealChainParams rp{};
       rp.n = w0.n;

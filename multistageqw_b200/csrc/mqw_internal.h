@@ -174,6 +174,15 @@ PassGeomHost pass_geom(int precision, int n, int lmax = 0, int threads = 0,
                         int lane_smem = 0, int tma = 0, int cluster = 1);
 cudaError_t launch_pass(int precision, const PassParams& p,
                         cudaStream_t stream);
+// Chain launch: every term of one walk-stage per walk in one launch, a
+// thread-block cluster of 2^(n-L) <= 16 CTAs per walk with cluster barriers
+// between the passes (n small enough that no axis is read from global
+// memory). chain_tile_log gives its tile log L for (precision, n), or 0 when
+// it does not apply (also with MQW_CHAIN=0). p: as for launch_pass with
+// p.L = chain_tile_log, per walk K (its degree) and active = K > 0; p.tiling
+// and the walks' r are not read.
+int chain_tile_log(int precision, int n);
+cudaError_t launch_pass_chain(int precision, const PassParams& p, cudaStream_t stream);
 
 // Stage-1 shared basis. Every walk of an instance starts from the uniform
 // state psi0 and its first stage applies the same operator H~ (one gamma and
@@ -251,8 +260,17 @@ struct RealChainParams {
   float psi0;
   const float* hp;
   float gamma, scale;
+  // Chain launch only (launch_real_chain; tiling, first, bin and bout are
+  // not read): passes j = 0 .. K-1 of terms r = R - j, pass j writing b_r to
+  // out_base[j & 1] + (j >> 1) * out_stride floats.
+  int K, R;
+  float* out_base[2];
+  long long out_stride;
 };
 cudaError_t launch_real_pass(const RealChainParams& p, cudaStream_t stream);
+// The whole chain in one launch: a cluster of 2^(n-L) CTAs with cluster
+// barriers between the passes, L = chain_tile_log(0, n) (FP32).
+cudaError_t launch_real_chain(const RealChainParams& p, cudaStream_t stream);
 // v = e_{E_loc} as a real vector of 2^n floats.
 cudaError_t launch_unit_eloc_real(float* v, int n, const DiagOut* diag, cudaStream_t stream);
 cudaError_t launch_combine(int precision, const CombineParams& p,

@@ -26,6 +26,7 @@
 //    its vectors once as coalesced tile rows (see the grid-path section).
 #include <stdlib.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -512,11 +513,13 @@ constexpr int pass_min_blocks() {
 // pass) at the cost of 16 B of shared memory per amplitude. Shapes with P in
 // registers (8 pairs per thread) only, where it still leaves two CTAs per
 // SM at the 2^12 tile.
+// pass_tile is one CTA's share of one pass: term r of walk W in tiling
+// `tiling` (1 or 2), on the CTA's tile `bx` (the x block index: tile and,
+// with CL > 0, cluster rank).
 template <typename R, int LT, int CL, int TB, bool LS = false, bool TMA = false,
           bool COMP = false, bool X2 = false>
-__global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
-                                  pass_min_blocks<LT, TB, sizeof(R) == 4, CL>())
-    pass_kernel(PassParams p) {
+__device__ __forceinline__ void pass_tile(const PassParams& p, const PassWalk& W, const int r,
+                                          const int tiling, const unsigned bx) {
   using S = PassShape<LT, TB>;
   constexpr int RP = S::kRP, LOGT = S::kLogT, T = S::kThreads;
   constexpr bool kStageP = S::kStageP || TMA;
@@ -527,8 +530,6 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ double s_red[32];
   __shared__ __align__(8) unsigned long long tma_bar;
-  const PassWalk& W = p.walk[blockIdx.y];
-  if (!W.active) return;
   const int n = p.n, a = p.a;
   const int tid = threadIdx.x;
   R* sx = reinterpret_cast<R*>(smem_raw);  // exchange tile: 2^LT complex
@@ -538,22 +539,22 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   // X2: b_r's exchange tile, after the staged D
   R* sx2 = X2 ? reinterpret_cast<R*>(sd + S::kPairs) : sx;
   // Global amplitude index of register pair j: g0 + j * gstride (32-bit: n <= 30).
-  // For a 1-D cluster the cluster rank is blockIdx.x mod 2^CL.
-  const unsigned rank = CL > 0 ? (blockIdx.x & ((1u << CL) - 1u)) : 0u;
+  // For a 1-D cluster the cluster rank is bx mod 2^CL.
+  const unsigned rank = CL > 0 ? (bx & ((1u << CL) - 1u)) : 0u;
   const int nu = n - (2 * LL - a) > 0 ? n - (2 * LL - a) : 0;
   // Launch order of the tiles: the tile bits of the nu axes read from global
   // memory come first, so that the tiles whose amplitudes a tile reads are
   // processed at about the same time and those reads hit L2. In T1 they are
   // the lowest tile bits already; in T2 they are the top nu of the n - LL
   // tile bits, rotated down here.
-  unsigned tile = blockIdx.x >> CL;
-  if (p.tiling == 2 && nu > 0) {
+  unsigned tile = bx >> CL;
+  if (tiling == 2 && nu > 0) {
     const int tb = n - LL;
     tile = ((tile & ((1u << nu) - 1u)) << (tb - nu)) | (tile >> nu);
   }
   const unsigned pos0 = (rank << LT) | (2u * tid);  // tile position of pair 0
   unsigned g0, gstride;
-  if (p.tiling == 1) {
+  if (tiling == 1) {
     g0 = (tile << LL) | pos0;
     gstride = 1u << (LOGT + 1);
   } else {
@@ -570,14 +571,14 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   R* __restrict__ part = reinterpret_cast<R*>(W.part);
   const R* __restrict__ psi = reinterpret_cast<const R*>(W.psi);
   const float* __restrict__ hp = W.hp;
-  const int r = W.r, K = W.K;
+  const int K = W.K;
   const bool first = r == K - 1;
   const bool uni = W.psi_uniform;
   // Finish axes (tile bits): T1 -> [a, min(L, n-L+a)), T2 -> [max(2L-n, a), L)
   // with L = LL; axes [LL, LL+nu) are in neither tiling and come from global
   // memory.
-  const int fb0 = p.tiling == 1 ? a : max(2 * LL - n, a);
-  const int fb1 = p.tiling == 1 ? min(LL, n - LL + a) : LL;
+  const int fb0 = tiling == 1 ? a : max(2 * LL - n, a);
+  const int fb1 = tiling == 1 ? min(LL, n - LL + a) : LL;
   // Partners along the rank bits [LT, LL) that lie in [q0, q1): all of a
   // pair's remote loads are issued together (before the local partner sums,
   // which hide their latency) and added afterwards.
@@ -600,10 +601,10 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
 
   Pair<R> va[RP];  // b_{r+1}
   Pair<R> pv[kStageP ? 1 : RP];  // P_r when kept in registers
-  const bool bulk = TMA && p.tiling == 1;
+  const bool bulk = TMA && tiling == 1;
   if (bulk) {
     // The tile as rows of contiguous amplitudes (T1: one row of 2^LT).
-    const int row_log = p.tiling == 1 ? LT : a;
+    const int row_log = tiling == 1 ? LT : a;
     const unsigned rows = 1u << (LT - row_log);
     const unsigned row_amps = 1u << row_log;
     const unsigned vec_bytes = row_amps * 2u * (unsigned)sizeof(R);
@@ -617,7 +618,7 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
       }
       __syncwarp();
       for (unsigned k = tid; k < rows; k += 32) {
-        const unsigned g = p.tiling == 1 ? (tile << LT)
+        const unsigned g = tiling == 1 ? (tile << LT)
                                          : ((tile << a) | (k << (n - LT + a)));
         const unsigned pos = k * row_amps;
         if (!first) {
@@ -721,7 +722,7 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
       nrm += (double)v.x * v.x + (double)v.y * v.y + (double)v.z * v.z + (double)v.w * v.w;
     }
     const double sum = block_sum<R>(nrm, s_red);
-    if (tid == 0) W.norm_part[blockIdx.x] = sum;
+    if (tid == 0) W.norm_part[bx] = sum;
     if constexpr (CL > 0) cluster_barrier();  // peers may still read sx
     return;
   }
@@ -756,6 +757,38 @@ __global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
   }
   // A CTA's shared memory must outlive its peers' reads of it.
   if constexpr (CL > 0) cluster_barrier();
+}
+
+// One pass (term W.r) for each walk of the launch: blockIdx.y is the walk,
+// blockIdx.x the tile (and cluster rank).
+template <typename R, int LT, int CL, int TB, bool LS = false, bool TMA = false,
+          bool COMP = false, bool X2 = false>
+__global__ void __launch_bounds__(PassShape<LT, TB>::kThreads,
+                                  pass_min_blocks<LT, TB, sizeof(R) == 4, CL>())
+    pass_kernel(PassParams p) {
+  const PassWalk& W = p.walk[blockIdx.y];
+  if (!W.active) return;
+  pass_tile<R, LT, CL, TB, LS, TMA, COMP, X2>(p, W, W.r, p.tiling, blockIdx.x);
+}
+
+// Chain launch (small n, no axis read from global memory): a thread-block
+// cluster of 2^(n-LT) CTAs, one per tile, runs all K terms of one walk-stage
+// (blockIdx.y the walk, b and P updated in place), passes r = K-1 .. 0 in
+// tilings 1 (even r) and 2 (odd r). A cluster barrier (arrive.release /
+// wait.acquire at cluster scope, which orders the global-memory writes of
+// every thread of the cluster) separates consecutive passes, so that each
+// pass reads the tiles its peers wrote in the one before. One launch
+// replaces K single-pass launches; the arithmetic is the same.
+template <typename R, int LT>
+__global__ void __launch_bounds__(PassShape<LT>::kThreads,
+                                  pass_min_blocks<LT, kPassThreads, sizeof(R) == 4, 0>())
+    pass_chain_kernel(PassParams p) {
+  const PassWalk& W = p.walk[blockIdx.y];
+  if (!W.active) return;  // every CTA of the cluster has the same walk
+  for (int r = W.K - 1; r >= 0; r--) {
+    pass_tile<R, LT, 0, kPassThreads>(p, W, r, (r & 1) ? 2 : 1, blockIdx.x);
+    if (r > 0) cluster_barrier();
+  }
 }
 
 // The shared bases are streamed (hundreds of MB per walk group at n = 20)
@@ -981,8 +1014,13 @@ __device__ __forceinline__ unsigned long long f2u(float2 f) {
   return v;
 }
 
+// real_tile is one CTA's share of one real pass: tiling `tiling`, the
+// chain's first pass when `first`, b_{r+1} read from `bin_` and b_r written
+// to `bout_`, on the CTA's tile `bx`.
 template <int LT>
-__global__ void __launch_bounds__(RealShape<LT>::kThreads) real_pass_kernel(RealChainParams p) {
+__device__ __forceinline__ void real_tile(const RealChainParams& p, const int tiling,
+                                          const bool first, const float* bin_, float* bout_,
+                                          const unsigned bx) {
   using S = RealShape<LT>;
   constexpr int RP = S::kRP, LOGT = S::kLogT, T = S::kThreads;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -991,14 +1029,14 @@ __global__ void __launch_bounds__(RealShape<LT>::kThreads) real_pass_kernel(Real
   float2* sd = reinterpret_cast<float2*>(sx2 + S::kPairs);                    // staged D
   const int n = p.n, a = p.a, tid = threadIdx.x;
   const int nu = n - (2 * LT - a) > 0 ? n - (2 * LT - a) : 0;
-  unsigned tile = blockIdx.x;
-  if (p.tiling == 2 && nu > 0) {
+  unsigned tile = bx;
+  if (tiling == 2 && nu > 0) {
     const int tb = n - LT;
     tile = ((tile & ((1u << nu) - 1u)) << (tb - nu)) | (tile >> nu);
   }
   const unsigned pos0 = 2u * tid;
   unsigned g0, gstride;
-  if (p.tiling == 1) {
+  if (tiling == 1) {
     g0 = (tile << LT) | pos0;
     gstride = 1u << (LOGT + 1);
   } else {
@@ -1006,17 +1044,17 @@ __global__ void __launch_bounds__(RealShape<LT>::kThreads) real_pass_kernel(Real
     g0 = (pos0 & amask) | (tile << a) | ((pos0 >> a) << (n - LT + a));
     gstride = 1u << (LOGT + 1 + n - LT);
   }
-  const int fb0 = p.tiling == 1 ? a : max(2 * LT - n, a);
-  const int fb1 = p.tiling == 1 ? min(LT, n - LT + a) : LT;
+  const int fb0 = tiling == 1 ? a : max(2 * LT - n, a);
+  const int fb1 = tiling == 1 ? min(LT, n - LT + a) : LT;
   const float* __restrict__ hp = p.hp;
-  const float* __restrict__ bin = p.bin;
+  const float* __restrict__ bin = bin_;
   float* __restrict__ part = p.part;
 #pragma unroll
   for (int j = 0; j < RP; j++) cp_async8(sd + (j * T + tid), hp + g0 + j * gstride);
   unsigned long long va[RP], vb[RP];
   const float am = 2.0f / p.scale;
   const float gamma = p.gamma;
-  if (p.first) {
+  if (first) {
 #pragma unroll
     for (int j = 0; j < RP; j++) {
       va[j] = 0ull;
@@ -1056,7 +1094,7 @@ __global__ void __launch_bounds__(RealShape<LT>::kThreads) real_pass_kernel(Real
   }
 #pragma unroll
   for (int j = 0; j < RP; j++)
-    *reinterpret_cast<unsigned long long*>(p.bout + g0 + j * gstride) = vb[j];
+    *reinterpret_cast<unsigned long long*>(bout_ + g0 + j * gstride) = vb[j];
   // Start P_{r-1} = a (D b_r - gamma X_Z b_r) - b_{r+1} over all tile axes.
 #pragma unroll
   for (int j = 0; j < RP; j++) sx2[tid | (j << LOGT)] = vb[j];
@@ -1070,6 +1108,30 @@ __global__ void __launch_bounds__(RealShape<LT>::kThreads) real_pass_kernel(Real
     const float2 out = make_float2(fmaf(am, fmaf(d.x, b.x, -gamma * s.x), 0.0f - b1.x),
                                    fmaf(am, fmaf(d.y, b.y, -gamma * s.y), 0.0f - b1.y));
     *reinterpret_cast<unsigned long long*>(part + g0 + j * gstride) = f2u(out);
+  }
+}
+
+// One real pass (p.tiling, p.first, p.bin -> p.bout); blockIdx.x is the tile.
+template <int LT>
+__global__ void __launch_bounds__(RealShape<LT>::kThreads) real_pass_kernel(RealChainParams p) {
+  real_tile<LT>(p, p.tiling, p.first != 0, p.bin, p.bout, blockIdx.x);
+}
+
+// Chain launch of a whole real chain (small n, no axis read from global
+// memory): a thread-block cluster of 2^(n-LT) CTAs, one per tile, runs the
+// passes j = 0 .. K-1 (term r = R - j, tiling 2 for odd r), pass j writing
+// b_r to out_base[j & 1] + (j >> 1) out_stride and reading b_{r+1} from the
+// previous pass's output; cluster barriers separate the passes (see
+// pass_chain_kernel).
+template <int LT>
+__global__ void __launch_bounds__(RealShape<LT>::kThreads) real_chain_kernel(RealChainParams p) {
+  for (int j = 0; j < p.K; j++) {
+    const int r = p.R - j;
+    const float* bin =
+        j > 0 ? p.out_base[(j - 1) & 1] + (size_t)((j - 1) >> 1) * (size_t)p.out_stride : nullptr;
+    float* bout = p.out_base[j & 1] + (size_t)(j >> 1) * (size_t)p.out_stride;
+    real_tile<LT>(p, (r & 1) ? 2 : 1, j == 0, bin, bout, blockIdx.x);
+    if (j + 1 < p.K) cluster_barrier();
   }
 }
 
@@ -1360,6 +1422,116 @@ cudaError_t launch_pass(int precision, const PassParams& p,
                         : launch_pass_t<double>(p, stream);
 }
 
+namespace {
+// Chain launches: a cluster of `tiles` CTAs per walk (non-portable sizes
+// above 8 are allowed: the attribute is set on every opt-in).
+template <typename R, int LT>
+cudaLaunchConfig_t chain_config(int tiles, int count, size_t* smem, cudaLaunchAttribute* attr) {
+  using S = PassShape<LT>;
+  *smem = S::template smem<R>();
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)tiles, (unsigned)count, 1);
+  cfg.blockDim = dim3(S::kThreads, 1, 1);
+  cfg.dynamicSmemBytes = *smem;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = (unsigned)tiles;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+template <typename R, int LT>
+cudaError_t launch_chain_lt(const PassParams& p, cudaStream_t stream) {
+  size_t smem = 0;
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = chain_config<R, LT>(1 << (p.n - LT), p.count, &smem, attr);
+  cfg.stream = stream;
+  cudaError_t e = ensure_smem_optin((const void*)pass_chain_kernel<R, LT>, smem, true);
+  if (e != cudaSuccess) return e;
+  return cudaLaunchKernelEx(&cfg, pass_chain_kernel<R, LT>, p);
+}
+
+// Whether clusters of `tiles` CTAs of the chain kernel can be resident.
+template <typename R, int LT>
+bool chain_fits(int tiles) {
+  size_t smem = 0;
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = chain_config<R, LT>(tiles, 1, &smem, attr);
+  if (ensure_smem_optin((const void*)pass_chain_kernel<R, LT>, smem, true) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  int clusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&clusters, pass_chain_kernel<R, LT>, &cfg) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  return clusters > 0;
+}
+
+template <typename R>
+bool chain_fits_t(int L, int tiles) {
+  switch (L) {
+    case 9: return chain_fits<R, 9>(tiles);
+    case 10: return chain_fits<R, 10>(tiles);
+    case 11: return chain_fits<R, 11>(tiles);
+    case 12:
+      if constexpr (sizeof(R) == 4) return chain_fits<R, 12>(tiles);
+      return false;
+    default: return false;
+  }
+}
+}  // namespace
+
+int chain_tile_log(int precision, int n) {
+  const char* e = getenv("MQW_CHAIN");
+  if (e && atoi(e) == 0) return 0;
+  const int cap = precision == 0 ? 12 : 11;
+  // Up to 16 tiles per walk (the largest cluster), none of its axes read
+  // from global memory (2L - 4 >= n), and at least the single-pass tile.
+  // MQW_CHAIN_TILE_LOG asks for wider tiles (fewer CTAs per walk).
+  int L = std::max(pass_geom(precision, n).L, n - 4);
+  if (const char* t = getenv("MQW_CHAIN_TILE_LOG")) L = std::max(L, std::min(atoi(t), cap));
+  if (L < 9 || L > cap || L > n || 2 * L - 4 < n) return 0;
+  const int tiles = 1 << (n - L);
+  // Residency of a cluster of that size, probed once per (device, shape).
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, bool> fits;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  std::lock_guard<std::mutex> lk(mu);
+  const auto key = std::make_pair(dev, precision * 64 + L * 4 + (n - L));
+  auto it = fits.find(key);
+  if (it == fits.end())
+    it = fits.emplace(key, precision == 0 ? chain_fits_t<float>(L, tiles)
+                                          : chain_fits_t<double>(L, tiles)).first;
+  return it->second ? L : 0;
+}
+
+cudaError_t launch_pass_chain(int precision, const PassParams& p, cudaStream_t stream) {
+  const int cap = precision == 0 ? 12 : 11;
+  if (p.a != 4 || p.L < 9 || p.L > cap || p.L > p.n || p.n - p.L > 4 || 2 * p.L - 4 < p.n ||
+      p.C != 0 || p.comp || p.count < 1 || p.count > kMaxGroup)
+    return cudaErrorInvalidValue;
+  if (precision == 0) {
+    switch (p.L) {
+      case 9: return launch_chain_lt<float, 9>(p, stream);
+      case 10: return launch_chain_lt<float, 10>(p, stream);
+      case 11: return launch_chain_lt<float, 11>(p, stream);
+      case 12: return launch_chain_lt<float, 12>(p, stream);
+      default: return cudaErrorInvalidValue;
+    }
+  }
+  switch (p.L) {
+    case 9: return launch_chain_lt<double, 9>(p, stream);
+    case 10: return launch_chain_lt<double, 10>(p, stream);
+    case 11: return launch_chain_lt<double, 11>(p, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
 template <bool kProject, typename Params>
 void launch_recombine(const Params& p, cudaStream_t stream) {
   const unsigned blocks = (unsigned)((size_t)1 << (p.n - p.L));
@@ -1430,6 +1602,45 @@ cudaError_t launch_real_lt(const RealChainParams& p, cudaStream_t stream) {
   return cudaGetLastError();
 }
 }  // namespace
+
+namespace {
+template <int LT>
+cudaError_t launch_real_chain_lt(const RealChainParams& p, cudaStream_t stream) {
+  using S = RealShape<LT>;
+  const size_t smem = S::smem();
+  cudaError_t e = ensure_smem_optin((const void*)real_chain_kernel<LT>, smem, true);
+  if (e != cudaSuccess) return e;
+  const unsigned tiles = 1u << (p.n - LT);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(tiles, 1, 1);
+  cfg.blockDim = dim3(S::kThreads, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = tiles;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, real_chain_kernel<LT>, p);
+}
+}  // namespace
+
+cudaError_t launch_real_chain(const RealChainParams& p, cudaStream_t stream) {
+  if (p.n < 6 || p.n > kMaxN || p.L < 9 || p.L > 12 || p.L > p.n || p.n - p.L > 4 ||
+      2 * p.L - 4 < p.n || p.a != 4 || p.K < 1 || p.R < p.K || !p.out_base[0] ||
+      (p.K > 1 && !p.out_base[1]) || p.out_stride < ((long long)1 << p.n) || !p.part || !p.hp ||
+      !(p.scale > 0.0f) || (!p.start_uniform && !p.start))
+    return cudaErrorInvalidValue;
+  switch (p.L) {
+    case 9: return launch_real_chain_lt<9>(p, stream);
+    case 10: return launch_real_chain_lt<10>(p, stream);
+    case 11: return launch_real_chain_lt<11>(p, stream);
+    case 12: return launch_real_chain_lt<12>(p, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
 
 cudaError_t launch_real_pass(const RealChainParams& p, cudaStream_t stream) {
   if (p.n < 6 || p.n > kMaxN || p.L < 6 || p.L > 13 || p.L > p.n || p.a != 4 ||

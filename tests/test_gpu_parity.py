@@ -709,6 +709,9 @@ def test_real_chains_match_complex_chains(ctx, orc, mqw, monkeypatch, n, m, samp
     three axes of every pass are read from global memory."""
     raw = orc.sk_instances(n, 1, 5300 + n)
     monkeypatch.setenv("MQW_STAGE2_BASIS", "1")
+    # one launch per pass on both kernels (the same tiles; chain launches
+    # are compared with single-pass launches in their own test)
+    monkeypatch.setenv("MQW_CHAIN", "0")
     shape = {"tile_log": tile} if tile else {}
 
     def run(real):
@@ -723,3 +726,37 @@ def test_real_chains_match_complex_chains(ctx, orc, mqw, monkeypatch, n, m, samp
     assert np.array_equal(on, off)
     r64 = ctx.run_problems(n, m, raw, samples=samples, precision="fp64", graph=0)
     assert abs(float(np.mean(on)) - r64["p"][0]) <= 1e-5
+
+
+@pytest.mark.parametrize("n,m,precision", [(13, 3, "fp32"), (13, 2, "fp64"), (14, 3, "fp32"),
+                                           (15, 4, "fp32"), (16, 3, "fp32"), (15, 2, "fp64")])
+def test_chain_launch_matches_single_pass_launches(ctx, orc, mqw, monkeypatch, n, m, precision):
+    """Small n: every term of a walk-stage in one launch (a thread-block
+    cluster of up to 16 CTAs per walk, cluster barriers between the passes)
+    against one launch per term (MQW_CHAIN=0), with a fraction of the
+    launches. At n = 13 both use 16 tiles of 2^9 per walk, so the passes are
+    the same arithmetic in the same order and every per-sample P is
+    identical; above it the chain launch uses wider tiles (at most 16 per
+    walk) than the single-pass launches, which changes the order of the
+    partner sums, so per-sample P agree to FP32 (FP64) rounding. The grid
+    path is forced (resident_max_n = -1) so that n = 13 takes it too."""
+    raw = orc.sk_instances(n, 2, 6100 + n)
+
+    def run(chain):
+        monkeypatch.setenv("MQW_CHAIN", "1" if chain else "0")
+        plan = mqw.Plan(ctx, n, m, raw, samples=8, graph=0, precision=precision,
+                        resident_max_n=-1)
+        plan.execute()
+        out = plan.results(per_sample=True)["p_sample"]
+        launches = plan.stats()["launches"]
+        plan.close()
+        return out, launches
+
+    (on, l_on), (off, l_off) = run(True), run(False)
+    if n == 13:
+        assert np.array_equal(on, off)
+    else:
+        assert np.abs(on - off).max() <= (1e-7 if precision == "fp32" else 1e-13)
+    assert l_on * 4 < l_off, (l_on, l_off)
+    r64 = ctx.run_problems(n, m, raw, samples=8, precision="fp64", graph=0)
+    assert np.abs(np.mean(on, axis=1) - r64["p"]).max() <= 1e-5
