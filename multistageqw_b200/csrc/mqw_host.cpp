@@ -127,6 +127,7 @@ struct mqw_ctx {
   // output, and the coefficient matrices (one instance at a time).
   DevMem s2y, s2psi, s2c;
   DevMem s2chain;  // chain slots of the build-ahead (4 complex vectors)
+  DevMem s2part;   // partial P of each batched product-basis chain (small n)
   // Bumped whenever a shared scratch buffer is reallocated: a plan's captured
   // graph holds the old addresses and is re-captured when this changes.
   unsigned long long scratch_gen = 1;
@@ -265,6 +266,7 @@ struct mqw_plan {
   // Per-buffer sizes (floats) of ctx->s2y / s2psi / s2c: one buffer set, two
   // with the build-ahead.
   size_t s2y_floats = 0, s2psi_floats = 0, s2c_floats = 0;
+  size_t s2part_floats = 0;  // ctx->s2part per buffer set (0: no batched chains)
   DevMem d_unit;
   int unit_len = 0;
   // CUDA graph of the whole device pipeline, replayed by later executes.
@@ -863,12 +865,11 @@ mqw_status issue_chain(mqw_plan& P, const ResidentWalk& w0, int stage, int K,
       for (int j = 0; j < K && affine; j++)
         affine = out_of(j) == (j & 1 ? base1 : base0) + (size_t)(j >> 1) * (size_t)stride;
       if (affine) {
-        RealChainParams rp{};
+        RealChainBatch rb{};
+        RealChainParams& rp = rb.p;
         rp.n = w0.n;
         rp.L = cL;
         rp.a = geo.a;
-        rp.part = static_cast<float*>(S.part);
-        rp.start = S.start_real;
         rp.start_uniform = S.uniform ? 1 : 0;
         rp.psi0 = (float)(1.0 / std::sqrt((double)N));
         rp.hp = P.d_hp.as<float>() + w0.hp_off;
@@ -876,10 +877,10 @@ mqw_status issue_chain(mqw_plan& P, const ResidentWalk& w0, int stage, int K,
         rp.scale = P.onenorm[job];
         rp.K = K;
         rp.R = R;
-        rp.out_base[0] = base0;
-        rp.out_base[1] = base1;
         rp.out_stride = stride;
-        CK(launch_real_chain(rp, stream));
+        rb.chains = 1;
+        rb.chain[0] = RealChainDesc{S.start_real, static_cast<float*>(S.part), {base0, base1}};
+        CK(launch_real_chain(rb, stream));
         if (P.counting) {
           P.stats.launches++;
           P.stats.term_launches++;
@@ -1024,7 +1025,50 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
     mqw_status s = extra(xl == 0 ? stream : lane_st[xl]);
     if (s != MQW_OK) return s;
   }
-  for (int j = 0; j < Kb; j++) {
+  // Small n: all Kb chains in chain launches of up to kMaxChainBatch chains
+  // each (a cluster per chain, each with its own partial P) on the launching
+  // stream, instead of one chain after another on each lane.
+  const int cL = use_real_chains(P, geo) && P.s2part_floats >= (size_t)Kb * N
+                     ? chain_tile_log(0, n) : 0;
+  auto chain_out = [&](int j, int k) {
+    const int h = (j + k) & 1;
+    return Y + ((size_t)(h ? lay.rows(0) : 0) + lay.index(j, k)) * N;
+  };
+  bool batched = cL > 0 && K2 > 0;
+  for (int j = 0; j < Kb && batched; j++)
+    for (int k = 2; k < K2 && batched; k++)
+      batched = chain_out(j, k) == chain_out(j, k - 2) + N;
+  if (batched) {
+    const int job = w0.stage_desc_off + 1;
+    float* part = ctx->s2part.as<float>() + (size_t)buf * P.s2part_floats;
+    for (int c0 = 0; c0 < Kb; c0 += kMaxChainBatch) {
+      RealChainBatch rb{};
+      RealChainParams& rp = rb.p;
+      rp.n = n;
+      rp.L = cL;
+      rp.a = geo.a;
+      rp.psi0 = (float)(1.0 / std::sqrt((double)N));
+      rp.hp = P.d_hp.as<float>() + w0.hp_off;
+      rp.gamma = P.jobs[job].gamma;
+      rp.scale = P.onenorm[job];
+      rp.K = K2;
+      rp.R = K2 + (K2 & 1);
+      rp.out_stride = (long long)N;
+      rb.chains = std::min(kMaxChainBatch, Kb - c0);
+      for (int c = 0; c < rb.chains; c++) {
+        const int j = c0 + c;
+        rb.chain[c] = RealChainDesc{basis + (size_t)j * N, part + (size_t)j * N,
+                                    {chain_out(j, 0), K2 > 1 ? chain_out(j, 1) : nullptr}};
+      }
+      CK(launch_real_chain(rb, stream));
+      if (P.counting) {
+        P.stats.launches++;
+        P.stats.term_launches++;
+        P.stats.aux_bytes += (double)N * 20.0 * K2 * rb.chains;
+      }
+    }
+  }
+  for (int j = 0; j < Kb && !batched; j++) {
     const int lane = j % lanes;
     cudaStream_t st = lane == 0 ? stream : lane_st[lane];
     char* base = builder ? ctx->s2chain.as<char>() + (size_t)lane * 4 * N * 8
@@ -1527,7 +1571,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     // whenever it fits). With the build-ahead its buffers are doubled.
     P.s2_k2.clear();
     P.s2_walks = 0;
-    size_t s2y_b = 0, s2psi_n = 0, s2c_b = 0;
+    size_t s2y_b = 0, s2psi_n = 0, s2c_b = 0, s2part_n = 0;
     {
       const char* env = getenv("MQW_STAGE2_BASIS");
       const int mode = env ? atoi(env) : -1;
@@ -1550,6 +1594,8 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
         s2c_b = std::max(s2c_b, ((size_t)k1 * K2 + 16) * (size_t)((wpi + 127) / 128 * 128) * 4);
         s2c_b = std::max(s2c_b, s2_tc_coef_floats(wpi, S2Layout{k1, K2}) * 4);
         rmax = std::max(rmax, K2 + (K2 & 1));
+        // small n: the product basis's chains run batched, one partial P each
+        if (chain_tile_log(0, n)) s2part_n = std::max(s2part_n, (size_t)k1 * N);
       }
     }
     if (!P.s2_k2.empty()) {
@@ -1562,6 +1608,8 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       CK(ctx->grow(ctx->s2psi, nb * P.s2psi_floats * 4));
       CK(ctx->grow(ctx->s2c, nb * s2c_b));
       if (ahead) CK(ctx->grow(ctx->s2chain, (size_t)kMaxLanes * 4 * s2psi_n * 8));
+      P.s2part_floats = s2part_n;
+      if (s2part_n) CK(ctx->grow(ctx->s2part, nb * s2part_n * 4));
     }
     if (basis_b) {
       CK(ctx->grow(ctx->basis, basis_b));

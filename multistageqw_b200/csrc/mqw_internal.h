@@ -260,17 +260,29 @@ struct RealChainParams {
   float psi0;
   const float* hp;
   float gamma, scale;
-  // Chain launch only (launch_real_chain; tiling, first, bin and bout are
-  // not read): passes j = 0 .. K-1 of terms r = R - j, pass j writing b_r to
+  // Chain launch only (launch_real_chain; tiling, first, bin, bout, part
+  // and start are taken per chain from RealChainDesc): passes j = 0 .. K-1
+  // of terms r = R - j, pass j writing b_r to
   // out_base[j & 1] + (j >> 1) * out_stride floats.
   int K, R;
-  float* out_base[2];
   long long out_stride;
 };
 cudaError_t launch_real_pass(const RealChainParams& p, cudaStream_t stream);
-// The whole chain in one launch: a cluster of 2^(n-L) CTAs with cluster
-// barriers between the passes, L = chain_tile_log(0, n) (FP32).
-cudaError_t launch_real_chain(const RealChainParams& p, cudaStream_t stream);
+// Whole chains in one launch: per chain a cluster of 2^(n-L) CTAs with
+// cluster barriers between the passes, L = chain_tile_log(0, n) (FP32);
+// the chains of a launch share n, K, R, the operator and out_stride.
+constexpr int kMaxChainBatch = 64;
+struct RealChainDesc {
+  const float* start;   // v (unused when start_uniform)
+  float* part;          // the chain's own partial P (real, 2^n floats)
+  float* out_base[2];   // outputs of even / odd j
+};
+struct RealChainBatch {
+  RealChainParams p;
+  int chains;
+  RealChainDesc chain[kMaxChainBatch];
+};
+cudaError_t launch_real_chain(const RealChainBatch& b, cudaStream_t stream);
 // v = e_{E_loc} as a real vector of 2^n floats.
 cudaError_t launch_unit_eloc_real(float* v, int n, const DiagOut* diag, cudaStream_t stream);
 cudaError_t launch_combine(int precision, const CombineParams& p,

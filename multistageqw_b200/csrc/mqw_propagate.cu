@@ -1016,11 +1016,12 @@ __device__ __forceinline__ unsigned long long f2u(float2 f) {
 
 // real_tile is one CTA's share of one real pass: tiling `tiling`, the
 // chain's first pass when `first`, b_{r+1} read from `bin_` and b_r written
-// to `bout_`, on the CTA's tile `bx`.
+// to `bout_`, the partial P in place at `part_`, the start vector `start_`,
+// on the CTA's tile `bx`.
 template <int LT>
 __device__ __forceinline__ void real_tile(const RealChainParams& p, const int tiling,
                                           const bool first, const float* bin_, float* bout_,
-                                          const unsigned bx) {
+                                          float* part_, const float* start_, const unsigned bx) {
   using S = RealShape<LT>;
   constexpr int RP = S::kRP, LOGT = S::kLogT, T = S::kThreads;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1048,7 +1049,7 @@ __device__ __forceinline__ void real_tile(const RealChainParams& p, const int ti
   const int fb1 = tiling == 1 ? min(LT, n - LT + a) : LT;
   const float* __restrict__ hp = p.hp;
   const float* __restrict__ bin = bin_;
-  float* __restrict__ part = p.part;
+  float* __restrict__ part = part_;
 #pragma unroll
   for (int j = 0; j < RP; j++) cp_async8(sd + (j * T + tid), hp + g0 + j * gstride);
   unsigned long long va[RP], vb[RP];
@@ -1059,7 +1060,7 @@ __device__ __forceinline__ void real_tile(const RealChainParams& p, const int ti
     for (int j = 0; j < RP; j++) {
       va[j] = 0ull;
       vb[j] = p.start_uniform ? f2u(make_float2(p.psi0, p.psi0))
-                              : *reinterpret_cast<const unsigned long long*>(p.start + g0 + j * gstride);
+                              : *reinterpret_cast<const unsigned long long*>(start_ + g0 + j * gstride);
     }
     cp_async_wait_all();
   } else {
@@ -1114,23 +1115,26 @@ __device__ __forceinline__ void real_tile(const RealChainParams& p, const int ti
 // One real pass (p.tiling, p.first, p.bin -> p.bout); blockIdx.x is the tile.
 template <int LT>
 __global__ void __launch_bounds__(RealShape<LT>::kThreads) real_pass_kernel(RealChainParams p) {
-  real_tile<LT>(p, p.tiling, p.first != 0, p.bin, p.bout, blockIdx.x);
+  real_tile<LT>(p, p.tiling, p.first != 0, p.bin, p.bout, p.part, p.start, blockIdx.x);
 }
 
-// Chain launch of a whole real chain (small n, no axis read from global
-// memory): a thread-block cluster of 2^(n-LT) CTAs, one per tile, runs the
-// passes j = 0 .. K-1 (term r = R - j, tiling 2 for odd r), pass j writing
-// b_r to out_base[j & 1] + (j >> 1) out_stride and reading b_{r+1} from the
-// previous pass's output; cluster barriers separate the passes (see
-// pass_chain_kernel).
+// Chain launch of whole real chains (small n, no axis read from global
+// memory): per chain (blockIdx.y; b.chain[] gives its start vector, partial
+// P and outputs) a thread-block cluster of 2^(n-LT) CTAs, one per tile, runs
+// the passes j = 0 .. K-1 (term r = R - j, tiling 2 for odd r), pass j
+// writing b_r to out_base[j & 1] + (j >> 1) out_stride and reading b_{r+1}
+// from the previous pass's output; cluster barriers separate the passes (see
+// pass_chain_kernel). The chains of a launch share n, K, R and the operator.
 template <int LT>
-__global__ void __launch_bounds__(RealShape<LT>::kThreads) real_chain_kernel(RealChainParams p) {
+__global__ void __launch_bounds__(RealShape<LT>::kThreads) real_chain_kernel(RealChainBatch b) {
+  const RealChainParams& p = b.p;
+  const RealChainDesc& c = b.chain[blockIdx.y];
   for (int j = 0; j < p.K; j++) {
     const int r = p.R - j;
     const float* bin =
-        j > 0 ? p.out_base[(j - 1) & 1] + (size_t)((j - 1) >> 1) * (size_t)p.out_stride : nullptr;
-    float* bout = p.out_base[j & 1] + (size_t)(j >> 1) * (size_t)p.out_stride;
-    real_tile<LT>(p, (r & 1) ? 2 : 1, j == 0, bin, bout, blockIdx.x);
+        j > 0 ? c.out_base[(j - 1) & 1] + (size_t)((j - 1) >> 1) * (size_t)p.out_stride : nullptr;
+    float* bout = c.out_base[j & 1] + (size_t)(j >> 1) * (size_t)p.out_stride;
+    real_tile<LT>(p, (r & 1) ? 2 : 1, j == 0, bin, bout, c.part, c.start, blockIdx.x);
     if (j + 1 < p.K) cluster_barrier();
   }
 }
@@ -1605,14 +1609,14 @@ cudaError_t launch_real_lt(const RealChainParams& p, cudaStream_t stream) {
 
 namespace {
 template <int LT>
-cudaError_t launch_real_chain_lt(const RealChainParams& p, cudaStream_t stream) {
+cudaError_t launch_real_chain_lt(const RealChainBatch& p, cudaStream_t stream) {
   using S = RealShape<LT>;
   const size_t smem = S::smem();
   cudaError_t e = ensure_smem_optin((const void*)real_chain_kernel<LT>, smem, true);
   if (e != cudaSuccess) return e;
-  const unsigned tiles = 1u << (p.n - LT);
+  const unsigned tiles = 1u << (p.p.n - LT);
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(tiles, 1, 1);
+  cfg.gridDim = dim3(tiles, (unsigned)p.chains, 1);
   cfg.blockDim = dim3(S::kThreads, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = stream;
@@ -1627,17 +1631,24 @@ cudaError_t launch_real_chain_lt(const RealChainParams& p, cudaStream_t stream) 
 }
 }  // namespace
 
-cudaError_t launch_real_chain(const RealChainParams& p, cudaStream_t stream) {
+cudaError_t launch_real_chain(const RealChainBatch& b, cudaStream_t stream) {
+  const RealChainParams& p = b.p;
   if (p.n < 6 || p.n > kMaxN || p.L < 9 || p.L > 12 || p.L > p.n || p.n - p.L > 4 ||
-      2 * p.L - 4 < p.n || p.a != 4 || p.K < 1 || p.R < p.K || !p.out_base[0] ||
-      (p.K > 1 && !p.out_base[1]) || p.out_stride < ((long long)1 << p.n) || !p.part || !p.hp ||
-      !(p.scale > 0.0f) || (!p.start_uniform && !p.start))
+      2 * p.L - 4 < p.n || p.a != 4 || p.K < 1 || p.R < p.K ||
+      p.out_stride < ((long long)1 << p.n) || !p.hp || !(p.scale > 0.0f) || b.chains < 1 ||
+      b.chains > kMaxChainBatch)
     return cudaErrorInvalidValue;
+  for (int c = 0; c < b.chains; c++) {
+    const RealChainDesc& d = b.chain[c];
+    if (!d.out_base[0] || (p.K > 1 && !d.out_base[1]) || !d.part ||
+        (!p.start_uniform && !d.start))
+      return cudaErrorInvalidValue;
+  }
   switch (p.L) {
-    case 9: return launch_real_chain_lt<9>(p, stream);
-    case 10: return launch_real_chain_lt<10>(p, stream);
-    case 11: return launch_real_chain_lt<11>(p, stream);
-    case 12: return launch_real_chain_lt<12>(p, stream);
+    case 9: return launch_real_chain_lt<9>(b, stream);
+    case 10: return launch_real_chain_lt<10>(b, stream);
+    case 11: return launch_real_chain_lt<11>(b, stream);
+    case 12: return launch_real_chain_lt<12>(b, stream);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -728,9 +728,12 @@ def test_real_chains_match_complex_chains(ctx, orc, mqw, monkeypatch, n, m, samp
     assert abs(float(np.mean(on)) - r64["p"][0]) <= 1e-5
 
 
-@pytest.mark.parametrize("n,m,precision", [(13, 3, "fp32"), (13, 2, "fp64"), (14, 3, "fp32"),
-                                           (15, 4, "fp32"), (16, 3, "fp32"), (15, 2, "fp64")])
-def test_chain_launch_matches_single_pass_launches(ctx, orc, mqw, monkeypatch, n, m, precision):
+@pytest.mark.parametrize("n,m,precision,s2", [(13, 3, "fp32", "-1"), (13, 2, "fp64", "-1"),
+                                              (14, 3, "fp32", "-1"), (15, 4, "fp32", "-1"),
+                                              (16, 3, "fp32", "-1"), (15, 2, "fp64", "-1"),
+                                              (13, 4, "fp32", "1"), (16, 3, "fp32", "1")])
+def test_chain_launch_matches_single_pass_launches(ctx, orc, mqw, monkeypatch, n, m, precision,
+                                                   s2):
     """Small n: every term of a walk-stage in one launch (a thread-block
     cluster of up to 16 CTAs per walk, cluster barriers between the passes)
     against one launch per term (MQW_CHAIN=0), with a fraction of the
@@ -739,8 +742,11 @@ def test_chain_launch_matches_single_pass_launches(ctx, orc, mqw, monkeypatch, n
     identical; above it the chain launch uses wider tiles (at most 16 per
     walk) than the single-pass launches, which changes the order of the
     partner sums, so per-sample P agree to FP32 (FP64) rounding. The grid
-    path is forced (resident_max_n = -1) so that n = 13 takes it too."""
+    path is forced (resident_max_n = -1) so that n = 13 takes it too. With
+    the stage-2 product basis forced on (s2 = "1"), its chains run batched,
+    one cluster per chain in one launch."""
     raw = orc.sk_instances(n, 2, 6100 + n)
+    monkeypatch.setenv("MQW_STAGE2_BASIS", s2)
 
     def run(chain):
         monkeypatch.setenv("MQW_CHAIN", "1" if chain else "0")
