@@ -2210,11 +2210,14 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
   if (comp) precision = MQW_FP32;  // FP32 storage, compensated partner sums
   const size_t N = (size_t)1 << n;
   const size_t amp = precision == 0 ? 8 : 16;
-  PassGeomHost geo = pass_geom(precision, n);
-  // Tiles spread over a cluster measured slower than one narrower tile with
-  // the remaining axes read from global memory; use the latter.
-  if (geo.C > 0) geo = pass_geom(precision, n, geo.L - 1);
+  // Single-CTA tiles: where the widest tile leaves axes to neither tiling
+  // they are read from global memory (tiles spread over a cluster measured
+  // slower).
+  const PassGeomHost geo = pass_geom(precision, n, 0, 0, 0, 0, 0);
   const int tiles = (int)(N >> geo.L);
+  // Small n: all K terms in one chain launch (in place, nothing read from
+  // global memory).
+  const int chain_L = comp ? 0 : chain_tile_log(precision, n);
   DevMem d_st, d_hp, d_c, d_np;
   CK(d_st.ensure(4 * N * amp));
   CK(d_hp.ensure(N * sizeof(float)));
@@ -2229,7 +2232,28 @@ mqw_status mqw_clenshaw(mqw_ctx* ctx, int precision, int n, int K,
   CK(cudaMemcpyAsync(P0, psi, N * amp, cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(d_hp.p, hp, N * sizeof(float), cudaMemcpyHostToDevice, st));
   CK(cudaMemcpyAsync(d_c.p, coeffs, K * sizeof(float), cudaMemcpyHostToDevice, st));
-  for (int r = K - 1; r >= 0; r--) {
+  if (chain_L) {
+    PassParams pp{};
+    pp.n = n;
+    pp.L = chain_L;
+    pp.a = geo.a;
+    pp.tiling = 1;
+    pp.err = ctx->dev_err.as<unsigned>();
+    pp.count = 1;
+    PassWalk& W = pp.walk[0];
+    W.active = 1;
+    W.bin = W.bout = X;  // b_0 ends in X, as with one launch per term
+    W.part = Pt;
+    W.psi = P0;
+    W.hp = d_hp.as<float>();
+    W.coef = d_c.as<float>();
+    W.norm_part = d_np.as<double>();  // N >> chain_L <= tiles partials
+    W.gamma = gamma;
+    W.scale = scale;
+    W.K = K;
+    CK(launch_pass_chain(precision, pp, st));
+  }
+  for (int r = chain_L ? -1 : K - 1; r >= 0; r--) {
     PassParams pp{};
     pp.n = n;
     pp.L = geo.L;
