@@ -16,9 +16,12 @@ read-back). L2 is flushed (256 MB write) between timed steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-Other workloads (--workload): mixed (a seeded subset of the mixed n=12..20,
-m=2..5 batch), n28 (one n=28, m=3 instance, a few samples per step) and
-precision (the n=24 near-degenerate FP32/FP64/CPU study; one JSON report).
+Other workloads (--workload): adam_n20_m4 (the headline's shape on the
+reference's own instances: the first --batch of data/AdamData/SK_20n, a
+committed byte copy), mixed (a seeded subset of the mixed n=12..20, m=2..5
+batch), n28 (one n=28, m=3 instance, a few samples per step), mixed_full (the
+whole 4096-instance mixed batch as one plan; one JSON report) and precision
+(the n=24 near-degenerate FP32/FP64/CPU study; one JSON report).
 
 With --impl reference the line times the reference's own CPU hot loop
 (Clenshaw_step, compiled from the reference source into oracle/_ref) driven
@@ -57,11 +60,11 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # DRAM bytes (read + write) per term·amp of one pass_kernel launch from an
 # ncu capture of the workload (cold caches: ncu flushes them between
 # replays), keyed by config.workload: n = 20, 29.40 MB per 2^20-amplitude
-# launch; n = 24 (tile 2^11, 6 global axes), 469.8 + 233.0 MB per
-# 2^24-amplitude launch; n = 28, the same pass shape captured on an n = 26
-# walk, 2373.8 MB per 2^26-amplitude first-stage launch, per amplitude.
-DRAM_BYTES_PER_TERM_AMP = {"sk_n20_m4": 29.40e6 / 2**20, "sk_n24_m4": 702.8e6 / 2**24,
-                           "sk_n28_m3_seed7": 2373.8e6 / 2**26}
+# launch; n = 24 and n = 28 (2^12 single-CTA tiles with global axes), the
+# same pass shape captured on an n = 26 walk (6 global axes), 1880.3 +
+# 1050.6 MB per 2^26-amplitude launch, per amplitude.
+DRAM_BYTES_PER_TERM_AMP = {"sk_n20_m4": 29.40e6 / 2**20, "adam_sk20n_m4": 29.40e6 / 2**20,
+                           "sk_n24_m4": 2930.9e6 / 2**26, "sk_n28_m3_seed7": 2930.9e6 / 2**26}
 # Host memory the CPU legs may use at once (all worker processes together).
 CPU_MEM_BUDGET = 24 << 30
 
@@ -73,7 +76,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mqw", choices=["mqw", "reference"])
     ap.add_argument("--workload", default="sk_n20_m4",
-                    choices=["sk_n20_m4", "mixed", "n28", "precision", "mixed_full"])
+                    choices=["sk_n20_m4", "adam_n20_m4", "mixed", "n28", "precision",
+                             "mixed_full"])
     ap.add_argument("--n", type=int, default=20)
     ap.add_argument("--m", type=int, default=4)
     ap.add_argument("--batch", type=int, default=2, help="instances per step per GPU")
@@ -245,14 +249,15 @@ def _step_desc(kind: str) -> str:
             else "oracle restatement")
 
 
-def cpu_baseline(n, m, seed):
-    """One whole seeded n, m instance (all 100 samples) of the reference
-    pipeline, timed on the host cores (about 10 s at n = 20, m = 4 on 16
-    cores)."""
+def cpu_baseline(n, m, seed, raw=None):
+    """One whole seeded n, m instance (all 100 samples; `raw` if given) of the
+    reference pipeline, timed on the host cores (about 10 s at n = 20, m = 4
+    on 16 cores)."""
     import multistageqw_b200 as M
     cpu = CpuInstances(n)
     try:
-        raw = M.sk_instances(n, 1, seed)[0]
+        if raw is None:
+            raw = M.sk_instances(n, 1, seed)[0]
         cpu.run(n, m, raw, samples=cpu.workers)  # warm-up: one sample per process
         _, wall, kind = cpu.run(n, m, raw)
     finally:
@@ -402,9 +407,32 @@ def make_batch(M, a, rank):
                 "note": f"one instance, {a.samples} of its 100 samples per step; "
                         "instances/s counts samples/100"}
         return [28], [3], raw.ravel(), desc
+    if a.workload == "adam_n20_m4":
+        raw = adam_instances()[: a.batch]
+        desc = {"workload": "adam_sk20n_m4", "n": 20, "m": 4,
+                "note": (f"the first {len(raw)} instances of the reference's data/AdamData/SK_20n "
+                         "(J ~ N(0, 1/2), h ~ N(0, 1); tests/golden/" + ADAM_FIXTURE + ")")}
+        return [20] * len(raw), [4] * len(raw), raw.ravel(), desc
     raw = M.sk_instances(a.n, a.batch, seed)
     desc = {"workload": f"sk_n{a.n}_m{a.m}", "n": a.n, "m": a.m}
     return [a.n] * a.batch, [a.m] * a.batch, raw.ravel(), desc
+
+
+ADAM_FIXTURE = "adam_sk20n_first16.bin"
+
+
+def adam_instances():
+    """The first 16 instances of the reference's data/AdamData/SK_20n (a
+    committed byte copy), [16, 210] float64."""
+    import numpy as np
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tests", "golden", ADAM_FIXTURE)
+    return np.fromfile(path, dtype="<f8").reshape(-1, 20 * 21 // 2)
+
+
+def data_note(a) -> str:
+    if a.workload == "adam_n20_m4":
+        return "the reference's own AdamData SK_20n instances (committed byte copy)"
+    return "synthetic seeded SK instances (J,h ~ N(0,1)); reference datasets not used"
 
 
 def instance_units(a, count: int) -> float:
@@ -419,7 +447,7 @@ def reference_arm(a):
     one sample per process). n28: seconds per term of the reference's step,
     scaled to the instance's term count (a whole instance is hours per
     core)."""
-    n, m = (28, 3) if a.workload == "n28" else (a.n, a.m)
+    n, m = (28, 3) if a.workload == "n28" else (20, 4) if a.workload == "adam_n20_m4" else (a.n, a.m)
     times, base = [], None
     import multistageqw_b200 as M
     if a.workload == "mixed":
@@ -443,8 +471,10 @@ def reference_arm(a):
     else:
         cpu = CpuInstances(n)
         try:
+            adam = adam_instances() if a.workload == "adam_n20_m4" else None
             for step in range(a.warmup + a.steps):
-                raw = M.sk_instances(n, 1, a.seed + 1000 * step)[0]
+                raw = (adam[step % len(adam)] if adam is not None
+                       else M.sk_instances(n, 1, a.seed + 1000 * step)[0])
                 if step < a.warmup:
                     cpu.run(n, m, raw, samples=cpu.workers)
                     continue
@@ -453,18 +483,20 @@ def reference_arm(a):
         finally:
             cpu.close()
         base = {"kind": kind, "cores": cpu.workers,
-                "sample": (f"every timed step one whole seeded n={n}, m={m} instance (100 samples "
+                "sample": (f"every timed step one whole {'AdamData SK_20n' if adam is not None else 'seeded'} "
+                           f"n={n}, m={m} instance (100 samples "
                            f"x {m} stages; FP32, {_step_desc(kind)}), its samples split into "
                            f"{cpu.workers} contiguous ranges, one process per core; warm-up steps "
                            "one sample per process")}
-        config = {"workload": f"sk_n{n}_m{m}", "n": n, "m": m, "samples": 100}
+        config = {"workload": "adam_sk20n_m4" if adam is not None else f"sk_n{n}_m{m}", "n": n,
+                  "m": m, "samples": 100}
     sec = sum(times)
     val = len(times) / sec
     return {
         "metric": METRIC, "value": val, "unit": "instances/s", "n_gpus": a.gpus,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1000.0 * sec / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic seeded SK instances (J,h ~ N(0,1))",
+        "dtype": "f32", "data": data_note(a),
         "impl": "reference",
         "config": config,
         "cpu_baseline": {k: base[k] for k in ("kind", "cores", "sample")} | {"value": val, "unit": "instances/s"},
@@ -703,6 +735,8 @@ def main():
                     cpu = cpu_baseline_per_term(28, int(terms * 100.0 / a.samples))
                 elif a.workload == "mixed":
                     cpu = cpu_baseline_mixed(ns, ms, raw)
+                elif a.workload == "adam_n20_m4":
+                    cpu = cpu_baseline(20, 4, 0, raw=adam_instances()[0])
                 else:
                     cpu = cpu_baseline(a.n, a.m, 4242)
             except Exception as ex:  # the baseline is reported, not required
@@ -727,7 +761,7 @@ def main():
             "steps": a.steps, "warmup": a.warmup, "ms_per_step": total_ms / a.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if a.precision == "fp64" else "f32",
-            "data": "synthetic seeded SK instances (J,h ~ N(0,1)); reference datasets not used",
+            "data": data_note(a),
             "config": config,
             "e2e": {"value": e2e_val, "unit": "instances/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "per_step": e2e_parts},

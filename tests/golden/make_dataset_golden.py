@@ -2,7 +2,8 @@
 instance files (run in a tree that has the reference checkout, so that the
 files can be read and oracle/_ref can be built).
 
-    python tests/golden/make_dataset_golden.py
+    python tests/golden/make_dataset_golden.py              # everything
+    python tests/golden/make_dataset_golden.py --bench-only # bench fixtures only
 
 The reference ships its instances as raw float64 files in the layout the
 command reads (data/AdamData/description.txt:14-17: per instance n(n-1)/2
@@ -26,6 +27,9 @@ them unchanged):
                             the summed Chebyshev degree and the gap between
                             the two lowest energies (reference arithmetic),
                             plus the SHA-256 of each fixture file.
+  adam_sk20n_first16.bin    the first 16 instances of data/AdamData/SK_20n,
+                            the instances of bench.py's adam_n20_m4 workload
+                            (bytes and SHA-256 only, under "bench_files").
 """
 from __future__ import annotations
 
@@ -41,6 +45,13 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from oracle import oracle as O  # noqa: E402
+
+# Byte copies for the bench's workload on the reference's own instances
+# (n = 20: no oracle runs, only the bytes and their SHA-256):
+# (fixture, source file within the reference checkout, n, instances)
+BENCH_FIXTURES = [
+    ("adam_sk20n_first16.bin", "data/AdamData/SK_20n", 20, 16),
+]
 
 # (fixture, source file within the reference checkout, n, instances, m values)
 CASES = [
@@ -58,10 +69,33 @@ def two_lowest_gap(n: int, raw: np.ndarray) -> float:
     return float(E.min() - e0)
 
 
+def write_bench_fixtures(ref: str) -> dict:
+    out = {}
+    for fixture, src, n, count in BENCH_FIXTURES:
+        per = O.params_per_instance(n)
+        with open(os.path.join(ref, src), "rb") as f:
+            data = f.read(8 * per * count)
+        assert len(data) == 8 * per * count, (src, len(data))
+        with open(os.path.join(HERE, fixture), "wb") as f:
+            f.write(data)
+        out[fixture] = {"source": src, "n": n, "instances": count,
+                        "sha256": hashlib.sha256(data).hexdigest()}
+    return out
+
+
 def main() -> None:
     ref = O.reference_dir()
     if ref is None:
         raise SystemExit("the reference checkout is required (MQW_REFERENCE_DIR)")
+    if "--bench-only" in sys.argv:  # refresh only the bench fixtures' bytes and hashes
+        path = os.path.join(HERE, "dataset_expect.json")
+        with open(path) as f:
+            out = json.load(f)
+        out["bench_files"] = write_bench_fixtures(ref)
+        with open(path, "w") as f:
+            json.dump(out, f, indent=0)
+            f.write("\n")
+        return
     O.build()
     if O.ref_lib() is None:
         raise SystemExit("the partial reference build (oracle/_ref) is required")
@@ -97,6 +131,7 @@ def main() -> None:
                   f"{np.abs(rr['p'] - r64['p']).max():.2e}, "
                   f"max |P_refdriven - P_own_invnorm| = {np.abs(rr['p'] - r32['p']).max():.2e}")
         out["files"][fixture] = entry
+    out["bench_files"] = write_bench_fixtures(ref)
     with open(os.path.join(HERE, "dataset_expect.json"), "w") as f:
         json.dump(out, f, indent=0)
         f.write("\n")

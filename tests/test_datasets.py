@@ -36,6 +36,20 @@ def test_fixture_bytes_are_the_recorded_ones(name):
     assert raw.shape[0] == EXPECT["files"][name]["instances"]
 
 
+@pytest.mark.parametrize("name", sorted(EXPECT["bench_files"]))
+def test_bench_fixture_bytes_are_the_recorded_ones(name):
+    """The instances of bench.py's adam_n20_m4 workload: the first 16 of the
+    reference's data/AdamData/SK_20n, byte for byte."""
+    e = EXPECT["bench_files"][name]
+    with open(os.path.join(GOLDEN, name), "rb") as f:
+        data = f.read()
+    assert hashlib.sha256(data).hexdigest() == e["sha256"]
+    n = e["n"]
+    raw = np.frombuffer(data, dtype="<f8").reshape(e["instances"], n * (n + 1) // 2)
+    J = raw[:, : n * (n - 1) // 2]
+    assert 0.6 < J.std() < 0.8  # the dataset's couplings: N(0, 1/2)
+
+
 @pytest.mark.parametrize("name", sorted(EXPECT["files"]))
 def test_oracle_restatement_matches_reference_driven_run_on_dataset(orc, name):
     """On the reference's instances the oracle's own FP32 step (a
