@@ -283,6 +283,10 @@ struct RealChainBatch {
   RealChainDesc chain[kMaxChainBatch];
 };
 cudaError_t launch_real_chain(const RealChainBatch& b, cudaStream_t stream);
+// Pass j (term r = R - j) of each of the b.chains chains in one launch
+// (single-CTA tiles of 2^L, L = p.L; any n, axes beyond both tilings read
+// from global memory).
+cudaError_t launch_real_batch(const RealChainBatch& b, int j, cudaStream_t stream);
 // v = e_{E_loc} as a real vector of 2^n floats.
 cudaError_t launch_unit_eloc_real(float* v, int n, const DiagOut* diag, cudaStream_t stream);
 cudaError_t launch_combine(int precision, const CombineParams& p,

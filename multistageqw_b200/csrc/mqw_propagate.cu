@@ -1139,6 +1139,22 @@ __global__ void __launch_bounds__(RealShape<LT>::kThreads) real_chain_kernel(Rea
   }
 }
 
+// One pass (term r = R - j) of each of b.chains real chains: blockIdx.y is
+// the chain (its start vector, partial P and outputs from b.chain[]),
+// blockIdx.x the tile. Axes in neither tiling are read from global memory as
+// in real_pass_kernel (b_{r+1} and b_r are different vectors).
+template <int LT>
+__global__ void __launch_bounds__(RealShape<LT>::kThreads)
+    real_batch_kernel(RealChainBatch b, int j) {
+  const RealChainParams& p = b.p;
+  const RealChainDesc& c = b.chain[blockIdx.y];
+  const int r = p.R - j;
+  const float* bin =
+      j > 0 ? c.out_base[(j - 1) & 1] + (size_t)((j - 1) >> 1) * (size_t)p.out_stride : nullptr;
+  float* bout = c.out_base[j & 1] + (size_t)(j >> 1) * (size_t)p.out_stride;
+  real_tile<LT>(p, (r & 1) ? 2 : 1, j == 0, bin, bout, c.part, c.start, blockIdx.x);
+}
+
 __global__ void unit_eloc_real_kernel(float* v, const DiagOut* diag) { v[diag->e_loc] = 1.0f; }
 
 template <typename R>
@@ -1649,6 +1665,44 @@ cudaError_t launch_real_chain(const RealChainBatch& b, cudaStream_t stream) {
     case 10: return launch_real_chain_lt<10>(b, stream);
     case 11: return launch_real_chain_lt<11>(b, stream);
     case 12: return launch_real_chain_lt<12>(b, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+namespace {
+template <int LT>
+cudaError_t launch_real_batch_lt(const RealChainBatch& b, int j, cudaStream_t stream) {
+  using S = RealShape<LT>;
+  const size_t smem = S::smem();
+  cudaError_t e = ensure_smem_optin((const void*)real_batch_kernel<LT>, smem, false);
+  if (e != cudaSuccess) return e;
+  const dim3 grid((unsigned)((size_t)1 << (b.p.n - LT)), (unsigned)b.chains);
+  real_batch_kernel<LT><<<grid, S::kThreads, smem, stream>>>(b, j);
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_real_batch(const RealChainBatch& b, int j, cudaStream_t stream) {
+  const RealChainParams& p = b.p;
+  if (p.n < 6 || p.n > kMaxN || p.L < 6 || p.L > 13 || p.L > p.n || p.a != 4 || j < 0 ||
+      j >= p.K || p.R < p.K || p.out_stride < ((long long)1 << p.n) || !p.hp ||
+      !(p.scale > 0.0f) || b.chains < 1 || b.chains > kMaxChainBatch)
+    return cudaErrorInvalidValue;
+  for (int c = 0; c < b.chains; c++) {
+    const RealChainDesc& d = b.chain[c];
+    if (!d.out_base[0] || (p.K > 1 && !d.out_base[1]) || !d.part ||
+        (j == 0 && !p.start_uniform && !d.start))
+      return cudaErrorInvalidValue;
+  }
+  switch (p.L) {
+    case 6: return launch_real_batch_lt<6>(b, j, stream);
+    case 7: return launch_real_batch_lt<7>(b, j, stream);
+    case 8: return launch_real_batch_lt<8>(b, j, stream);
+    case 9: return launch_real_batch_lt<9>(b, j, stream);
+    case 10: return launch_real_batch_lt<10>(b, j, stream);
+    case 11: return launch_real_batch_lt<11>(b, j, stream);
+    case 12: return launch_real_batch_lt<12>(b, j, stream);
+    case 13: return launch_real_batch_lt<13>(b, j, stream);
     default: return cudaErrorInvalidValue;
   }
 }

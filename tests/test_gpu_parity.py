@@ -766,3 +766,29 @@ def test_chain_launch_matches_single_pass_launches(ctx, orc, mqw, monkeypatch, n
     assert l_on * 4 < l_off, (l_on, l_off)
     r64 = ctx.run_problems(n, m, raw, samples=8, precision="fp64", graph=0)
     assert np.abs(np.mean(on, axis=1) - r64["p"]).max() <= 1e-5
+
+
+@pytest.mark.parametrize("n,m,samples,tile", [(18, 3, 40, 0), (21, 3, 12, 0), (20, 4, 24, 11)])
+def test_batched_chain_passes_match_one_chain_per_launch(ctx, orc, mqw, monkeypatch, n, m,
+                                                         samples, tile):
+    """The stage-2 product basis's chains with up to 8 chains per launch
+    (MQW_CHAIN_BATCH=8, each chain its own partial P) against one chain per
+    launch: the same real passes on the same tiles, so every per-sample P is
+    identical — at n = 21 and with 2^11 tiles at n = 20 with axes read from
+    global memory."""
+    raw = orc.sk_instances(n, 1, 7700 + n)
+    monkeypatch.setenv("MQW_STAGE2_BASIS", "1")
+    shape = {"tile_log": tile} if tile else {}
+
+    def run(batch):
+        monkeypatch.setenv("MQW_CHAIN_BATCH", str(batch))
+        plan = mqw.Plan(ctx, n, m, raw, samples=samples, graph=0, **shape)
+        plan.execute()
+        out = plan.results(per_sample=True)["p_sample"]
+        launches = plan.stats()["launches"]
+        plan.close()
+        return out, launches
+
+    (on, l_on), (off, l_off) = run(8), run(1)
+    assert np.array_equal(on, off)
+    assert l_on < l_off
