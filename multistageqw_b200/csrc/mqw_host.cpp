@@ -127,7 +127,9 @@ struct mqw_ctx {
   // output, and the coefficient matrices (one instance at a time).
   DevMem s2y, s2psi, s2c;
   DevMem s2chain;  // chain slots of the build-ahead (4 complex vectors)
-  DevMem s2part;   // partial P of each batched product-basis chain (small n)
+  DevMem s2part;   // partial P of each batched product-basis chain
+  DevMem s3y, s3v, s3part;  // product basis of the last two stages, its
+                            // recombined vectors, projection partials
   // Bumped whenever a shared scratch buffer is reallocated: a plan's captured
   // graph holds the old addresses and is re-captured when this changes.
   unsigned long long scratch_gen = 1;
@@ -267,6 +269,9 @@ struct mqw_plan {
   // with the build-ahead.
   size_t s2y_floats = 0, s2psi_floats = 0, s2c_floats = 0;
   size_t s2part_floats = 0;  // ctx->s2part per buffer set (0: no batched chains)
+  std::map<int, int> s3_k3;  // n -> largest stage-3 degree: the product basis
+                             // of the last two stages is used for this n
+  int s3_mode = -1;          // MQW_LAST2_BASIS: -1 auto, 0 off, 1 whenever it fits
   DevMem d_unit;
   int unit_len = 0;
   // CUDA graph of the whole device pipeline, replayed by later executes.
@@ -841,14 +846,18 @@ bool use_real_chains(const mqw_plan& P, const PassGeomHost& geo) {
 // every later pass is b_r = 2 H~ b_{r+1} - b_{r+2}; each pass also stores
 // Re(b_r). The passes stop at r = R - K + 1 >= 1 (the r = 0 form is never
 // used).
+// With `tbasis` the chain's vectors are first-kind, w_j = T_j(H~) v (the
+// real chain kernel only).
 template <typename OutOf>
 mqw_status issue_chain(mqw_plan& P, const ResidentWalk& w0, int stage, int K,
                        const ChainSlots& S, const PassGeomHost& geo, OutOf out_of,
-                       cudaStream_t stream) {
+                       cudaStream_t stream, bool tbasis = false) {
   mqw_ctx* ctx = P.ctx;
   const size_t N = (size_t)1 << w0.n;
   const int R = K + (K & 1);
   const int job = w0.stage_desc_off + stage;
+  if (tbasis && !use_real_chains(P, geo))
+    return fail(ctx, MQW_ERR_INVALID, "first-kind chains need the real chain kernel");
   if (use_real_chains(P, geo)) {
     // Every vector of the chain is real: the real chain kernel, writing
     // each b_r straight into its basis slot and reading b_{r+1} back from
@@ -878,6 +887,7 @@ mqw_status issue_chain(mqw_plan& P, const ResidentWalk& w0, int stage, int K,
         rp.K = K;
         rp.R = R;
         rp.out_stride = stride;
+        rp.tbasis = tbasis ? 1 : 0;
         rb.chains = 1;
         rb.chain[0] = RealChainDesc{S.start_real, static_cast<float*>(S.part), {base0, base1}};
         CK(launch_real_chain(rb, stream));
@@ -905,6 +915,8 @@ mqw_status issue_chain(mqw_plan& P, const ResidentWalk& w0, int stage, int K,
       rp.hp = P.d_hp.as<float>() + w0.hp_off;
       rp.gamma = P.jobs[job].gamma;
       rp.scale = P.onenorm[job];
+      rp.half_start = tbasis && j == 0;
+      rp.half_finish = tbasis && j == 1;
       CK(launch_real_pass(rp, stream));
       if (P.counting) {
         P.stats.launches++;
@@ -969,7 +981,7 @@ mqw_status issue_chain(mqw_plan& P, const ResidentWalk& w0, int stage, int K,
 // uniform state for the first stage and e_{E_loc} for the last.
 mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
                        const BasisLayout& B, const PassGeomHost& geo, float* real,
-                       cudaStream_t stream) {
+                       cudaStream_t stream, bool tbasis = false) {
   const size_t N = (size_t)1 << w0.n;
   const bool from_eloc = stage > 0;
   const bool real_chain = use_real_chains(P, geo);
@@ -985,7 +997,7 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
   const ChainSlots S{B.slot(0), {B.slot(1), B.slot(2)}, B.slot(3), !from_eloc,
                      from_eloc ? static_cast<const float*>(B.slot(3)) : nullptr};
   return issue_chain(P, w0, stage, Kb, S, geo, [&](int j) { return real + (size_t)j * N; },
-                     stream);
+                     stream, tbasis);
 }
 
 // The stage-2 product basis of one instance (FP32): Y_jk = U_k(H~_2) w_j for
@@ -999,18 +1011,29 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
 // build-ahead, which calls this on the basis stream with `builder` set: the
 // chains then run on the basis stream's own lanes and on the context's chain
 // slots, one set per lane, instead of the walk lanes and their slots).
+// With `last2` set the same machinery builds the product basis of the last
+// two stages instead (m = 4): Y'_jk = U_k(H~_3) w'_j from the last-stage
+// basis w'_j = U_j(H~_4) e_{E_loc} (`basis`, Kb vectors) with chains of
+// stage 3 (K2 passes), into ctx->s3y, and the GEMM leaves every walk's
+// V = sum_jk d4_j d3_k Y'_jk, planar, in ctx->s3v (see issue_last2).
 mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size_t b1,
                         const float* basis, int Kb, int K2, const PassGeomHost& geo,
                         int lanes, int gmax,
                         const std::function<mqw_status(cudaStream_t)>& extra,
-                        cudaStream_t stream, int buf = 0, bool builder = false) {
+                        cudaStream_t stream, int buf = 0, bool builder = false,
+                        bool last2 = false) {
   mqw_ctx* ctx = P.ctx;
   const ResidentWalk& w0 = P.walks[ws[b0]];
   const int n = w0.n;
   const size_t N = (size_t)1 << n;
   const int nw = (int)(b1 - b0);
   const S2Layout lay{Kb, K2};
-  float* Y = ctx->s2y.as<float>() + (size_t)buf * P.s2y_floats;
+  // the chains' stage and the coefficient stages of the basis index j and
+  // the chain index k
+  const int chain_stage = last2 ? w0.stages - 2 : 1;
+  const int sj = last2 ? w0.stages - 1 : 0;
+  float* Y = last2 ? ctx->s3y.as<float>()
+                   : ctx->s2y.as<float>() + (size_t)buf * P.s2y_floats;
   const int slots = walk_slots(geo);
   const int all = extra ? std::min(lanes + 1, kMaxLanes) : lanes;
   cudaStream_t* lane_st = builder ? ctx->bld_stream : ctx->lane_stream;
@@ -1039,7 +1062,7 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
     for (int k = 2; k < K2 && batched; k++)
       batched = chain_out(j, k) == chain_out(j, k - 2) + N;
   if (batched) {
-    const int job = w0.stage_desc_off + 1;
+    const int job = w0.stage_desc_off + chain_stage;
     float* part = ctx->s2part.as<float>() + (size_t)buf * P.s2part_floats;
     for (int c0 = 0; c0 < Kb; c0 += kMaxChainBatch) {
       RealChainBatch rb{};
@@ -1054,6 +1077,7 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
       rp.K = K2;
       rp.R = K2 + (K2 & 1);
       rp.out_stride = (long long)N;
+      rp.tbasis = last2 ? 1 : 0;
       rb.chains = std::min(kMaxChainBatch, Kb - c0);
       for (int c = 0; c < rb.chains; c++) {
         const int j = c0 + c;
@@ -1084,7 +1108,7 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
         if (chain_out(j, k) != chain_out(j, k - 2) + N) B = 1;
   }
   if (B > 1) {
-    const int job = w0.stage_desc_off + 1;
+    const int job = w0.stage_desc_off + chain_stage;
     float* part = ctx->s2part.as<float>() + (size_t)buf * P.s2part_floats;
     const int nbatch = (Kb + B - 1) / B;
     for (int i = 0; i < nbatch; i++) {
@@ -1102,6 +1126,7 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
       rp.K = K2;
       rp.R = K2 + (K2 & 1);
       rp.out_stride = (long long)N;
+      rp.tbasis = last2 ? 1 : 0;
       rb.chains = std::min(B, Kb - i * B);
       for (int c = 0; c < rb.chains; c++) {
         const int j = i * B + c;
@@ -1136,7 +1161,7 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
       const int h = (j + k) & 1;
       return Y + ((size_t)(h ? lay.rows(0) : 0) + lay.index(j, k)) * N;
     };
-    mqw_status s = issue_chain(P, w0, 1, K2, S, geo, out_of, st);
+    mqw_status s = issue_chain(P, w0, chain_stage, K2, S, geo, out_of, st, last2);
     if (s != MQW_OK) return s;
   }
   if (builder) {
@@ -1154,6 +1179,9 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
   cp.coef = P.d_coef.as<float>();
   cp.job0 = w0.stage_desc_off;
   cp.m = w0.stages;
+  cp.sj = sj;
+  cp.sk = chain_stage;
+  cp.tbasis = last2 ? 1 : 0;
   cp.walks = nw;
   cp.col_stride = col_stride;
   cp.lay = lay;
@@ -1173,7 +1201,7 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
   gp.n = n;
   gp.walks = nw;
   gp.out_walks = P.s2_walks;
-  gp.out = ctx->s2psi.as<float>() + (size_t)buf * P.s2psi_floats;
+  gp.out = last2 ? ctx->s3v.as<float>() : ctx->s2psi.as<float>() + (size_t)buf * P.s2psi_floats;
   // The GEMM on the tensor cores (tcgen05, three-product TF32 split) unless
   // MQW_S2_GEMM=simt selects the FP32 SIMT kernel.
   const char* gemm_env = getenv("MQW_S2_GEMM");
@@ -1292,6 +1320,26 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
       return bk.Kb > 0 && P.s2_k2.count(n) && wb.stages >= 3 && nwb <= P.s2_walks &&
              (P.s2_mode > 0 || 2 * bk.Kb <= nwb);
     };
+    // The product basis of the last two stages of a block (m = 4, stage-2
+    // product basis, last-stage basis, one instance per block in order; the
+    // walks' sample offsets consecutive).
+    auto use_last2 = [&](const Block& bk) {
+      const ResidentWalk& wb = P.walks[ws[bk.b0]];
+      if (!P.s3_k3.count(n) || wb.stages != 4 || !bk.Kl || !use_s2(bk) || nbuf == 2 ||
+          !use_real_chains(P, geo))
+        return false;
+      int K3b = 0;
+      long long sum3 = 0;  // the per-walk recurrences' passes
+      for (size_t k = bk.b0; k < bk.b1; k++) {
+        const ResidentWalk& w = P.walks[ws[k]];
+        if (w.stages != 4 || w.record_each || w.p_off != wb.p_off + (int)(k - bk.b0)) return false;
+        K3b = std::max(K3b, P.degree[w.stage_desc_off + 2]);
+        sum3 += P.degree[w.stage_desc_off + 2];
+      }
+      // real chain passes at 0.6 of a complex pass (see the layout)
+      return K3b > 0 && K3b <= P.s3_k3.at(n) &&
+             (P.s3_mode > 0 || 3LL * bk.Kl * K3b <= 5 * sum3);
+    };
     auto s2_degree = [&](const Block& bk) {
       int K2b = 0;
       for (size_t k = bk.b0; k < bk.b1; k++)
@@ -1366,11 +1414,38 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
         std::function<mqw_status(cudaStream_t)> last_build;
         if (bk.Kl)
           last_build = [&](cudaStream_t st) {
-            return issue_basis(P, wb, wb.stages - 1, bk.Kl, B, geo, B.real2(), st);
+            // first-kind vectors when they seed the last two stages' basis
+            return issue_basis(P, wb, wb.stages - 1, bk.Kl, B, geo, B.real2(), st,
+                               use_last2(bk));
           };
         mqw_status s = issue_stage2(P, ws, bk.b0, bk.b1, basis, bk.Kb, K2b, geo,
                                     std::min(gs.lanes, bk.Kb), gs.bgroup, last_build, stream);
         if (s != MQW_OK) return s;
+        if (use_last2(bk)) {
+          // m = 4: the last two stages by projection onto their product
+          // basis; no walk runs a recurrence.
+          int K3b = 0;
+          for (size_t k = bk.b0; k < bk.b1; k++)
+            K3b = std::max(K3b, P.degree[P.walks[ws[k]].stage_desc_off + 2]);
+          s = issue_stage2(P, ws, bk.b0, bk.b1, lastb, bk.Kl, K3b, geo,
+                           std::min(gs.lanes, bk.Kl), gs.bgroup, nullptr, stream, 0, false, true);
+          if (s != MQW_OK) return s;
+          Last2Params lp{};
+          lp.V = ctx->s3v.as<float>();
+          lp.psi = ctx->s2psi.as<float>();
+          lp.n = n;
+          lp.L = std::min(n, 12);
+          lp.walks = (int)(bk.b1 - bk.b0);
+          lp.v_walks = lp.psi_walks = P.s2_walks;
+          lp.part = ctx->s3part.as<double>();
+          lp.p_out = P.d_p_sample.as<double>() + wb.p_off;
+          CK(launch_last2(lp, stream));
+          if (P.counting) {
+            P.stats.launches += 2;
+            P.stats.aux_bytes += (double)lp.walks * ((size_t)1 << n) * 16.0;
+          }
+          continue;
+        }
       }
       // Groups are dealt round-robin to the lanes, which run concurrently.
       // With shared bases a group is a basis group of up to gs.bgroup walks
@@ -1574,6 +1649,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     const size_t budget = std::min(free_b / 2, (size_t)64 << 30);
     std::map<int, std::pair<int, int>> kb;
     std::map<int, int> s2k;             // largest stage-2 degree (m >= 3 walks)
+    std::map<int, int> s3k;             // largest stage-3 degree (m == 4 walks)
     std::map<int, int> inst_walks;      // walks of one instance (largest)
     std::map<std::pair<int, int>, int> per_inst;
     for (size_t w = 0; w < P.walks.size(); w++) {
@@ -1584,6 +1660,8 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
       k.second = std::max(k.second, P.degree[wk.stage_desc_off + wk.stages - 1]);
       if (wk.stages >= 3) {
         s2k[wk.n] = std::max(s2k[wk.n], P.degree[wk.stage_desc_off + 1]);
+        if (wk.stages == 4)
+          s3k[wk.n] = std::max(s3k[wk.n], P.degree[wk.stage_desc_off + 2]);
         const int c = ++per_inst[std::make_pair(wk.n, wk.inst)];
         inst_walks[wk.n] = std::max(inst_walks[wk.n], c);
       }
@@ -1649,6 +1727,50 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
         // the product basis's chains run batched, one partial P each
         s2part_n = cb / 4;
       }
+    }
+    // The product basis of the last two stages (m = 4 instances with the
+    // stage-2 product basis and a last-stage basis): Y'_jk = U_k(H~_3) w'_j,
+    // its walks' recombined vectors and the projection partials, one
+    // instance at a time, without the build-ahead. Its cost is one real
+    // chain of K_3 passes per last-stage basis vector against one complex
+    // recurrence per walk; a real pass costs about 0.6 of a complex one
+    // (measured at n = 20: 4.5 against 7.8 us). Laid out when the basis
+    // vectors are at most 5/3 of an instance's walks and chosen per instance
+    // (use_last2 in issue_rest) by that cost, or always with
+    // MQW_LAST2_BASIS=1; MQW_LAST2_BASIS=0 turns it off.
+    P.s3_k3.clear();
+    size_t s3y_b = 0, s3v_b = 0, s3p_b = 0;
+    {
+      const char* env = getenv("MQW_LAST2_BASIS");
+      const int mode = env ? atoi(env) : -1;
+      P.s3_mode = mode;
+      for (auto& e : s3k) {
+        const int n = e.first, K3 = e.second;
+        if (mode == 0 || ahead || !P.s2_k2.count(n) || !P.basis_kb2.count(n)) continue;
+        const int k4 = P.basis_kb2.at(n), wpi = inst_walks[n];
+        if (k4 == 0 || K3 == 0 || (mode < 0 && 3 * k4 > 5 * wpi)) continue;
+        const size_t N = (size_t)1 << n;
+        const size_t yb = std::max(s3y_b, (size_t)k4 * K3 * N * 4);
+        // V has the stage-2 outputs' walk stride (the GEMM writes both alike)
+        const size_t vb = std::max(s3v_b, 2 * (size_t)P.s2_walks * N * 4);
+        const size_t qb = std::max(s3p_b, last2_part_bytes(n, wpi));
+        const size_t cb = std::max(s2part_n, (size_t)k4 * N) * 4;
+        if (basis_b + s2y_b + 2 * (size_t)P.s2_walks * s2psi_n * 4 + cb + yb + vb > budget)
+          continue;
+        P.s3_k3[n] = K3;
+        s3y_b = yb;
+        s3v_b = vb;
+        s3p_b = qb;
+        s2part_n = cb / 4;
+        s2c_b = std::max(s2c_b, ((size_t)k4 * K3 + 16) * (size_t)((wpi + 127) / 128 * 128) * 4);
+        s2c_b = std::max(s2c_b, s2_tc_coef_floats(wpi, S2Layout{k4, K3}) * 4);
+        rmax = std::max(rmax, K3 + (K3 & 1));
+      }
+    }
+    if (!P.s3_k3.empty()) {
+      CK(ctx->grow(ctx->s3y, s3y_b));
+      CK(ctx->grow(ctx->s3v, s3v_b));
+      CK(ctx->grow(ctx->s3part, s3p_b));
     }
     if (!P.s2_k2.empty()) {
       const size_t nb = ahead ? 2 : 1;

@@ -260,12 +260,18 @@ struct RealChainParams {
   float psi0;
   const float* hp;
   float gamma, scale;
-  // Chain launch only (launch_real_chain; tiling, first, bin, bout, part
-  // and start are taken per chain from RealChainDesc): passes j = 0 .. K-1
-  // of terms r = R - j, pass j writing b_r to
-  // out_base[j & 1] + (j >> 1) * out_stride floats.
+  // Single-pass launches: this pass finishes / starts its term with
+  // a = 1/onenorm (the second and first pass of a first-kind chain).
+  int half_finish, half_start;
+  // Chain and batch launches only (launch_real_chain, launch_real_batch;
+  // tiling, first, bin, bout, part and start are taken per chain from
+  // RealChainDesc): passes j = 0 .. K-1 of terms r = R - j, pass j writing
+  // b_r to out_base[j & 1] + (j >> 1) * out_stride floats. tbasis: the
+  // chains' vectors are first-kind, T_j(H~) v (T_1 = H~ v), instead of
+  // U_j(H~) v.
   int K, R;
   long long out_stride;
+  int tbasis;
 };
 cudaError_t launch_real_pass(const RealChainParams& p, cudaStream_t stream);
 // Whole chains in one launch: per chain a cluster of 2^(n-L) CTAs with
@@ -323,11 +329,17 @@ struct S2Layout {
   }
 };
 // Coefficient matrices of one instance's walks: walk `col` (< walks) has its
-// stage-s job at job0 + col * m + s.
+// stage-s job at job0 + col * m + s. Row (j, k) of class h weighs basis
+// vector j with the walk's stage-sj coefficients and chain step k with its
+// stage-sk ones (the stage-2 product basis: sj = 0, sk = 1; the product
+// basis of the last two stages: sj = m - 1, sk = m - 2).
 struct S2CoefParams {
   const StageDesc* stages;
   const float* coef;
   int job0, m, walks;
+  int sj, sk;
+  int tbasis;  // first-kind basis vectors: the weights are the coefficients
+               // c themselves (else the second-kind weights d)
   int col_stride;      // columns per row (a multiple of s2_tile_cols(walks))
   S2Layout lay;
   int rows_pad[2];     // rows of C0 / C1 (zero-padded to multiples of 8)
@@ -355,6 +367,21 @@ struct UnpackParams {
   int n, L, count;
   UnpackWalk walk[kMaxGroup];
 };
+// Projection onto the product basis of the last two stages (m = 4): per
+// walk P = |sum_i V_i psi_i|^2 / |psi|^2 with V (the walk's recombined
+// last-two-stage vector) and psi (its stage-2 state) planar: Re of walk w at
+// base + w 2^n, Im at base + (stride + w) 2^n. Blocks of 2^L amplitudes
+// (L = min(n, 12)) leave FP64 partials in `part` (last2_part_bytes).
+struct Last2Params {
+  const float* V;
+  const float* psi;
+  int n, L, walks;
+  int v_walks, psi_walks;  // walk strides of V and psi
+  double* part;
+  double* p_out;           // P of walk w at p_out[w]
+};
+cudaError_t launch_last2(const Last2Params& p, cudaStream_t stream);
+size_t last2_part_bytes(int n, int walks);
 cudaError_t launch_real_to_complex(void* dst, const float* src, int n, cudaStream_t stream);
 cudaError_t launch_s2_coef(const S2CoefParams& p, cudaStream_t stream);
 // Columns of one GEMM tile for `walks` walks (C's row stride is a multiple).

@@ -1017,11 +1017,15 @@ __device__ __forceinline__ unsigned long long f2u(float2 f) {
 // real_tile is one CTA's share of one real pass: tiling `tiling`, the
 // chain's first pass when `first`, b_{r+1} read from `bin_` and b_r written
 // to `bout_`, the partial P in place at `part_`, the start vector `start_`,
-// on the CTA's tile `bx`.
+// on the CTA's tile `bx`. `half_finish` / `half_start`: the term this pass
+// finishes / starts uses a = 1/onenorm instead of 2/onenorm (a chain of
+// first-kind vectors T_j v: T_1 = H~ v).
 template <int LT>
 __device__ __forceinline__ void real_tile(const RealChainParams& p, const int tiling,
                                           const bool first, const float* bin_, float* bout_,
-                                          float* part_, const float* start_, const unsigned bx) {
+                                          float* part_, const float* start_, const unsigned bx,
+                                          const bool half_finish = false,
+                                          const bool half_start = false) {
   using S = RealShape<LT>;
   constexpr int RP = S::kRP, LOGT = S::kLogT, T = S::kThreads;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1054,6 +1058,8 @@ __device__ __forceinline__ void real_tile(const RealChainParams& p, const int ti
   for (int j = 0; j < RP; j++) cp_async8(sd + (j * T + tid), hp + g0 + j * gstride);
   unsigned long long va[RP], vb[RP];
   const float am = 2.0f / p.scale;
+  const float afin = half_finish ? 1.0f / p.scale : am;  // the term finished here
+  const float ast = half_start ? 1.0f / p.scale : am;    // the term started here
   const float gamma = p.gamma;
   if (first) {
 #pragma unroll
@@ -1074,7 +1080,7 @@ __device__ __forceinline__ void real_tile(const RealChainParams& p, const int ti
     for (int j = 0; j < RP; j++) sx1[tid | (j << LOGT)] = va[j];
     __syncthreads();
     cp_async_wait_all();
-    const float ag = am * gamma;
+    const float ag = afin * gamma;
 #pragma unroll
     for (int j = 0; j < RP; j++) {
       unsigned long long acc = real_axis_sum<LT, LOGT, RP>(va, j, sx1, fb0, fb1, tid);
@@ -1106,8 +1112,8 @@ __device__ __forceinline__ void real_tile(const RealChainParams& p, const int ti
     const float2 d = sd[j * T + tid];
     const float2 b = u2f(vb[j]), b1 = u2f(va[j]);
     // pass_kernel's arithmetic with a zero coefficient: (0 - b1) + a (...)
-    const float2 out = make_float2(fmaf(am, fmaf(d.x, b.x, -gamma * s.x), 0.0f - b1.x),
-                                   fmaf(am, fmaf(d.y, b.y, -gamma * s.y), 0.0f - b1.y));
+    const float2 out = make_float2(fmaf(ast, fmaf(d.x, b.x, -gamma * s.x), 0.0f - b1.x),
+                                   fmaf(ast, fmaf(d.y, b.y, -gamma * s.y), 0.0f - b1.y));
     *reinterpret_cast<unsigned long long*>(part + g0 + j * gstride) = f2u(out);
   }
 }
@@ -1115,7 +1121,8 @@ __device__ __forceinline__ void real_tile(const RealChainParams& p, const int ti
 // One real pass (p.tiling, p.first, p.bin -> p.bout); blockIdx.x is the tile.
 template <int LT>
 __global__ void __launch_bounds__(RealShape<LT>::kThreads) real_pass_kernel(RealChainParams p) {
-  real_tile<LT>(p, p.tiling, p.first != 0, p.bin, p.bout, p.part, p.start, blockIdx.x);
+  real_tile<LT>(p, p.tiling, p.first != 0, p.bin, p.bout, p.part, p.start, blockIdx.x,
+                p.half_finish != 0, p.half_start != 0);
 }
 
 // Chain launch of whole real chains (small n, no axis read from global
@@ -1134,7 +1141,8 @@ __global__ void __launch_bounds__(RealShape<LT>::kThreads) real_chain_kernel(Rea
     const float* bin =
         j > 0 ? c.out_base[(j - 1) & 1] + (size_t)((j - 1) >> 1) * (size_t)p.out_stride : nullptr;
     float* bout = c.out_base[j & 1] + (size_t)(j >> 1) * (size_t)p.out_stride;
-    real_tile<LT>(p, (r & 1) ? 2 : 1, j == 0, bin, bout, c.part, c.start, blockIdx.x);
+    real_tile<LT>(p, (r & 1) ? 2 : 1, j == 0, bin, bout, c.part, c.start, blockIdx.x,
+                  p.tbasis && j == 1, p.tbasis && j == 0);
     if (j + 1 < p.K) cluster_barrier();
   }
 }
@@ -1152,7 +1160,8 @@ __global__ void __launch_bounds__(RealShape<LT>::kThreads)
   const float* bin =
       j > 0 ? c.out_base[(j - 1) & 1] + (size_t)((j - 1) >> 1) * (size_t)p.out_stride : nullptr;
   float* bout = c.out_base[j & 1] + (size_t)(j >> 1) * (size_t)p.out_stride;
-  real_tile<LT>(p, (r & 1) ? 2 : 1, j == 0, bin, bout, c.part, c.start, blockIdx.x);
+  real_tile<LT>(p, (r & 1) ? 2 : 1, j == 0, bin, bout, c.part, c.start, blockIdx.x,
+                p.tbasis && j == 1, p.tbasis && j == 0);
 }
 
 __global__ void unit_eloc_real_kernel(float* v, const DiagOut* diag) { v[diag->e_loc] = 1.0f; }

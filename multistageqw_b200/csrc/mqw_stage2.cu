@@ -51,10 +51,12 @@ __global__ void s2_coef_kernel(S2CoefParams p) {
     if (q < p.lay.rows(h) && col < p.walks) {
       int j, k;
       p.lay.pair(h, q, &j, &k);
-      const StageDesc s1 = p.stages[p.job0 + col * p.m];
-      const StageDesc s2 = p.stages[p.job0 + col * p.m + 1];
-      const double d1 = recomb_weight(p.coef + s1.coef_off, s1.K, j);
-      const double d2 = recomb_weight(p.coef + s2.coef_off, s2.K, k);
+      const StageDesc s1 = p.stages[p.job0 + col * p.m + p.sj];
+      const StageDesc s2 = p.stages[p.job0 + col * p.m + p.sk];
+      const float* c1 = p.coef + s1.coef_off;
+      const float* c2 = p.coef + s2.coef_off;
+      const double d1 = p.tbasis ? (j < s1.K ? (double)c1[j] : 0.0) : recomb_weight(c1, s1.K, j);
+      const double d2 = p.tbasis ? (k < s2.K ? (double)c2[k] : 0.0) : recomb_weight(c2, s2.K, k);
       const double s = (h == 0 && (j & 1) && (k & 1)) ? -1.0 : 1.0;
       v = (float)(s * d1 * d2);
     }
@@ -207,7 +209,81 @@ __global__ void __launch_bounds__(256) unpack_kernel(UnpackParams p) {
   }
 }
 
+// Projection onto the last two stages (m = 4): per walk w (blockIdx.y) the
+// bilinear sum a = sum_i V_i psi_i (complex, no conjugation: psi_4[E_loc] =
+// e^T U_4 U_3 psi_2 = sum_i (U_3^T U_4^T e)_i psi_2,i with H~ real symmetric)
+// of the walk's recombined vector V and its stage-2 state psi_2, and
+// |psi_2|^2; block b covers amplitudes [b 2^L, (b+1) 2^L) and leaves its
+// FP64 partials (Re a, Im a, |psi_2|^2) at part[(w nblk + b) 3 + c] (fixed
+// order, so the result is reproducible run to run).
+__global__ void __launch_bounds__(256) last2_partial_kernel(Last2Params p) {
+  __shared__ double s_red[32];
+  const size_t N = (size_t)1 << p.n;
+  const size_t chunk = (size_t)1 << p.L;
+  const size_t base = (size_t)blockIdx.x * chunk;
+  const int w = blockIdx.y;
+  const float* vr = p.V + (size_t)w * N;
+  const float* vi = p.V + (size_t)(p.v_walks + w) * N;
+  const float* pr = p.psi + (size_t)w * N;
+  const float* pi = p.psi + (size_t)(p.psi_walks + w) * N;
+  double are = 0.0, aim = 0.0, nrm = 0.0;
+  for (size_t i = base + 4 * threadIdx.x; i < base + chunk; i += 4 * blockDim.x) {
+    const float4 a = __ldcs(reinterpret_cast<const float4*>(vr + i));
+    const float4 b = __ldcs(reinterpret_cast<const float4*>(vi + i));
+    const float4 c = __ldcs(reinterpret_cast<const float4*>(pr + i));
+    const float4 d = __ldcs(reinterpret_cast<const float4*>(pi + i));
+    are += (double)a.x * c.x - (double)b.x * d.x + (double)a.y * c.y - (double)b.y * d.y +
+           (double)a.z * c.z - (double)b.z * d.z + (double)a.w * c.w - (double)b.w * d.w;
+    aim += (double)a.x * d.x + (double)b.x * c.x + (double)a.y * d.y + (double)b.y * c.y +
+           (double)a.z * d.z + (double)b.z * c.z + (double)a.w * d.w + (double)b.w * c.w;
+    nrm += (double)c.x * c.x + (double)d.x * d.x + (double)c.y * c.y + (double)d.y * d.y +
+           (double)c.z * c.z + (double)d.z * d.z + (double)c.w * c.w + (double)d.w * d.w;
+  }
+  const double sa = block_sum_d(are, s_red);
+  const double sb = block_sum_d(aim, s_red);
+  const double sc = block_sum_d(nrm, s_red);
+  if (threadIdx.x == 0) {
+    double* o = p.part + ((size_t)w * gridDim.x + blockIdx.x) * 3;
+    o[0] = sa;
+    o[1] = sb;
+    o[2] = sc;
+  }
+}
+
+// Per walk (one thread each): the partials summed in block order, and
+// P = |a|^2 / |psi_2|^2 (the norms of the stage-3 and stage-4 outputs taken
+// as their inputs', exact up to the 1e-6 Chebyshev tail).
+__global__ void last2_final_kernel(Last2Params p, int nblk) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= p.walks) return;
+  double a = 0.0, b = 0.0, c = 0.0;
+  const double* q = p.part + (size_t)w * nblk * 3;
+  for (int k = 0; k < nblk; k++) {
+    a += q[3 * k];
+    b += q[3 * k + 1];
+    c += q[3 * k + 2];
+  }
+  p.p_out[w] = (a * a + b * b) / c;
+}
+
 }  // namespace
+
+cudaError_t launch_last2(const Last2Params& p, cudaStream_t stream) {
+  if (p.n < 8 || p.n > kMaxN || p.L < 8 || p.L > p.n || p.walks < 1 || p.walks > 65535 ||
+      p.v_walks < p.walks || p.psi_walks < p.walks || !p.V || !p.psi || !p.part || !p.p_out)
+    return cudaErrorInvalidValue;
+  const int nblk = 1 << (p.n - p.L);
+  last2_partial_kernel<<<dim3((unsigned)nblk, (unsigned)p.walks), 256, 0, stream>>>(p);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  last2_final_kernel<<<(p.walks + 127) / 128, 128, 0, stream>>>(p, nblk);
+  return cudaGetLastError();
+}
+
+size_t last2_part_bytes(int n, int walks) {
+  const int L = n < 12 ? n : 12;
+  return (size_t)walks * ((size_t)1 << (n - L)) * 3 * sizeof(double);
+}
 
 cudaError_t launch_real_to_complex(void* dst, const float* src, int n, cudaStream_t stream) {
   if (n < 1 || n > kMaxN || !dst || !src) return cudaErrorInvalidValue;

@@ -6,9 +6,9 @@
 //   out_h[walk][amp] = sum_q Y_h[q][amp] C_h[q][walk]
 // (q the (j, k) pairs of the class, K_h of them; Y the basis vectors, 2^n
 // floats each; C the walks' coefficient products). Here the amplitudes are
-// the MMA's M dimension (two M = 128 halves per CTA, 256 amplitudes), the
-// walks its N dimension (padded to a multiple of 16, at most 128) and the
-// pairs its K dimension, in chunks of 32.
+// the MMA's M dimension (M = 128 per CTA), the walks its N dimension (padded
+// to a multiple of 16, at most 128) and the pairs its K dimension, in chunks
+// of 32.
 //
 // TF32 keeps 10 mantissa bits. Each FP32 operand is split as x = hi + lo
 // with hi = x rounded to TF32 (exact in TF32) and lo = x - hi (exact in
@@ -18,6 +18,13 @@
 // rounding of the lo parts are ~2^-21 relative, the level of FP32 rounding.
 // The coefficient matrix is split once (s2_coef_tc_kernel, K-major hi and lo
 // copies); the basis tile is split in shared memory as it arrives.
+//
+// The tensor cores' FP32 accumulation is not round-to-nearest: summed over
+// the whole K dimension in TMEM, the result drifts toward zero by ~0.3 ulp
+// per accumulation step (measured: P of the last-two-stage projection 2e-5
+// low after ~500 steps). So the TMEM accumulator is restarted every
+// kTcGroup chunks (two buffers, alternating) and the epilogue warps add each
+// group's result into FP32 registers with round-to-nearest.
 //
 // Data movement: Y tiles (MN-major: 32 amplitudes x 32 pairs per box, eight
 // boxes per chunk) and the C tiles (K-major: 32 pairs x N walks) arrive by
@@ -49,16 +56,17 @@ namespace mqw {
 namespace {
 
 constexpr int kTcM = 128;            // amplitudes per MMA (TMEM lanes)
-constexpr int kTcAmps = 2 * kTcM;    // amplitudes per CTA (two M halves)
+constexpr int kTcAmps = kTcM;        // amplitudes per CTA
 constexpr int kTcBK = 32;            // pairs per chunk: one 128-byte row of tf32
-constexpr int kTcStages = 2;
+constexpr int kTcStages = 3;
 constexpr int kTcThreads = 192;
 constexpr int kTcMaxN = 128;         // walks (MMA N) per CTA
-constexpr unsigned kTcTmemCols = 256;  // two accumulators at columns 0 and 128
+constexpr int kTcGroup = 2;          // chunks per TMEM accumulation group
+constexpr unsigned kTcTmemCols = 256;  // two accumulator buffers, columns 0 and 128
 constexpr unsigned long long kTcWaitNs = 200000000ull;  // 200 ms
 
 // Shared-memory layout (offsets from a 1024-byte aligned base).
-constexpr unsigned kTcATile = kTcAmps * kTcBK * 4;        // 32 KB: eight 4 KB boxes
+constexpr unsigned kTcATile = kTcAmps * kTcBK * 4;        // 16 KB: four 4 KB boxes
 constexpr unsigned kTcBTile = kTcMaxN * kTcBK * 4;        // 16 KB
 constexpr unsigned kTcStage = 2 * kTcATile + 2 * kTcBTile;  // A(hi), A lo, B hi, B lo
 constexpr unsigned kTcBarOff = kTcStages * kTcStage;
@@ -185,7 +193,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   auto full = [&](int s) { return bars + 8u * s; };
   auto conv = [&](int s) { return bars + 8u * (kTcStages + s); };
   auto empty = [&](int s) { return bars + 8u * (2 * kTcStages + s); };
-  const unsigned accf = bars + 8u * (3 * kTcStages);
+  const unsigned accf = bars + 8u * (3 * kTcStages);  // every MMA done (teardown)
+  // accumulation group g lives in TMEM buffer g & 1: full once its MMAs
+  // completed, free once the epilogue warps have read it
+  auto accfull = [&](int b) { return bars + 8u * (3 * kTcStages + 1 + b); };
+  auto accfree = [&](int b) { return bars + 8u * (3 * kTcStages + 3 + b); };
   auto a_tile = [&](int s) { return sbase + s * kTcStage; };
   auto alo_tile = [&](int s) { return sbase + s * kTcStage + kTcATile; };
   auto bhi_tile = [&](int s) { return sbase + s * kTcStage + 2 * kTcATile; };
@@ -195,6 +207,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   const int h = blockIdx.y;
   const int m0 = blockIdx.x * kTcAmps;
   const int chunks = p.chunks[h];
+  const int groups = (chunks + kTcGroup - 1) / kTcGroup;
   volatile int* abort_flag = &abort_sh;
 
   if (threadIdx.x == 0) {
@@ -205,6 +218,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       bar_init(empty(s), 1);
     }
     bar_init(accf, 1);
+    for (int b = 0; b < 2; b++) {
+      bar_init(accfull(b), 1);
+      bar_init(accfree(b), 128);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) {
@@ -252,30 +269,31 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       int done = 0;
       for (int c = 0; c < chunks; c++) {
         const int s = c % kTcStages;
+        const int g = c / kTcGroup, first = c % kTcGroup == 0;
+        // A group's buffer is reused once the epilogue has read the group
+        // two before it.
+        if (first && g >= 2 && !bar_wait(accfree(g & 1), ((g >> 1) - 1) & 1, abort_flag, p.err))
+          break;
         if (!bar_wait(conv(s), (c / kTcStages) & 1, abort_flag, p.err)) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned d = tmem + (unsigned)((g & 1) * kTcM);
 #pragma unroll
         for (int kk = 0; kk < kTcBK / 8; kk++) {
-#pragma unroll
-          for (int half = 0; half < 2; half++) {
-            // A (MN-major, 32-byte-atom swizzle): blocks of 32 amplitudes
-            // 4 KB apart (LBO), groups of 4 pair rows 512 B apart (SBO); the
-            // MMA's 8 pairs start 1 KB further per step. B (K-major, 128-byte
-            // swizzle): groups of 8 walk rows 1 KB apart (SBO); the MMA's 8
-            // pairs start 32 B further per step.
-            const unsigned long long ahi =
-                umma_desc(a_tile(s) + half * (kTcATile / 2) + kk * 1024u, 4096u, 512u, 1u);
-            const unsigned long long alo =
-                umma_desc(alo_tile(s) + half * (kTcATile / 2) + kk * 1024u, 4096u, 512u, 1u);
-            const unsigned long long bhi = umma_desc(bhi_tile(s) + kk * 32u, 16u, 1024u, 2u);
-            const unsigned long long blo = umma_desc(blo_tile(s) + kk * 32u, 16u, 1024u, 2u);
-            const unsigned d = tmem + (unsigned)(half * kTcM);
-            umma_tf32(d, ahi, bhi, idesc, c > 0 || kk > 0);
-            umma_tf32(d, ahi, blo, idesc, true);
-            umma_tf32(d, alo, bhi, idesc, true);
-          }
+          // A (MN-major, 32-byte-atom swizzle): blocks of 32 amplitudes 4 KB
+          // apart (LBO), groups of 4 pair rows 512 B apart (SBO); the MMA's
+          // 8 pairs start 1 KB further per step. B (K-major, 128-byte
+          // swizzle): groups of 8 walk rows 1 KB apart (SBO); the MMA's 8
+          // pairs start 32 B further per step.
+          const unsigned long long ahi = umma_desc(a_tile(s) + kk * 1024u, 4096u, 512u, 1u);
+          const unsigned long long alo = umma_desc(alo_tile(s) + kk * 1024u, 4096u, 512u, 1u);
+          const unsigned long long bhi = umma_desc(bhi_tile(s) + kk * 32u, 16u, 1024u, 2u);
+          const unsigned long long blo = umma_desc(blo_tile(s) + kk * 32u, 16u, 1024u, 2u);
+          umma_tf32(d, ahi, bhi, idesc, !(first && kk == 0));
+          umma_tf32(d, ahi, blo, idesc, true);
+          umma_tf32(d, alo, bhi, idesc, true);
         }
         umma_commit(empty(s));  // the stage's tiles are free once these MMAs finish
+        if (c % kTcGroup == kTcGroup - 1 || c == chunks - 1) umma_commit(accfull(g & 1));
         done = c + 1;
       }
       umma_commit(accf);  // every MMA issued so far has completed when accf flips
@@ -283,9 +301,39 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     }
     __syncwarp();
   } else {
-    // Warps 2-5: split each Y tile into hi (in place) and lo.
+    // Warps 2-5: split each Y tile into hi (in place) and lo; add each
+    // accumulation group's result into registers (this warp's TMEM lane
+    // quarter: 32 amplitudes, one per thread, all walks); store at the end.
     const int ct = threadIdx.x - 64;  // 0..127
+    const int q = warp & 3;
+    float acc[kTcMaxN];
+#pragma unroll
+    for (int j = 0; j < kTcMaxN; j++) acc[j] = 0.0f;
     bool ok = true;
+    int gread = 0;  // next group to add
+    auto read_group = [&](int g) -> bool {
+      if (!bar_wait(accfull(g & 1), (g >> 1) & 1, abort_flag, p.err)) return false;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const unsigned base = tmem + ((unsigned)(32 * q) << 16) + (unsigned)((g & 1) * kTcM);
+#pragma unroll
+      for (int c0 = 0; c0 < kTcMaxN; c0 += 8) {
+        if (c0 < p.Np) {
+          unsigned r[8];
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+              : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                "=r"(r[6]), "=r"(r[7])
+              : "r"(base + (unsigned)c0)
+              : "memory");
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int j = 0; j < 8; j++) acc[c0 + j] = __fadd_rn(acc[c0 + j], __uint_as_float(r[j]));
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      bar_arrive(accfree(g & 1));
+      return true;
+    };
     for (int c = 0; c < chunks && ok; c++) {
       const int s = c % kTcStages;
       if (!bar_wait(full(s), (c / kTcStages) & 1, abort_flag, p.err)) {
@@ -307,30 +355,28 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       bar_arrive(conv(s));
+      // After the last chunk of group g, add group g - 1 (its MMAs were
+      // issued a group ago), which frees its buffer for group g + 1.
+      const int g = c / kTcGroup;
+      if ((c % kTcGroup == kTcGroup - 1 || c == chunks - 1) && g >= 1 && gread == g - 1) {
+        if (!read_group(gread)) {
+          ok = false;
+          break;
+        }
+        gread++;
+      }
     }
-    // Epilogue: this warp's TMEM lane quarter = 32 amplitudes of each half.
-    if (ok && bar_wait(accf, 0, abort_flag, p.err)) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int q = warp & 3;
+    while (ok && gread < groups) {
+      if (!read_group(gread)) ok = false;
+      gread++;
+    }
+    if (ok && !*abort_flag) {
       const size_t N = (size_t)1 << p.n;
       float* out = p.out + (size_t)h * p.out_walks * N;
-      for (int half = 0; half < 2; half++) {
-        const size_t amp = (size_t)m0 + half * kTcM + 32 * q + lane;
-        for (int c0 = 0; c0 < p.Np; c0 += 8) {
-          const unsigned ta = tmem + ((unsigned)(32 * q) << 16) + (unsigned)(half * kTcM + c0);
-          unsigned r[8];
-          asm volatile(
-              "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-              : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-                "=r"(r[6]), "=r"(r[7])
-              : "r"(ta)
-              : "memory");
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      const size_t amp = (size_t)m0 + 32 * q + lane;
 #pragma unroll
-          for (int j = 0; j < 8; j++)
-            if (c0 + j < p.walks) out[(size_t)(c0 + j) * N + amp] = __uint_as_float(r[j]);
-        }
-      }
+      for (int j = 0; j < kTcMaxN; j++)
+        if (j < p.walks) out[(size_t)j * N + amp] = acc[j];
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -357,15 +403,17 @@ __global__ void s2_coef_tc_kernel(S2CoefParams p, float* Ct, int Np, int Kp) {
     if (q < p.lay.rows(h) && w < p.walks) {
       int j, k;
       p.lay.pair(h, q, &j, &k);
-      const StageDesc s1 = p.stages[p.job0 + w * p.m];
-      const StageDesc s2 = p.stages[p.job0 + w * p.m + 1];
+      const StageDesc s1 = p.stages[p.job0 + w * p.m + p.sj];
+      const StageDesc s2 = p.stages[p.job0 + w * p.m + p.sk];
       auto weight = [](const float* c, int K, int i) {
         const double ci = i < K ? (double)c[i] : 0.0;
         const double ci2 = i + 2 < K ? (double)c[i + 2] : 0.0;
         return i == 0 ? ci - 0.5 * ci2 : 0.5 * (ci - ci2);
       };
-      const double d1 = weight(p.coef + s1.coef_off, s1.K, j);
-      const double d2 = weight(p.coef + s2.coef_off, s2.K, k);
+      const float* c1 = p.coef + s1.coef_off;
+      const float* c2 = p.coef + s2.coef_off;
+      const double d1 = p.tbasis ? (j < s1.K ? (double)c1[j] : 0.0) : weight(c1, s1.K, j);
+      const double d2 = p.tbasis ? (k < s2.K ? (double)c2[k] : 0.0) : weight(c2, s2.K, k);
       const double sg = (h == 0 && (j & 1) && (k & 1)) ? -1.0 : 1.0;
       v = (float)(sg * d1 * d2);
     }

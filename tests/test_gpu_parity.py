@@ -792,3 +792,31 @@ def test_batched_chain_passes_match_one_chain_per_launch(ctx, orc, mqw, monkeypa
     (on, l_on), (off, l_off) = run(8), run(1)
     assert np.array_equal(on, off)
     assert l_on < l_off
+
+
+@pytest.mark.parametrize("n,samples", [(14, 40), (16, 24), (18, 16), (20, 100)])
+def test_last_two_stage_basis_matches_recurrence(ctx, orc, mqw, monkeypatch, n, samples):
+    """m = 4 with the product basis of the last two stages (MQW_LAST2_BASIS=1:
+    chains U_k(H~_3) w'_j from the last-stage basis w'_j = U_j(H~_4) e_{E_loc},
+    one GEMM for every walk's recombined vector, one bilinear sum with the
+    walk's stage-2 state) against the stage-3 recurrence per walk and the
+    last-stage projection (MQW_LAST2_BASIS=0). Both take a stage's output
+    norm as its input norm only where the Chebyshev tail (1e-6) allows it,
+    so per-sample P agree to a few 1e-6 relative; both within 1e-5 of FP64."""
+    raw = orc.sk_instances(n, 1, 8800 + n)
+    monkeypatch.setenv("MQW_STAGE2_BASIS", "1")
+
+    def run(mode):
+        monkeypatch.setenv("MQW_LAST2_BASIS", mode)
+        plan = mqw.Plan(ctx, n, 4, raw, samples=samples, graph=0)
+        plan.execute()
+        out = plan.results(per_sample=True)["p_sample"]
+        pass_amps = plan.stats()["pass_amps"]
+        plan.close()
+        return out, pass_amps
+
+    (on, a_on), (off, a_off) = run("1"), run("0")
+    assert np.all(np.abs(on - off) <= 1e-5 * np.abs(off) + 1e-10), np.abs(on / off - 1).max()
+    assert a_on == 0 < a_off  # no walk ran a recurrence
+    r64 = ctx.run_problems(n, 4, raw, samples=samples, precision="fp64", graph=0)
+    assert abs(float(np.mean(on)) - r64["p"][0]) <= 1e-5
