@@ -32,9 +32,11 @@ times terms of the reference's step and scales them (a whole instance takes
 hours per core); the mixed workload runs the first samples of every
 instance.
 
-roofline: the dominant kernel, pass_kernel, timed alone (CUDA events around
-a pass-only replay in the plan's tuned shape) against the tier that holds
-its working set — L2 (the library's own L2 copy probe) when the walks in
+roofline: the dominant kernel — pass_kernel, or real_pass_kernel when the
+shared-basis chains carry more bytes than the walks' passes (the headline:
+with the product bases no walk runs a recurrence) — timed alone (CUDA events
+around a pass-only replay in the plan's tuned shape) against the tier that
+holds its working set — L2 (the library's own L2 copy probe) when the walks in
 flight fit, else HBM (MEASURED_PEAKS.json); frac = bytes_per_launch /
 avg_launch_us / peak.
 """
@@ -65,6 +67,11 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 # 1050.6 MB per 2^26-amplitude launch, per amplitude.
 DRAM_BYTES_PER_TERM_AMP = {"sk_n20_m4": 29.40e6 / 2**20, "adam_sk20n_m4": 29.40e6 / 2**20,
                            "sk_n24_m4": 2930.9e6 / 2**26, "sk_n28_m3_seed7": 2930.9e6 / 2**26}
+# The real chain pass (shared-basis chains, FP32): algorithmic bytes per
+# amplitude (read b_{r+1}, b_{r+2} and D, write b_r) and cold-cache DRAM
+# bytes per amplitude of one launch from an ncu capture, keyed by workload.
+CHAIN_BYTES_PER_AMP = 16
+CHAIN_DRAM_BYTES_PER_AMP: dict = {}
 # Host memory the CPU legs may use at once (all worker processes together).
 CPU_MEM_BUDGET = 24 << 30
 
@@ -672,21 +679,32 @@ def main():
     # workload's largest n. Its algorithmic bytes per launch are 36 B per
     # term·amp (FP32; 72 B in FP64) x 2^n x walks per launch.
     n_dom = int(max(ns))
-    pt = ctx.pass_timing(n_dom, a.precision if a.precision != "fp32c" else "fp32", reps=64)
-    bytes_per_launch = BYTES_PER_TERM_AMP[a.precision] * float(1 << n_dom) * pt["walks_per_launch"]
+    # When the shared-basis chains carry more bytes than the walks' own
+    # passes (FP32 with the product bases: at n = 20, m = 4 no walk runs a
+    # recurrence), the dominant kernel is the real chain pass instead:
+    # 16 B per amplitude algorithmic (read b_{r+1}, b_{r+2}, D; write b_r),
+    # timed alone the same way (mqw_chain_pass_timing).
+    chain_dom = a.precision == "fp32" and BYTES_PER_TERM_AMP["fp32"] * pass_amps < aux_bytes
+    if chain_dom:
+        pt = ctx.chain_pass_timing(n_dom, reps=64)
+        per_amp, vec_bytes, kname = CHAIN_BYTES_PER_AMP, 4, "real_pass_kernel"
+    else:
+        pt = ctx.pass_timing(n_dom, a.precision if a.precision != "fp32c" else "fp32", reps=64)
+        per_amp = BYTES_PER_TERM_AMP[a.precision]
+        vec_bytes, kname = (8 if a.precision != "fp64" else 16), "pass_kernel"
+    bytes_per_launch = per_amp * float(1 << n_dom) * pt["walks_per_launch"]
     achieved = bytes_per_launch / (pt["us_per_launch"] * 1e-6) / 1e9
-    # Bound tier: the memory tier that holds the concurrent walks' working
-    # set (3 state vectors of 8 B and the 4 B diagonal per amplitude, per
-    # walk in flight): L2 (126 MB; the library's own L2 copy probe is the
+    # Bound tier: the memory tier that holds the concurrent walks' (chains')
+    # working set (3 vectors and the 4 B diagonal per amplitude, per walk in
+    # flight): L2 (126 MB; the library's own L2 copy probe is the
     # denominator) when it fits in 96 MB, else HBM (MEASURED_PEAKS.json).
-    ws = (3 * (8 if a.precision != "fp64" else 16) + 4) * float(1 << n_dom) * \
-        pt["walks_per_launch"] * pt["lanes"]
+    ws = (3 * vec_bytes + 4) * float(1 << n_dom) * pt["walks_per_launch"] * pt["lanes"]
     l2_resident = ws <= 96e6 and tiers is not None
     if l2_resident:
         bound, peak, peak_src = "l2", tiers["l2_copy_gbs"], "l2_copy_gbs of the library's own probe"
     else:
         bound, peak, peak_src = "hbm", pk["hbm_gbs"], f"hbm_gbs of {pk_kind}"
-    dram = DRAM_BYTES_PER_TERM_AMP.get(desc["workload"])
+    dram = (CHAIN_DRAM_BYTES_PER_AMP if chain_dom else DRAM_BYTES_PER_TERM_AMP).get(desc["workload"])
     # Propagation phase as a whole (every pass plus the shared-basis kernels'
     # reads and writes, over the plan's device time): context for the
     # kernel figure above.
@@ -696,11 +714,12 @@ def main():
         "bound": bound, "achieved": achieved, "peak": peak, "unit": "GB/s",
         "frac": achieved / peak, "traffic": dram * float(1 << n_dom) * pt["walks_per_launch"] if dram else None,
         "peak_source": peak_src,
-        "kernel": (f"pass_kernel at n={n_dom}: frac = bytes_per_launch / avg_launch_us / peak; "
+        "kernel": (f"{kname} at n={n_dom}: frac = bytes_per_launch / avg_launch_us / peak; "
                    "avg_launch_us from CUDA events around a pass-only replay in the plan's tuned "
-                   f"shape ({pt['walks_per_launch']} walk(s) per launch, {pt['lanes']} lane(s) "
-                   "in flight, so it is the launch-to-launch time); traffic = cold-cache DRAM "
-                   "bytes per launch from ncu"),
+                   f"shape ({pt['walks_per_launch']} walk(s) or chain(s) per launch, "
+                   f"{pt['lanes']} lane(s) in flight, so it is the launch-to-launch time); "
+                   f"bytes_per_launch = {per_amp} B per amplitude algorithmic; traffic = "
+                   "cold-cache DRAM bytes per launch from ncu"),
         "bytes_per_launch": bytes_per_launch,
         "avg_launch_us": pt["us_per_launch"],
         "walks_per_launch": pt["walks_per_launch"], "lanes": pt["lanes"],
@@ -715,7 +734,7 @@ def main():
     # per launch over its launch-to-launch time, against the SIMT FP32 peak
     # at the maximum SM clock (the kernel is memory-bound; this is the
     # compute roof it stays far below).
-    if a.precision != "fp64":
+    if a.precision != "fp64" and not chain_dom:
         sms = torch.cuda.get_device_properties(dev).multi_processor_count
         mhz = float((clk or {}).get("sm_max_mhz") or 1965.0)
         peak_tf = sms * 128 * 2 * mhz * 1e6 / 1e12

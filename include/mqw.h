@@ -71,8 +71,9 @@ typedef struct mqw_options {
                                (m_0 + m_1 + ... pairs, caller order): a
                                learned schedule; NULL = the paper heuristic */
   int tile_log;    /* grid-path tile (log2 amplitudes), 0 = autotuned */
-  int graph;       /* 1 (default): a plan's second and later executions
-                      replay a CUDA graph of its whole device pipeline;
+  int graph;       /* 1 (default): a plan's second execution captures a
+                      CUDA graph of its whole device pipeline and the later
+                      ones replay it (a plan executed once pays no capture);
                       0: launch kernels one by one every time */
   int lanes;       /* grid-path walk groups in flight at once, each on its
                       own stream (1..4), 0 = autotuned */
@@ -309,6 +310,14 @@ mqw_status mqw_grid_shape_for(mqw_ctx* ctx, int precision, int n,
 mqw_status mqw_pass_timing(mqw_ctx* ctx, int precision, int n, int reps,
                            double* us_per_launch, double* us_per_walk_pass,
                            int* walks_per_launch, int* lanes);
+/* The same for the real chain pass (FP32 shared-basis chains: 20 B per
+ * amplitude), one chain per launch on the tuned lanes of n with the tuned
+ * tile: `reps` passes per lane on zero-filled vectors, CUDA events on the
+ * context's stream; us_per_pass = elapsed / (reps * lanes) (the
+ * launch-to-launch time with `lanes` in flight). Tiles spread over a
+ * cluster are MQW_ERR_UNSUPPORTED (the chains never use them). */
+mqw_status mqw_chain_pass_timing(mqw_ctx* ctx, int n, int reps, double* us_per_pass,
+                                 int* lanes, int* tile_log);
 
 /* ---- learned stage schedule (no counterpart in the reference) ---------- */
 /* Building blocks of the MLP that proposes per-stage (gamma, t) multipliers

@@ -155,6 +155,7 @@ def _bind(L):
         "mqw_clenshaw_noalloc": (i, [i, i, i, _vp, _vp, f, f, _vp, _vp, _vp]),
         "mqw_grid_shape_for": (i, [_vp, i, i, _P(GridShape)]),
         "mqw_pass_timing": (i, [_vp, i, i, i, _P(d), _P(d), _P(i), _P(i)]),
+        "mqw_chain_pass_timing": (i, [_vp, i, i, _P(d), _P(i), _P(i)]),
         "mqw_diag_moments": (i, [_vp, i, _P(d), _P(d), _P(DiagInfo)]),
         "mqw_selftest_wait_timeout": (i, [_vp]),
         "mqw_measure_peaks": (i, [_vp, _P(TierPeaks)]),
@@ -385,6 +386,16 @@ class Context:
                                              ctypes.byref(uw), ctypes.byref(g), ctypes.byref(ln)))
         return {"us_per_launch": ul.value, "us_per_walk_pass": uw.value,
                 "walks_per_launch": g.value, "lanes": ln.value, "reps": reps}
+
+    def chain_pass_timing(self, n: int, reps: int = 64) -> dict:
+        """Device time of the real chain pass alone (mqw_chain_pass_timing):
+        microseconds per pass, launch-to-launch with the tuned lanes in
+        flight, one chain per launch."""
+        us, ln, tl = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+        _check(self.h, lib().mqw_chain_pass_timing(self.h, n, reps, ctypes.byref(us),
+                                                   ctypes.byref(ln), ctypes.byref(tl)))
+        return {"us_per_launch": us.value, "lanes": ln.value, "tile_log": tl.value,
+                "walks_per_launch": 1, "reps": reps}
 
     def multiqw(self, n: int, m: int, filename: str, start: int = 0, problems: int = 2000,
                 out_dir: str | None = None, print_: bool = True):

@@ -284,6 +284,7 @@ struct mqw_plan {
   std::vector<long long> coef_off;
   mqw_run_stats stats{};
   bool executed = false;
+  int eager_runs = 0;  // executions issued eagerly (the second one captures)
   // Propagation-phase timing (recorded on the launching stream).
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   bool timed = false;
@@ -1829,14 +1830,16 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
   if (s != MQW_OK) return s;
   P.timed = true;
   P.executed = true;
-  // Capture the whole device pipeline for later executes. The capture runs
-  // on the context's private stream (nothing executes while capturing); the
-  // graph is later launched on whatever stream the caller passes. Very large
-  // pipelines (over kMaxGraphLaunches kernels) stay eager: their launch
-  // overhead is already negligible and a graph of millions of nodes costs
-  // host memory and instantiation time.
+  P.eager_runs++;
+  // Capture the whole device pipeline for later executes, once the plan is
+  // executed a second time (a plan run once pays no capture). The capture
+  // runs on the context's private stream (nothing executes while
+  // capturing); the graph is later launched on whatever stream the caller
+  // passes. Very large pipelines (over kMaxGraphLaunches kernels) stay
+  // eager: their launch overhead is already negligible and a graph of
+  // millions of nodes costs host memory and instantiation time.
   constexpr long long kMaxGraphLaunches = 200000;
-  if (P.opt.graph && P.stats.launches <= kMaxGraphLaunches) {
+  if (P.opt.graph && P.eager_runs >= 2 && P.stats.launches <= kMaxGraphLaunches) {
     CK(cudaStreamSynchronize(stream));
     cudaStream_t cs = ctx->stream;
     P.counting = false;
@@ -2240,6 +2243,75 @@ mqw_status mqw_pass_timing(mqw_ctx* ctx, int precision, int n, int reps,
   if (us_per_launch) *us_per_launch = us * gs.group;
   if (walks_per_launch) *walks_per_launch = gs.group;
   if (lanes) *lanes = gs.lanes;
+  return MQW_OK;
+}
+
+mqw_status mqw_chain_pass_timing(mqw_ctx* ctx, int n, int reps, double* us_per_pass,
+                                 int* lanes_out, int* tile_log) {
+  mqw_status st = check_ctx(ctx);
+  if (st != MQW_OK) return st;
+  if (n < 6 || n > kMaxN || reps < 1 || reps > 100000)
+    return fail(ctx, MQW_ERR_INVALID, "mqw_chain_pass_timing: bad arguments");
+  // The plan's shape for this n: its tuned tile and lanes (chains run one
+  // per launch, dealt to the lanes).
+  GridShape want, gs;
+  want.group = want.lanes = 0;
+  st = tune_grid(ctx, MQW_FP32, n, want, &gs);
+  if (st != MQW_OK) return st;
+  const PassGeomHost geo = pass_geom(0, n, gs.lmax, gs.threads, gs.lane_smem > 0,
+                                     std::max(0, gs.tma), gs.cl < 0 ? 0 : 1);
+  if (geo.C != 0)
+    return fail(ctx, MQW_ERR_UNSUPPORTED, "mqw_chain_pass_timing: cluster-spanning tiles");
+  const int lanes = std::max(1, gs.lanes);
+  const size_t N = (size_t)1 << n;
+  // per lane: two chain vectors (alternating b_{r+1} / b_r) and P; then D
+  CK(ctx->ensure_lanes(lanes));
+  const size_t bytes = ((size_t)lanes * 3 + 1) * N * sizeof(float);
+  CK(ctx->grow(ctx->state, bytes));
+  cudaStream_t s0 = ctx->stream;
+  CK(cudaMemsetAsync(ctx->state.p, 0, bytes, s0));
+  float* base = ctx->state.as<float>();
+  const float* hp = base + (size_t)lanes * 3 * N;
+  auto issue = [&](int j, int lane) -> cudaError_t {
+    float* v = base + (size_t)lane * 3 * N;
+    RealChainParams rp{};
+    rp.n = n;
+    rp.L = geo.L;
+    rp.a = geo.a;
+    rp.tiling = (j & 1) ? 2 : 1;
+    rp.first = 0;
+    rp.bin = v + (size_t)((j + 1) & 1) * N;
+    rp.bout = v + (size_t)(j & 1) * N;
+    rp.part = v + 2 * N;
+    rp.start_uniform = 1;
+    rp.hp = hp;
+    rp.gamma = 1.0f;
+    rp.scale = 64.0f;
+    return launch_real_pass(rp, lane == 0 ? s0 : ctx->lane_stream[lane]);
+  };
+  CK(ctx->fork(s0, lanes));
+  for (int j = 0; j < 4; j++)
+    for (int l = 0; l < lanes; l++) CK(issue(j, l));
+  CK(ctx->join(s0, lanes));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, s0));
+  CK(ctx->fork(s0, lanes));
+  for (int j = 0; j < reps; j++)
+    for (int l = 0; l < lanes; l++) CK(issue(j, l));
+  CK(ctx->join(s0, lanes));
+  CK(cudaEventRecord(e1, s0));
+  CK(cudaEventSynchronize(e1));
+  float ms = 0.0f;
+  CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  st = take_device_error(ctx);
+  if (st != MQW_OK) return st;
+  if (us_per_pass) *us_per_pass = 1000.0 * ms / ((double)reps * lanes);
+  if (lanes_out) *lanes_out = lanes;
+  if (tile_log) *tile_log = geo.L;
   return MQW_OK;
 }
 

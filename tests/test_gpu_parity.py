@@ -226,6 +226,7 @@ def test_lanes_give_identical_results(ctx, orc, mqw):
     for lanes in (1, 2, 3):
         plan = mqw.Plan(ctx, 16, 3, raw, samples=7, group=2, lanes=lanes)
         plan.execute()
+        plan.execute()  # captures the graph
         plan.execute()  # graph replay
         out.append(plan.results(per_sample=True)["p_sample"])
         plan.close()
@@ -399,6 +400,7 @@ def mqw_plan_samples(ctx, n, m, raw):
     import multistageqw_b200 as M
     plan = M.Plan(ctx, n, m, raw, samples=8)
     plan.execute()
+    plan.execute()  # captures the graph
     plan.execute()  # graph replay
     ps = plan.results(per_sample=True)["p_sample"]
     plan.close()
@@ -474,7 +476,8 @@ def test_stage2_basis_matches_per_walk(ctx, orc, mqw, monkeypatch, n, m, samples
         plan = mqw.Plan(ctx, n, m, raw, samples=samples, graph=graph, **shape)
         plan.execute()
         first = plan.results(per_sample=True)["p_sample"]
-        plan.execute()
+        plan.execute()  # captures the graph (graph = 1)
+        plan.execute()  # replays it
         again = plan.results(per_sample=True)["p_sample"]
         plan.close()
         return first, again
