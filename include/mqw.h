@@ -311,11 +311,14 @@ mqw_status mqw_pass_timing(mqw_ctx* ctx, int precision, int n, int reps,
                            double* us_per_launch, double* us_per_walk_pass,
                            int* walks_per_launch, int* lanes);
 /* The same for the real chain pass (FP32 shared-basis chains: 20 B per
- * amplitude), one chain per launch on the tuned lanes of n with the tuned
- * tile: `reps` passes per lane on zero-filled vectors, CUDA events on the
- * context's stream; us_per_pass = elapsed / (reps * lanes) (the
- * launch-to-launch time with `lanes` in flight). Tiles spread over a
- * cluster are MQW_ERR_UNSUPPORTED (the chains never use them). */
+ * amplitude), one chain per launch with the tuned tile of n, on the lanes a
+ * plan runs its one-chain-per-launch chains on (4 from n = 19,
+ * MQW_CHAIN_LANES if set, else the tuned walk lanes): `reps` passes per
+ * lane on zero-filled vectors, captured in a CUDA graph as a plan's
+ * pipeline is, the second replay timed with CUDA events on the context's
+ * stream; us_per_pass = elapsed / (reps * lanes) (the launch-to-launch time
+ * with `lanes` in flight). Tiles spread over a cluster are
+ * MQW_ERR_UNSUPPORTED (the chains never use them). */
 mqw_status mqw_chain_pass_timing(mqw_ctx* ctx, int n, int reps, double* us_per_pass,
                                  int* lanes, int* tile_log);
 

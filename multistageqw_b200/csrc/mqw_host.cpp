@@ -78,7 +78,11 @@ struct GridShape {
   double us = 0.0;  // timed microseconds per walk-pass (0: not timed)
   int bgroup = 1;   // walks per shared-basis group (>= group; set by the plan)
 };
-constexpr int kMaxLanes = 4;
+constexpr int kMaxLanes = 4;    // walk lanes (the tuner's range)
+constexpr int kMaxStreams = 8;  // lane streams: walk lanes and chain lanes
+// Chain lanes of the one-chain-per-launch product-basis chains (n >= 19):
+// measured at n = 20, m = 4 (26.5 instances/s on 3 lanes, 27.9 on 4).
+constexpr int kChainLanes = 4;
 
 // A context owns the reusable device scratch that plans share: the grid-path
 // state slots, norm partials, the coefficient pool and its tables, and the
@@ -102,9 +106,9 @@ struct mqw_ctx {
   cudaEvent_t basis_built[2] = {}, basis_free[2] = {};
   // The basis stream's own lanes (1..): its stage-2 chains run on the basis
   // stream and these, forked and joined like the walk lanes.
-  cudaStream_t bld_stream[kMaxLanes] = {};
+  cudaStream_t bld_stream[kMaxStreams] = {};
   cudaEvent_t bld_fork_ev = nullptr;
-  cudaEvent_t bld_join_ev[kMaxLanes] = {};
+  cudaEvent_t bld_join_ev[kMaxStreams] = {};
   cudaError_t ensure_basis_stream() {
     cudaError_t e = cudaSuccess;
     if (!basis_stream) e = cudaStreamCreateWithFlags(&basis_stream, cudaStreamNonBlocking);
@@ -115,7 +119,7 @@ struct mqw_ctx {
     }
     if (e == cudaSuccess && !bld_fork_ev)
       e = cudaEventCreateWithFlags(&bld_fork_ev, cudaEventDisableTiming);
-    for (int k = 1; k < kMaxLanes && e == cudaSuccess; k++) {
+    for (int k = 1; k < kMaxStreams && e == cudaSuccess; k++) {
       if (!bld_stream[k]) e = cudaStreamCreateWithFlags(&bld_stream[k], cudaStreamNonBlocking);
       if (e == cudaSuccess && !bld_join_ev[k])
         e = cudaEventCreateWithFlags(&bld_join_ev[k], cudaEventDisableTiming);
@@ -139,15 +143,15 @@ struct mqw_ctx {
   // launching stream, lanes 1.. on these private streams, forked from and
   // joined back into the launching stream with events (which a CUDA graph
   // capture follows, so a captured pipeline keeps its lanes concurrent).
-  cudaStream_t lane_stream[kMaxLanes] = {};
+  cudaStream_t lane_stream[kMaxStreams] = {};
   cudaEvent_t fork_ev = nullptr;
-  cudaEvent_t join_ev[kMaxLanes] = {};
+  cudaEvent_t join_ev[kMaxStreams] = {};
   cudaError_t ensure_lanes(int lanes) {
     if (!fork_ev) {
       cudaError_t e = cudaEventCreateWithFlags(&fork_ev, cudaEventDisableTiming);
       if (e != cudaSuccess) return e;
     }
-    for (int k = 1; k < lanes && k < kMaxLanes; k++) {
+    for (int k = 1; k < lanes && k < kMaxStreams; k++) {
       if (!lane_stream[k]) {
         cudaError_t e = cudaStreamCreateWithFlags(&lane_stream[k], cudaStreamNonBlocking);
         if (e != cudaSuccess) return e;
@@ -1019,7 +1023,7 @@ mqw_status issue_basis(mqw_plan& P, const ResidentWalk& w0, int stage, int Kb,
 // V = sum_jk d4_j d3_k Y'_jk, planar, in ctx->s3v (see issue_last2).
 mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size_t b1,
                         const float* basis, int Kb, int K2, const PassGeomHost& geo,
-                        int lanes, int gmax,
+                        int lanes,
                         const std::function<mqw_status(cudaStream_t)>& extra,
                         cudaStream_t stream, int buf = 0, bool builder = false,
                         bool last2 = false) {
@@ -1036,19 +1040,6 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
   float* Y = last2 ? ctx->s3y.as<float>()
                    : ctx->s2y.as<float>() + (size_t)buf * P.s2y_floats;
   const int slots = walk_slots(geo);
-  const int all = extra ? std::min(lanes + 1, kMaxLanes) : lanes;
-  cudaStream_t* lane_st = builder ? ctx->bld_stream : ctx->lane_stream;
-  if (builder) {  // fork the basis stream's lanes
-    CK(cudaEventRecord(ctx->bld_fork_ev, stream));
-    for (int k = 1; k < all; k++) CK(cudaStreamWaitEvent(ctx->bld_stream[k], ctx->bld_fork_ev, 0));
-  } else {
-    CK(ctx->fork(stream, all));
-  }
-  if (extra) {
-    const int xl = all - 1;
-    mqw_status s = extra(xl == 0 ? stream : lane_st[xl]);
-    if (s != MQW_OK) return s;
-  }
   // Small n: all Kb chains in chain launches of up to kMaxChainBatch chains
   // each (a cluster per chain, each with its own partial P) on the launching
   // stream, instead of one chain after another on each lane.
@@ -1062,6 +1053,45 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
   for (int j = 0; j < Kb && batched; j++)
     for (int k = 2; k < K2 && batched; k++)
       batched = chain_out(j, k) == chain_out(j, k - 2) + N;
+  // Larger n: the chains in per-term launches of up to B chains each (the
+  // batches dealt round-robin to the lanes, each chain with its own partial
+  // P), instead of one single-chain launch per term. B = 8 up to n = 18
+  // (measured at n = 18, m = 4: 84.2 -> 88.5 instances/s); from n = 20 the
+  // batched chains' vectors no longer fit in L2 beside each other and one
+  // chain per launch is faster (measured at n = 20, m = 4: 26.5 instances/s
+  // with one chain per launch on 3 lanes, 26.1-26.3 with 2 chains per launch
+  // on 2-3 lanes, 23.6 with 8 on one lane), B = 1. MQW_CHAIN_BATCH sets B.
+  int B = 1;
+  if (!batched && use_real_chains(P, geo) && P.s2part_floats >= (size_t)Kb * N && K2 > 0) {
+    const char* e = getenv("MQW_CHAIN_BATCH");
+    B = std::min(kMaxChainBatch, std::max(1, e ? atoi(e) : (n <= 18 ? 8 : 1)));
+    for (int j = 0; j < Kb && B > 1; j++)
+      for (int k = 2; k < K2 && B > 1; k++)
+        if (chain_out(j, k) != chain_out(j, k - 2) + N) B = 1;
+  }
+  // One chain per launch (the walks' lanes' state slots, packed): from
+  // n = 19 on kChainLanes lanes (MQW_CHAIN_LANES sets it), as far as the
+  // state buffer holds their slots.
+  const size_t chain_slot_bytes = (size_t)slots * N * 8;
+  if (!builder && !batched && B == 1 && Kb > 0 && K2 > 0) {
+    const char* e = getenv("MQW_CHAIN_LANES");
+    int cl = e ? atoi(e) : (use_real_chains(P, geo) && n >= 19 ? kChainLanes : lanes);
+    cl = std::min(cl, (int)std::min<size_t>(kMaxStreams - 1, ctx->state.bytes / chain_slot_bytes));
+    lanes = std::max(1, std::min(std::max(cl, 1), Kb));
+  }
+  const int all = extra ? std::min(lanes + 1, builder ? kMaxLanes : kMaxStreams) : lanes;
+  cudaStream_t* lane_st = builder ? ctx->bld_stream : ctx->lane_stream;
+  if (builder) {  // fork the basis stream's lanes
+    CK(cudaEventRecord(ctx->bld_fork_ev, stream));
+    for (int k = 1; k < all; k++) CK(cudaStreamWaitEvent(ctx->bld_stream[k], ctx->bld_fork_ev, 0));
+  } else {
+    CK(ctx->fork(stream, all));
+  }
+  if (extra) {
+    const int xl = all - 1;
+    mqw_status s = extra(xl == 0 ? stream : lane_st[xl]);
+    if (s != MQW_OK) return s;
+  }
   if (batched) {
     const int job = w0.stage_desc_off + chain_stage;
     float* part = ctx->s2part.as<float>() + (size_t)buf * P.s2part_floats;
@@ -1092,21 +1122,6 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
         P.stats.aux_bytes += (double)N * 20.0 * K2 * rb.chains;
       }
     }
-  }
-  // Larger n: the chains in per-term launches of up to B chains each (the
-  // batches dealt round-robin to the lanes, each chain with its own partial
-  // P), instead of one single-chain launch per term. B = 8 up to n = 18
-  // (measured at n = 18, m = 4: 84.2 -> 88.5 instances/s); from n = 20 the
-  // batched chains' vectors no longer fit in L2 beside each other and one
-  // chain per launch is faster (22.9 against 22.6 at n = 20), B = 1.
-  // MQW_CHAIN_BATCH sets B.
-  int B = 1;
-  if (!batched && use_real_chains(P, geo) && P.s2part_floats >= (size_t)Kb * N && K2 > 0) {
-    const char* e = getenv("MQW_CHAIN_BATCH");
-    B = std::min(kMaxChainBatch, std::max(1, e ? atoi(e) : (n <= 18 ? 8 : 1)));
-    for (int j = 0; j < Kb && B > 1; j++)
-      for (int k = 2; k < K2 && B > 1; k++)
-        if (chain_out(j, k) != chain_out(j, k - 2) + N) B = 1;
   }
   if (B > 1) {
     const int job = w0.stage_desc_off + chain_stage;
@@ -1148,7 +1163,7 @@ mqw_status issue_stage2(mqw_plan& P, const std::vector<int>& ws, size_t b0, size
     const int lane = j % lanes;
     cudaStream_t st = lane == 0 ? stream : lane_st[lane];
     char* base = builder ? ctx->s2chain.as<char>() + (size_t)lane * 4 * N * 8
-                         : ctx->state.as<char>() + (size_t)lane * gmax * slots * N * 8;
+                         : ctx->state.as<char>() + (size_t)lane * chain_slot_bytes;
     auto slot = [&](int k) -> void* { return base + (size_t)k * N * 8; };
     const ChainSlots S{slot(0), {slot(1), slot(2)}, slot(slots - 1), false, basis + (size_t)j * N};
     if (!use_real_chains(P, geo)) {  // the complex kernel starts from a complex copy
@@ -1363,7 +1378,7 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
             return issue_basis(P, w0, w0.stages - 1, bk.Kl, B, geo, B.real2(), ls);
           };
         return issue_stage2(P, ws, bk.b0, bk.b1, B.real1(), bk.Kb, s2_degree(bk), geo,
-                            std::min(gs.lanes, bk.Kb), gs.bgroup, last_build, st, buf, true);
+                            std::min(gs.lanes, bk.Kb), last_build, st, buf, true);
       }
       if (bk.Kl) {
         mqw_status s = issue_basis(P, w0, w0.stages - 1, bk.Kl, B, geo, B.real2(), st);
@@ -1420,7 +1435,7 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
                                use_last2(bk));
           };
         mqw_status s = issue_stage2(P, ws, bk.b0, bk.b1, basis, bk.Kb, K2b, geo,
-                                    std::min(gs.lanes, bk.Kb), gs.bgroup, last_build, stream);
+                                    std::min(gs.lanes, bk.Kb), last_build, stream);
         if (s != MQW_OK) return s;
         if (use_last2(bk)) {
           // m = 4: the last two stages by projection onto their product
@@ -1429,7 +1444,7 @@ mqw_status issue_rest(mqw_plan& P, cudaStream_t stream) {
           for (size_t k = bk.b0; k < bk.b1; k++)
             K3b = std::max(K3b, P.degree[P.walks[ws[k]].stage_desc_off + 2]);
           s = issue_stage2(P, ws, bk.b0, bk.b1, lastb, bk.Kl, K3b, geo,
-                           std::min(gs.lanes, bk.Kl), gs.bgroup, nullptr, stream, 0, false, true);
+                           std::min(gs.lanes, bk.Kl), nullptr, stream, 0, false, true);
           if (s != MQW_OK) return s;
           Last2Params lp{};
           lp.V = ctx->s3v.as<float>();
@@ -1775,7 +1790,7 @@ mqw_status plan_execute(mqw_plan& P, cudaStream_t stream) {
     }
     if (!P.s2_k2.empty()) {
       const size_t nb = ahead ? 2 : 1;
-      CK(ctx->ensure_lanes(kMaxLanes));  // the last-stage basis beside the chains
+      CK(ctx->ensure_lanes(kMaxStreams));  // chain lanes and the last-stage basis beside them
       P.s2y_floats = s2y_b / 4;
       P.s2psi_floats = 2 * (size_t)P.s2_walks * s2psi_n;
       P.s2c_floats = s2c_b / 4;
@@ -1912,13 +1927,13 @@ void mqw_destroy(mqw_ctx* ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
-  for (int k = 1; k < kMaxLanes; k++) {
+  for (int k = 1; k < kMaxStreams; k++) {
     if (ctx->lane_stream[k]) cudaStreamDestroy(ctx->lane_stream[k]);
     if (ctx->join_ev[k]) cudaEventDestroy(ctx->join_ev[k]);
   }
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   if (ctx->basis_stream) cudaStreamDestroy(ctx->basis_stream);
-  for (int k = 1; k < kMaxLanes; k++) {
+  for (int k = 1; k < kMaxStreams; k++) {
     if (ctx->bld_stream[k]) cudaStreamDestroy(ctx->bld_stream[k]);
     if (ctx->bld_join_ev[k]) cudaEventDestroy(ctx->bld_join_ev[k]);
   }
@@ -2252,8 +2267,9 @@ mqw_status mqw_chain_pass_timing(mqw_ctx* ctx, int n, int reps, double* us_per_p
   if (st != MQW_OK) return st;
   if (n < 6 || n > kMaxN || reps < 1 || reps > 100000)
     return fail(ctx, MQW_ERR_INVALID, "mqw_chain_pass_timing: bad arguments");
-  // The plan's shape for this n: its tuned tile and lanes (chains run one
-  // per launch, dealt to the lanes).
+  // The plan's shape for this n: its tuned tile, and the lanes its
+  // one-chain-per-launch product-basis chains run on (kChainLanes from
+  // n = 19, MQW_CHAIN_LANES if set, else the tuned walk lanes).
   GridShape want, gs;
   want.group = want.lanes = 0;
   st = tune_grid(ctx, MQW_FP32, n, want, &gs);
@@ -2262,7 +2278,9 @@ mqw_status mqw_chain_pass_timing(mqw_ctx* ctx, int n, int reps, double* us_per_p
                                      std::max(0, gs.tma), gs.cl < 0 ? 0 : 1);
   if (geo.C != 0)
     return fail(ctx, MQW_ERR_UNSUPPORTED, "mqw_chain_pass_timing: cluster-spanning tiles");
-  const int lanes = std::max(1, gs.lanes);
+  const char* env = getenv("MQW_CHAIN_LANES");
+  int lanes = env ? atoi(env) : (n >= 19 ? kChainLanes : gs.lanes);
+  lanes = std::max(1, std::min(lanes, kMaxStreams - 1));
   const size_t N = (size_t)1 << n;
   // per lane: two chain vectors (alternating b_{r+1} / b_r) and P; then D
   CK(ctx->ensure_lanes(lanes));
@@ -2293,20 +2311,39 @@ mqw_status mqw_chain_pass_timing(mqw_ctx* ctx, int n, int reps, double* us_per_p
   for (int j = 0; j < 4; j++)
     for (int l = 0; l < lanes; l++) CK(issue(j, l));
   CK(ctx->join(s0, lanes));
-  cudaEvent_t e0, e1;
-  CK(cudaEventCreate(&e0));
-  CK(cudaEventCreate(&e1));
-  CK(cudaEventRecord(e0, s0));
-  CK(ctx->fork(s0, lanes));
-  for (int j = 0; j < reps; j++)
-    for (int l = 0; l < lanes; l++) CK(issue(j, l));
-  CK(ctx->join(s0, lanes));
-  CK(cudaEventRecord(e1, s0));
-  CK(cudaEventSynchronize(e1));
+  // The passes as the plan runs them: a CUDA graph of `reps` passes per
+  // lane (forked from and joined into the stream like the plan's lanes),
+  // replayed once untimed and once between the events.
+  CK(cudaStreamSynchronize(s0));
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+  cudaError_t ce = ctx->fork(s0, lanes);
+  for (int j = 0; j < reps && ce == cudaSuccess; j++)
+    for (int l = 0; l < lanes && ce == cudaSuccess; l++) ce = issue(j, l);
+  if (ce == cudaSuccess) ce = ctx->join(s0, lanes);
+  const cudaError_t ee = cudaStreamEndCapture(s0, &graph);
+  if (ce != cudaSuccess || ee != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    CK(ce != cudaSuccess ? ce : ee);
+  }
+  cudaGraphExec_t gexec = nullptr;
+  const cudaError_t ie = cudaGraphInstantiate(&gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  CK(ie);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaGraphLaunch(gexec, s0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  if (e == cudaSuccess) e = cudaEventRecord(e0, s0);
+  if (e == cudaSuccess) e = cudaGraphLaunch(gexec, s0);
+  if (e == cudaSuccess) e = cudaEventRecord(e1, s0);
+  if (e == cudaSuccess) e = cudaEventSynchronize(e1);
   float ms = 0.0f;
-  CK(cudaEventElapsedTime(&ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaGraphExecDestroy(gexec);
+  CK(e);
   st = take_device_error(ctx);
   if (st != MQW_OK) return st;
   if (us_per_pass) *us_per_pass = 1000.0 * ms / ((double)reps * lanes);

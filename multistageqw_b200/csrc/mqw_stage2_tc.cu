@@ -23,8 +23,8 @@
 // the whole K dimension in TMEM, the result drifts toward zero by ~0.3 ulp
 // per accumulation step (measured: P of the last-two-stage projection 2e-5
 // low after ~500 steps). So the TMEM accumulator is restarted every
-// kTcGroup chunks (two buffers, alternating) and the epilogue warps add each
-// group's result into FP32 registers with round-to-nearest.
+// kTcGroup chunks (a ring of kTcBufs buffers) and the accumulate warps add
+// each group's result into FP32 registers with round-to-nearest.
 //
 // Data movement: Y tiles (MN-major: 32 amplitudes x 32 pairs per box, eight
 // boxes per chunk) and the C tiles (K-major: 32 pairs x N walks) arrive by
@@ -32,14 +32,16 @@
 // stage. An MN-major tf32 operand has one shared-memory layout the MMA
 // accepts: 128-byte rows along M with the swizzle applied to 32-byte units
 // (atoms of 4 rows; the TMA's 128B_ATOM_32B swizzle writes it); the K-major
-// C tiles use the ordinary 128-byte swizzle. Warp roles per CTA (192 threads):
+// C tiles use the ordinary 128-byte swizzle. The kernel is persistent (one
+// CTA per SM walks its share of the tiles); warp roles per CTA (320 threads):
 //   warp 0      TMA producer (one thread);
 //   warp 1      TMEM allocator and MMA issuer (one thread issues tcgen05.mma);
-//   warps 2-5   split the Y tile into hi (in place) and lo, then, after the
-//               last chunk, read the accumulators (tcgen05.ld) and store
-//               them to the planar outputs (each warp reads its TMEM lane
-//               quarter: 32 amplitudes; a store covers 32 consecutive
-//               amplitudes of one walk).
+//   warps 2-5   split the Y tile into hi (in place) and lo;
+//   warps 6-9   read each accumulation group (tcgen05.ld), add it into FP32
+//               registers, and after a tile's last group store the tile to
+//               the planar outputs (each warp reads its TMEM lane quarter:
+//               32 amplitudes; a store covers 32 consecutive amplitudes of
+//               one walk) while the MMAs of the next tile run.
 // Every wait is bounded (%globaltimer): on expiry the CTA sets bit 1 of the
 // device error word, the other roles see the abort flag and stop, in-flight
 // copies and MMAs are waited for (bounded), the TMEM is freed and the CTA
@@ -59,10 +61,11 @@ constexpr int kTcM = 128;            // amplitudes per MMA (TMEM lanes)
 constexpr int kTcAmps = kTcM;        // amplitudes per CTA
 constexpr int kTcBK = 32;            // pairs per chunk: one 128-byte row of tf32
 constexpr int kTcStages = 3;
-constexpr int kTcThreads = 192;
+constexpr int kTcThreads = 320;
 constexpr int kTcMaxN = 128;         // walks (MMA N) per CTA
 constexpr int kTcGroup = 2;          // chunks per TMEM accumulation group
-constexpr unsigned kTcTmemCols = 256;  // two accumulator buffers, columns 0 and 128
+constexpr int kTcBufs = 4;           // TMEM accumulator buffers (a ring over groups)
+constexpr unsigned kTcTmemCols = kTcBufs * kTcMaxN;  // 512: the whole TMEM
 constexpr unsigned long long kTcWaitNs = 200000000ull;  // 200 ms
 
 // Shared-memory layout (offsets from a 1024-byte aligned base).
@@ -70,13 +73,15 @@ constexpr unsigned kTcATile = kTcAmps * kTcBK * 4;        // 16 KB: four 4 KB bo
 constexpr unsigned kTcBTile = kTcMaxN * kTcBK * 4;        // 16 KB
 constexpr unsigned kTcStage = 2 * kTcATile + 2 * kTcBTile;  // A(hi), A lo, B hi, B lo
 constexpr unsigned kTcBarOff = kTcStages * kTcStage;
-constexpr unsigned kTcSmem = kTcBarOff + 128 + 1024;     // barriers + alignment slack
+constexpr unsigned kTcSmem = kTcBarOff + 256 + 1024;     // barriers + alignment slack
+static_assert(8 * (3 * kTcStages + 1 + 2 * kTcBufs) <= 256, "barrier space");
 
 struct TcArgs {
   float* out;          // planar outputs: class 0 at out, class 1 at out + out_walks 2^n
   unsigned* err;       // device error word (bit 1: a bounded wait expired)
   int n, walks, out_walks;
   int Np;              // MMA N: walks padded to a multiple of 16
+  int tiles;           // 2 x 2^n / 128: (block of 128 amplitudes, class) pairs
   int chunks[2];       // K chunks of 32 per class
   int crow[2];         // first row of the class's hi copy in the C map (lo: + Np)
 };
@@ -171,6 +176,22 @@ __device__ __forceinline__ void umma_commit(unsigned bar) {
       : "memory");
 }
 
+// 32 consecutive TMEM columns of this warp's lane quarter, one lane per
+// thread (wait with tcgen05.wait::ld before use).
+__device__ __forceinline__ void tmem_ld32(unsigned addr, unsigned (&r)[32]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, "
+      "%28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+        "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+        "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(addr)
+      : "memory");
+}
+
 // x = hi + lo: hi rounded to TF32 (nearest, ties away; 10 mantissa bits),
 // lo = x - hi exactly.
 __device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
@@ -179,6 +200,12 @@ __device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
   lo = x - hi;
 }
 
+// Persistent: one CTA per SM takes the tiles t = blockIdx.x, blockIdx.x +
+// gridDim.x, ... (t & 1 the parity class, t >> 1 the block of 128
+// amplitudes). Every role walks the same sequence of (tile, chunk) steps, so
+// the stage ring (index `it`, all chunks of all the CTA's tiles) and the
+// accumulator ring (index `gi`, all groups) run on across tiles: the MMAs of
+// tile t + 1 proceed while the accumulate warps still add and store tile t.
 __global__ void __launch_bounds__(kTcThreads, 1)
     s2_gemm_tc_kernel(const __grid_constant__ CUtensorMap mapY0,
                       const __grid_constant__ CUtensorMap mapY1,
@@ -194,20 +221,16 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   auto conv = [&](int s) { return bars + 8u * (kTcStages + s); };
   auto empty = [&](int s) { return bars + 8u * (2 * kTcStages + s); };
   const unsigned accf = bars + 8u * (3 * kTcStages);  // every MMA done (teardown)
-  // accumulation group g lives in TMEM buffer g & 1: full once its MMAs
-  // completed, free once the epilogue warps have read it
+  // accumulation group gi lives in TMEM buffer gi % kTcBufs: full once its
+  // MMAs completed, free once the accumulate warps have read it
   auto accfull = [&](int b) { return bars + 8u * (3 * kTcStages + 1 + b); };
-  auto accfree = [&](int b) { return bars + 8u * (3 * kTcStages + 3 + b); };
+  auto accfree = [&](int b) { return bars + 8u * (3 * kTcStages + 1 + kTcBufs + b); };
   auto a_tile = [&](int s) { return sbase + s * kTcStage; };
   auto alo_tile = [&](int s) { return sbase + s * kTcStage + kTcATile; };
   auto bhi_tile = [&](int s) { return sbase + s * kTcStage + 2 * kTcATile; };
   auto blo_tile = [&](int s) { return sbase + s * kTcStage + 2 * kTcATile + kTcBTile; };
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int h = blockIdx.y;
-  const int m0 = blockIdx.x * kTcAmps;
-  const int chunks = p.chunks[h];
-  const int groups = (chunks + kTcGroup - 1) / kTcGroup;
   volatile int* abort_flag = &abort_sh;
 
   if (threadIdx.x == 0) {
@@ -218,7 +241,7 @@ __global__ void __launch_bounds__(kTcThreads, 1)
       bar_init(empty(s), 1);
     }
     bar_init(accf, 1);
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < kTcBufs; b++) {
       bar_init(accfull(b), 1);
       bar_init(accfree(b), 128);
     }
@@ -240,19 +263,26 @@ __global__ void __launch_bounds__(kTcThreads, 1)
   if (warp == 0) {
     if (lane == 0) {
       // TMA producer.
-      const CUtensorMap* mY = h ? &mapY1 : &mapY0;
-      int issued = 0;
-      for (int c = 0; c < chunks; c++) {
-        const int s = c % kTcStages;
-        if (c >= kTcStages && !bar_wait(empty(s), ((c / kTcStages) - 1) & 1, abort_flag, p.err))
-          break;
-        bar_expect_tx(full(s), kTcATile + 2 * b_bytes);
-        const int k0 = c * kTcBK;
-        for (int b = 0; b < kTcAmps / 32; b++)
-          tma_load_2d(a_tile(s) + b * 4096u, mY, m0 + 32 * b, k0, full(s));
-        tma_load_2d(bhi_tile(s), &mapC, k0, p.crow[h], full(s));
-        tma_load_2d(blo_tile(s), &mapC, k0, p.crow[h] + p.Np, full(s));
-        issued = c + 1;
+      int it = 0, issued = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < p.tiles && ok; t += gridDim.x) {
+        const int h = t & 1, m0 = (t >> 1) * kTcAmps;
+        const CUtensorMap* mY = h ? &mapY1 : &mapY0;
+        for (int c = 0; c < p.chunks[h]; c++, it++) {
+          const int s = it % kTcStages;
+          if (it >= kTcStages &&
+              !bar_wait(empty(s), ((it / kTcStages) - 1) & 1, abort_flag, p.err)) {
+            ok = false;
+            break;
+          }
+          bar_expect_tx(full(s), kTcATile + 2 * b_bytes);
+          const int k0 = c * kTcBK;
+          for (int b = 0; b < kTcAmps / 32; b++)
+            tma_load_2d(a_tile(s) + b * 4096u, mY, m0 + 32 * b, k0, full(s));
+          tma_load_2d(bhi_tile(s), &mapC, k0, p.crow[h], full(s));
+          tma_load_2d(blo_tile(s), &mapC, k0, p.crow[h] + p.Np, full(s));
+          issued = it + 1;
+        }
       }
       if (*abort_flag) {
         // Copies issued but never consumed must land before the CTA's shared
@@ -266,112 +296,126 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     if (lane == 0) {
       // MMA issuer.
       const unsigned idesc = umma_idesc(p.Np);
-      int done = 0;
-      for (int c = 0; c < chunks; c++) {
-        const int s = c % kTcStages;
-        const int g = c / kTcGroup, first = c % kTcGroup == 0;
-        // A group's buffer is reused once the epilogue has read the group
-        // two before it.
-        if (first && g >= 2 && !bar_wait(accfree(g & 1), ((g >> 1) - 1) & 1, abort_flag, p.err))
-          break;
-        if (!bar_wait(conv(s), (c / kTcStages) & 1, abort_flag, p.err)) break;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const unsigned d = tmem + (unsigned)((g & 1) * kTcM);
+      int it = 0, gi = 0;
+      bool ok = true;
+      for (int t = blockIdx.x; t < p.tiles && ok; t += gridDim.x) {
+        const int chunks = p.chunks[t & 1];
+        unsigned d = tmem;
+        for (int c = 0; c < chunks; c++, it++) {
+          const int s = it % kTcStages;
+          const bool first = c % kTcGroup == 0;
+          if (first) {
+            // A group's buffer is reused once the accumulate warps have read
+            // the group kTcBufs before it.
+            const int b = gi % kTcBufs;
+            if (gi >= kTcBufs &&
+                !bar_wait(accfree(b), ((gi / kTcBufs) - 1) & 1, abort_flag, p.err)) {
+              ok = false;
+              break;
+            }
+            d = tmem + (unsigned)(b * kTcMaxN);
+          }
+          if (!bar_wait(conv(s), (it / kTcStages) & 1, abort_flag, p.err)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-        for (int kk = 0; kk < kTcBK / 8; kk++) {
-          // A (MN-major, 32-byte-atom swizzle): blocks of 32 amplitudes 4 KB
-          // apart (LBO), groups of 4 pair rows 512 B apart (SBO); the MMA's
-          // 8 pairs start 1 KB further per step. B (K-major, 128-byte
-          // swizzle): groups of 8 walk rows 1 KB apart (SBO); the MMA's 8
-          // pairs start 32 B further per step.
-          const unsigned long long ahi = umma_desc(a_tile(s) + kk * 1024u, 4096u, 512u, 1u);
-          const unsigned long long alo = umma_desc(alo_tile(s) + kk * 1024u, 4096u, 512u, 1u);
-          const unsigned long long bhi = umma_desc(bhi_tile(s) + kk * 32u, 16u, 1024u, 2u);
-          const unsigned long long blo = umma_desc(blo_tile(s) + kk * 32u, 16u, 1024u, 2u);
-          umma_tf32(d, ahi, bhi, idesc, !(first && kk == 0));
-          umma_tf32(d, ahi, blo, idesc, true);
-          umma_tf32(d, alo, bhi, idesc, true);
+          for (int kk = 0; kk < kTcBK / 8; kk++) {
+            // A (MN-major, 32-byte-atom swizzle): blocks of 32 amplitudes 4 KB
+            // apart (LBO), groups of 4 pair rows 512 B apart (SBO); the MMA's
+            // 8 pairs start 1 KB further per step. B (K-major, 128-byte
+            // swizzle): groups of 8 walk rows 1 KB apart (SBO); the MMA's 8
+            // pairs start 32 B further per step.
+            const unsigned long long ahi = umma_desc(a_tile(s) + kk * 1024u, 4096u, 512u, 1u);
+            const unsigned long long alo = umma_desc(alo_tile(s) + kk * 1024u, 4096u, 512u, 1u);
+            const unsigned long long bhi = umma_desc(bhi_tile(s) + kk * 32u, 16u, 1024u, 2u);
+            const unsigned long long blo = umma_desc(blo_tile(s) + kk * 32u, 16u, 1024u, 2u);
+            umma_tf32(d, ahi, bhi, idesc, !(first && kk == 0));
+            umma_tf32(d, ahi, blo, idesc, true);
+            umma_tf32(d, alo, bhi, idesc, true);
+          }
+          umma_commit(empty(s));  // the stage's tiles are free once these MMAs finish
+          if (c % kTcGroup == kTcGroup - 1 || c == chunks - 1) {
+            umma_commit(accfull(gi % kTcBufs));
+            gi++;
+          }
         }
-        umma_commit(empty(s));  // the stage's tiles are free once these MMAs finish
-        if (c % kTcGroup == kTcGroup - 1 || c == chunks - 1) umma_commit(accfull(g & 1));
-        done = c + 1;
       }
-      umma_commit(accf);  // every MMA issued so far has completed when accf flips
-      if (*abort_flag || done < chunks) bar_drain(accf, 0);
+      // Every MMA issued has completed when accf flips (waited for on every
+      // path, so that no commit is left to arrive after the CTA exits).
+      umma_commit(accf);
+      bar_drain(accf, 0);
     }
     __syncwarp();
-  } else {
-    // Warps 2-5: split each Y tile into hi (in place) and lo; add each
-    // accumulation group's result into registers (this warp's TMEM lane
-    // quarter: 32 amplitudes, one per thread, all walks); store at the end.
+  } else if (warp < 6) {
+    // Warps 2-5: split each Y tile into hi (in place) and lo.
     const int ct = threadIdx.x - 64;  // 0..127
-    const int q = warp & 3;
-    float acc[kTcMaxN];
-#pragma unroll
-    for (int j = 0; j < kTcMaxN; j++) acc[j] = 0.0f;
+    int it = 0;
     bool ok = true;
-    int gread = 0;  // next group to add
-    auto read_group = [&](int g) -> bool {
-      if (!bar_wait(accfull(g & 1), (g >> 1) & 1, abort_flag, p.err)) return false;
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const unsigned base = tmem + ((unsigned)(32 * q) << 16) + (unsigned)((g & 1) * kTcM);
-#pragma unroll
-      for (int c0 = 0; c0 < kTcMaxN; c0 += 8) {
-        if (c0 < p.Np) {
-          unsigned r[8];
-          asm volatile(
-              "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-              : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
-                "=r"(r[6]), "=r"(r[7])
-              : "r"(base + (unsigned)c0)
-              : "memory");
-          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-          for (int j = 0; j < 8; j++) acc[c0 + j] = __fadd_rn(acc[c0 + j], __uint_as_float(r[j]));
-        }
-      }
-      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-      bar_arrive(accfree(g & 1));
-      return true;
-    };
-    for (int c = 0; c < chunks && ok; c++) {
-      const int s = c % kTcStages;
-      if (!bar_wait(full(s), (c / kTcStages) & 1, abort_flag, p.err)) {
-        ok = false;
-        break;
-      }
-      float4* a = reinterpret_cast<float4*>(smem + s * kTcStage);
-      float4* alo = reinterpret_cast<float4*>(smem + s * kTcStage + kTcATile);
-#pragma unroll 4
-      for (int e = ct; e < (int)(kTcATile / 16); e += 128) {
-        const float4 v = a[e];
-        float4 hi, lo;
-        split_tf32(v.x, hi.x, lo.x);
-        split_tf32(v.y, hi.y, lo.y);
-        split_tf32(v.z, hi.z, lo.z);
-        split_tf32(v.w, hi.w, lo.w);
-        a[e] = hi;
-        alo[e] = lo;
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      bar_arrive(conv(s));
-      // After the last chunk of group g, add group g - 1 (its MMAs were
-      // issued a group ago), which frees its buffer for group g + 1.
-      const int g = c / kTcGroup;
-      if ((c % kTcGroup == kTcGroup - 1 || c == chunks - 1) && g >= 1 && gread == g - 1) {
-        if (!read_group(gread)) {
+    for (int t = blockIdx.x; t < p.tiles && ok; t += gridDim.x) {
+      const int chunks = p.chunks[t & 1];
+      for (int c = 0; c < chunks; c++, it++) {
+        const int s = it % kTcStages;
+        if (!bar_wait(full(s), (it / kTcStages) & 1, abort_flag, p.err)) {
           ok = false;
           break;
         }
-        gread++;
+        float4* a = reinterpret_cast<float4*>(smem + s * kTcStage);
+        float4* alo = reinterpret_cast<float4*>(smem + s * kTcStage + kTcATile);
+#pragma unroll 4
+        for (int e = ct; e < (int)(kTcATile / 16); e += 128) {
+          const float4 v = a[e];
+          float4 hi, lo;
+          split_tf32(v.x, hi.x, lo.x);
+          split_tf32(v.y, hi.y, lo.y);
+          split_tf32(v.z, hi.z, lo.z);
+          split_tf32(v.w, hi.w, lo.w);
+          a[e] = hi;
+          alo[e] = lo;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        bar_arrive(conv(s));
       }
     }
-    while (ok && gread < groups) {
-      if (!read_group(gread)) ok = false;
-      gread++;
-    }
-    if (ok && !*abort_flag) {
-      const size_t N = (size_t)1 << p.n;
+  } else {
+    // Warps 6-9: add each accumulation group's result into FP32 registers
+    // with round-to-nearest (this warp's TMEM lane quarter: 32 amplitudes,
+    // one per thread, all walks), then store the tile's planar outputs (a
+    // store covers 32 consecutive amplitudes of one walk).
+    const int q = warp & 3;
+    const size_t N = (size_t)1 << p.n;
+    int gi = 0;
+    bool ok = true;
+    for (int t = blockIdx.x; t < p.tiles && ok; t += gridDim.x) {
+      const int h = t & 1, m0 = (t >> 1) * kTcAmps;
+      const int groups = (p.chunks[h] + kTcGroup - 1) / kTcGroup;
+      float acc[kTcMaxN];
+#pragma unroll
+      for (int j = 0; j < kTcMaxN; j++) acc[j] = 0.0f;
+      for (int g = 0; g < groups; g++, gi++) {
+        const int b = gi % kTcBufs;
+        if (!bar_wait(accfull(b), (gi / kTcBufs) & 1, abort_flag, p.err)) {
+          ok = false;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const unsigned base = tmem + ((unsigned)(32 * q) << 16) + (unsigned)(b * kTcMaxN);
+#pragma unroll
+        for (int c0 = 0; c0 < kTcMaxN; c0 += 32) {
+          if (c0 < p.Np) {
+            unsigned r[32];
+            tmem_ld32(base + (unsigned)c0, r);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < 32; j++)
+              acc[c0 + j] = __fadd_rn(acc[c0 + j], __uint_as_float(r[j]));
+          }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        bar_arrive(accfree(b));
+      }
+      if (!ok || *abort_flag) break;
       float* out = p.out + (size_t)h * p.out_walks * N;
       const size_t amp = (size_t)m0 + 32 * q + lane;
 #pragma unroll
@@ -455,7 +499,7 @@ bool make_map(CUtensorMap* m, const float* base, unsigned long long inner,
 }
 
 std::mutex g_tc_mu;
-std::map<int, bool> g_tc_optin;  // per device: the kernel's shared-memory opt-in is made
+std::map<int, int> g_tc_sms;  // per device: SM count, once the shared-memory opt-in is made
 
 }  // namespace
 
@@ -491,23 +535,31 @@ cudaError_t launch_s2_gemm_tc_raw(const float* Y, const int rows[2], const float
   a.walks = walks;
   a.out_walks = out_walks;
   a.Np = Np;
+  a.tiles = (int)(2 * (N / kTcAmps));
   for (int h = 0; h < 2; h++) {
     a.chunks[h] = (rows[h] + kTcBK - 1) / kTcBK;
     a.crow[h] = 2 * h * Np;
   }
+  int sms = 0;
   {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     std::lock_guard<std::mutex> lk(g_tc_mu);
-    if (!g_tc_optin[dev]) {
+    int& known = g_tc_sms[dev];
+    if (known <= 0) {
       e = cudaFuncSetAttribute(s2_gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)kTcSmem);
       if (e != cudaSuccess) return e;
-      g_tc_optin[dev] = true;
+      int count = 0;
+      e = cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return e;
+      known = count;
     }
+    sms = known;
   }
-  const dim3 grid((unsigned)(N / kTcAmps), 2);
+  // Persistent: one CTA per SM (its shared memory admits no second one).
+  const unsigned grid = (unsigned)(a.tiles < sms ? a.tiles : sms);
   s2_gemm_tc_kernel<<<grid, kTcThreads, kTcSmem, stream>>>(mY0, mY1, mC, a);
   return cudaGetLastError();
 }
