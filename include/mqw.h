@@ -311,16 +311,19 @@ mqw_status mqw_pass_timing(mqw_ctx* ctx, int precision, int n, int reps,
                            double* us_per_launch, double* us_per_walk_pass,
                            int* walks_per_launch, int* lanes);
 /* The same for the real chain pass (FP32 shared-basis chains: 20 B per
- * amplitude), one chain per launch with the tuned tile of n, on the lanes a
- * plan runs its one-chain-per-launch chains on (4 from n = 19,
- * MQW_CHAIN_LANES if set, else the tuned walk lanes): `reps` passes per
- * lane on zero-filled vectors, captured in a CUDA graph as a plan's
- * pipeline is, the second replay timed with CUDA events on the context's
- * stream; us_per_pass = elapsed / (reps * lanes) (the launch-to-launch time
- * with `lanes` in flight). Tiles spread over a cluster are
- * MQW_ERR_UNSUPPORTED (the chains never use them). */
-mqw_status mqw_chain_pass_timing(mqw_ctx* ctx, int n, int reps, double* us_per_pass,
-                                 int* lanes, int* tile_log);
+ * amplitude), with the tuned tile of n and the plan's launches of the
+ * product-basis chains: 8 chains per launch at n = 17-18 (MQW_CHAIN_BATCH
+ * if set) on the tuned walk lanes, else one chain per launch on 4 lanes from
+ * n = 19 (MQW_CHAIN_LANES if set) or the tuned walk lanes below (at n <= 16
+ * a plan runs whole chains per launch instead; this times their passes
+ * launched one by one). `reps` launches per lane on zero-filled vectors,
+ * captured in a CUDA graph as a plan's pipeline is, the second replay timed
+ * with CUDA events on the context's stream; us_per_launch = elapsed /
+ * (reps * lanes) (the launch-to-launch time with `lanes` in flight), each
+ * launch one pass of `chains_per_launch` chains. Tiles spread over a
+ * cluster are MQW_ERR_UNSUPPORTED (the chains never use them). */
+mqw_status mqw_chain_pass_timing(mqw_ctx* ctx, int n, int reps, double* us_per_launch,
+                                 int* lanes, int* tile_log, int* chains_per_launch);
 
 /* ---- learned stage schedule (no counterpart in the reference) ---------- */
 /* Building blocks of the MLP that proposes per-stage (gamma, t) multipliers

@@ -155,7 +155,7 @@ def _bind(L):
         "mqw_clenshaw_noalloc": (i, [i, i, i, _vp, _vp, f, f, _vp, _vp, _vp]),
         "mqw_grid_shape_for": (i, [_vp, i, i, _P(GridShape)]),
         "mqw_pass_timing": (i, [_vp, i, i, i, _P(d), _P(d), _P(i), _P(i)]),
-        "mqw_chain_pass_timing": (i, [_vp, i, i, _P(d), _P(i), _P(i)]),
+        "mqw_chain_pass_timing": (i, [_vp, i, i, _P(d), _P(i), _P(i), _P(i)]),
         "mqw_diag_moments": (i, [_vp, i, _P(d), _P(d), _P(DiagInfo)]),
         "mqw_selftest_wait_timeout": (i, [_vp]),
         "mqw_measure_peaks": (i, [_vp, _P(TierPeaks)]),
@@ -389,13 +389,15 @@ class Context:
 
     def chain_pass_timing(self, n: int, reps: int = 64) -> dict:
         """Device time of the real chain pass alone (mqw_chain_pass_timing):
-        microseconds per pass, launch-to-launch with the tuned lanes in
-        flight, one chain per launch."""
-        us, ln, tl = ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+        microseconds per launch, launch-to-launch with the plan's chain lanes
+        in flight, each launch one pass of `walks_per_launch` chains (the
+        plan's chains per launch at this n)."""
+        us, ln, tl, cp = ctypes.c_double(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _check(self.h, lib().mqw_chain_pass_timing(self.h, n, reps, ctypes.byref(us),
-                                                   ctypes.byref(ln), ctypes.byref(tl)))
+                                                   ctypes.byref(ln), ctypes.byref(tl),
+                                                   ctypes.byref(cp)))
         return {"us_per_launch": us.value, "lanes": ln.value, "tile_log": tl.value,
-                "walks_per_launch": 1, "reps": reps}
+                "walks_per_launch": cp.value, "reps": reps}
 
     def multiqw(self, n: int, m: int, filename: str, start: int = 0, problems: int = 2000,
                 out_dir: str | None = None, print_: bool = True):

@@ -2261,14 +2261,16 @@ mqw_status mqw_pass_timing(mqw_ctx* ctx, int precision, int n, int reps,
   return MQW_OK;
 }
 
-mqw_status mqw_chain_pass_timing(mqw_ctx* ctx, int n, int reps, double* us_per_pass,
-                                 int* lanes_out, int* tile_log) {
+mqw_status mqw_chain_pass_timing(mqw_ctx* ctx, int n, int reps, double* us_per_launch,
+                                 int* lanes_out, int* tile_log, int* chains_per_launch) {
   mqw_status st = check_ctx(ctx);
   if (st != MQW_OK) return st;
   if (n < 6 || n > kMaxN || reps < 1 || reps > 100000)
     return fail(ctx, MQW_ERR_INVALID, "mqw_chain_pass_timing: bad arguments");
-  // The plan's shape for this n: its tuned tile, and the lanes its
-  // one-chain-per-launch product-basis chains run on (kChainLanes from
+  // The plan's shape for this n: its tuned tile; the product-basis chains'
+  // launches (B chains per per-term launch where the plan batches them:
+  // 8 at n = 17-18, MQW_CHAIN_BATCH if set; one elsewhere) and their lanes
+  // (batches: the tuned walk lanes; one chain per launch: kChainLanes from
   // n = 19, MQW_CHAIN_LANES if set, else the tuned walk lanes).
   GridShape want, gs;
   want.group = want.lanes = 0;
@@ -2278,19 +2280,50 @@ mqw_status mqw_chain_pass_timing(mqw_ctx* ctx, int n, int reps, double* us_per_p
                                      std::max(0, gs.tma), gs.cl < 0 ? 0 : 1);
   if (geo.C != 0)
     return fail(ctx, MQW_ERR_UNSUPPORTED, "mqw_chain_pass_timing: cluster-spanning tiles");
+  const char* be = getenv("MQW_CHAIN_BATCH");
+  const int B = chain_tile_log(0, n) > 0
+                    ? 1
+                    : std::min(kMaxChainBatch, std::max(1, be ? atoi(be) : (n <= 18 ? 8 : 1)));
   const char* env = getenv("MQW_CHAIN_LANES");
-  int lanes = env ? atoi(env) : (n >= 19 ? kChainLanes : gs.lanes);
+  int lanes = B > 1 ? gs.lanes : env ? atoi(env) : (n >= 19 ? kChainLanes : gs.lanes);
   lanes = std::max(1, std::min(lanes, kMaxStreams - 1));
   const size_t N = (size_t)1 << n;
-  // per lane: two chain vectors (alternating b_{r+1} / b_r) and P; then D
+  // per chain: its two output slots (each 2N: pass j writes b_r at
+  // out_base[j & 1] + (j >> 1) N) and P, or for a single-chain launch two
+  // vectors (alternating b_{r+1} / b_r) and P; then D
+  const size_t per_chain = B > 1 ? 5 * N : 3 * N;
   CK(ctx->ensure_lanes(lanes));
-  const size_t bytes = ((size_t)lanes * 3 + 1) * N * sizeof(float);
+  const size_t bytes = ((size_t)lanes * B * per_chain + N) * sizeof(float);
   CK(ctx->grow(ctx->state, bytes));
   cudaStream_t s0 = ctx->stream;
   CK(cudaMemsetAsync(ctx->state.p, 0, bytes, s0));
   float* base = ctx->state.as<float>();
-  const float* hp = base + (size_t)lanes * 3 * N;
+  const float* hp = base + (size_t)lanes * B * per_chain;
   auto issue = [&](int j, int lane) -> cudaError_t {
+    cudaStream_t st = lane == 0 ? s0 : ctx->lane_stream[lane];
+    if (B > 1) {
+      // passes j = 2, 3, 2, 3, ... of a batch (both tilings, b_{r+1} read
+      // from the other slot), as the plan's per-term batch launches
+      RealChainBatch rb{};
+      RealChainParams& rp = rb.p;
+      rp.n = n;
+      rp.L = geo.L;
+      rp.a = geo.a;
+      rp.start_uniform = 1;
+      rp.psi0 = 1.0f;
+      rp.hp = hp;
+      rp.gamma = 1.0f;
+      rp.scale = 64.0f;
+      rp.K = 4;
+      rp.R = 4;
+      rp.out_stride = (long long)N;
+      rb.chains = B;
+      for (int c = 0; c < B; c++) {
+        float* v = base + ((size_t)lane * B + c) * per_chain;
+        rb.chain[c] = RealChainDesc{nullptr, v + 4 * N, {v, v + 2 * N}};
+      }
+      return launch_real_batch(rb, 2 + (j & 1), st);
+    }
     float* v = base + (size_t)lane * 3 * N;
     RealChainParams rp{};
     rp.n = n;
@@ -2305,7 +2338,7 @@ mqw_status mqw_chain_pass_timing(mqw_ctx* ctx, int n, int reps, double* us_per_p
     rp.hp = hp;
     rp.gamma = 1.0f;
     rp.scale = 64.0f;
-    return launch_real_pass(rp, lane == 0 ? s0 : ctx->lane_stream[lane]);
+    return launch_real_pass(rp, st);
   };
   CK(ctx->fork(s0, lanes));
   for (int j = 0; j < 4; j++)
@@ -2346,9 +2379,10 @@ mqw_status mqw_chain_pass_timing(mqw_ctx* ctx, int n, int reps, double* us_per_p
   CK(e);
   st = take_device_error(ctx);
   if (st != MQW_OK) return st;
-  if (us_per_pass) *us_per_pass = 1000.0 * ms / ((double)reps * lanes);
+  if (us_per_launch) *us_per_launch = 1000.0 * ms / ((double)reps * lanes);
   if (lanes_out) *lanes_out = lanes;
   if (tile_log) *tile_log = geo.L;
+  if (chains_per_launch) *chains_per_launch = B;
   return MQW_OK;
 }
 

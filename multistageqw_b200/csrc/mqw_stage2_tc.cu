@@ -115,25 +115,34 @@ __device__ __forceinline__ void bar_expect_tx(unsigned bar, unsigned bytes) {
                : "memory");
 }
 // Waits for phase `parity` of `bar`; false when the CTA is aborting or the
-// wait ran out of time (which starts the abort).
+// wait ran out of time (which starts the abort). The clock and the abort
+// flag are read every 64 polls only: hundreds of polling threads reading
+// %globaltimer on every poll saturate the SM's XU pipe, which the working
+// warps share.
 __device__ __forceinline__ bool bar_wait(unsigned bar, unsigned parity, volatile int* abort_flag,
                                          unsigned* err) {
+  if (bar_try(bar, parity)) return true;
   const unsigned long long t0 = gtime();
-  while (!bar_try(bar, parity)) {
-    if (*abort_flag) return false;
-    if (gtime() - t0 > kTcWaitNs) {
-      *abort_flag = 1;
-      if (err) atomicOr(err, 2u);
-      return false;
+  for (unsigned i = 1;; i++) {
+    if (bar_try(bar, parity)) return true;
+    if ((i & 63u) == 0) {
+      if (*abort_flag) return false;
+      if (gtime() - t0 > kTcWaitNs) {
+        *abort_flag = 1;
+        if (err) atomicOr(err, 2u);
+        return false;
+      }
     }
   }
-  return true;
 }
 // The same without the abort flag, for the teardown's drains.
 __device__ __forceinline__ void bar_drain(unsigned bar, unsigned parity) {
+  if (bar_try(bar, parity)) return;
   const unsigned long long t0 = gtime();
-  while (!bar_try(bar, parity))
-    if (gtime() - t0 > kTcWaitNs) return;
+  for (unsigned i = 1;; i++) {
+    if (bar_try(bar, parity)) return;
+    if ((i & 63u) == 0 && gtime() - t0 > kTcWaitNs) return;
+  }
 }
 __device__ __forceinline__ void tma_load_2d(unsigned dst, const CUtensorMap* map, int x, int y,
                                             unsigned bar) {
