@@ -71,7 +71,9 @@ DRAM_BYTES_PER_TERM_AMP = {"sk_n20_m4": 29.40e6 / 2**20, "adam_sk20n_m4": 29.40e
 # amplitude (read b_{r+1}, b_{r+2} and D, write b_r) and cold-cache DRAM
 # bytes per amplitude of one launch from an ncu capture, keyed by workload.
 CHAIN_BYTES_PER_AMP = 16
-CHAIN_DRAM_BYTES_PER_AMP: dict = {}
+# profiles/real_pass_kernel_sk_n20_m4.md: 12.63 MB read, 0 written per
+# launch of 2^20 amplitudes (the read set b_{r+1}, P, D).
+CHAIN_DRAM_BYTES_PER_AMP = {"sk_n20_m4": 12.62592e6 / 2**20, "adam_sk20n_m4": 12.62592e6 / 2**20}
 # Host memory the CPU legs may use at once (all worker processes together).
 CPU_MEM_BUDGET = 24 << 30
 
