@@ -965,11 +965,16 @@ __global__ void mean_kernel(const double* p_sample, const int* p_off,
 // 2^LT floats. 256 threads, P in registers, D staged by cp.async, two
 // exchange tiles (b_{r+1}'s and b_r's) so that no barrier separates the
 // last read of one from the first write of the other.
-template <int LT> struct RealShape {
+template <int LT, int TB = 256> struct RealShape {
   static constexpr int kPairs = 1 << (LT - 1);
-  static constexpr int kThreads = kPairs < 256 ? kPairs : 256;
+  static constexpr int kThreads = kPairs < TB ? kPairs : TB;
   static constexpr int kRP = kPairs / kThreads;
-  static constexpr int kLogT = kThreads >= 256 ? 8 : kThreads >= 128 ? 7 : kThreads >= 64 ? 6 : 5;
+  static constexpr int kLogT = kThreads >= 1024  ? 10
+                               : kThreads >= 512 ? 9
+                               : kThreads >= 256 ? 8
+                               : kThreads >= 128 ? 7
+                               : kThreads >= 64  ? 6
+                                                 : 5;
   static constexpr size_t smem() { return (size_t)kPairs * (2 * 8 + 8); }
 };
 
@@ -1020,13 +1025,13 @@ __device__ __forceinline__ unsigned long long f2u(float2 f) {
 // on the CTA's tile `bx`. `half_finish` / `half_start`: the term this pass
 // finishes / starts uses a = 1/onenorm instead of 2/onenorm (a chain of
 // first-kind vectors T_j v: T_1 = H~ v).
-template <int LT>
+template <int LT, int TB = 256>
 __device__ __forceinline__ void real_tile(const RealChainParams& p, const int tiling,
                                           const bool first, const float* bin_, float* bout_,
                                           float* part_, const float* start_, const unsigned bx,
                                           const bool half_finish = false,
                                           const bool half_start = false) {
-  using S = RealShape<LT>;
+  using S = RealShape<LT, TB>;
   constexpr int RP = S::kRP, LOGT = S::kLogT, T = S::kThreads;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned long long* sx1 = reinterpret_cast<unsigned long long*>(smem_raw);  // b_{r+1}
@@ -1119,10 +1124,12 @@ __device__ __forceinline__ void real_tile(const RealChainParams& p, const int ti
 }
 
 // One real pass (p.tiling, p.first, p.bin -> p.bout); blockIdx.x is the tile.
-template <int LT>
-__global__ void __launch_bounds__(RealShape<LT>::kThreads) real_pass_kernel(RealChainParams p) {
-  real_tile<LT>(p, p.tiling, p.first != 0, p.bin, p.bout, p.part, p.start, blockIdx.x,
-                p.half_finish != 0, p.half_start != 0);
+// TB caps the CTA's threads (128 to 1024; see real_threads).
+template <int LT, int TB = 256>
+__global__ void __launch_bounds__(RealShape<LT, TB>::kThreads)
+    real_pass_kernel(RealChainParams p) {
+  real_tile<LT, TB>(p, p.tiling, p.first != 0, p.bin, p.bout, p.part, p.start, blockIdx.x,
+                    p.half_finish != 0, p.half_start != 0);
 }
 
 // Chain launch of whole real chains (small n, no axis read from global
@@ -1151,8 +1158,8 @@ __global__ void __launch_bounds__(RealShape<LT>::kThreads) real_chain_kernel(Rea
 // the chain (its start vector, partial P and outputs from b.chain[]),
 // blockIdx.x the tile. Axes in neither tiling are read from global memory as
 // in real_pass_kernel (b_{r+1} and b_r are different vectors).
-template <int LT>
-__global__ void __launch_bounds__(RealShape<LT>::kThreads)
+template <int LT, int TB = 256>
+__global__ void __launch_bounds__(RealShape<LT, TB>::kThreads)
     real_batch_kernel(RealChainBatch b, int j) {
   const RealChainParams& p = b.p;
   const RealChainDesc& c = b.chain[blockIdx.y];
@@ -1160,7 +1167,7 @@ __global__ void __launch_bounds__(RealShape<LT>::kThreads)
   const float* bin =
       j > 0 ? c.out_base[(j - 1) & 1] + (size_t)((j - 1) >> 1) * (size_t)p.out_stride : nullptr;
   float* bout = c.out_base[j & 1] + (size_t)(j >> 1) * (size_t)p.out_stride;
-  real_tile<LT>(p, (r & 1) ? 2 : 1, j == 0, bin, bout, c.part, c.start, blockIdx.x,
+  real_tile<LT, TB>(p, (r & 1) ? 2 : 1, j == 0, bin, bout, c.part, c.start, blockIdx.x,
                 p.tbasis && j == 1, p.tbasis && j == 0);
 }
 
@@ -1621,14 +1628,40 @@ cudaError_t launch_unit_eloc_real(float* v, int n, const DiagOut* diag, cudaStre
 }
 
 namespace {
+// CTA threads of the per-pass real chain launches (real_pass_kernel,
+// real_batch_kernel) for tile log LT: 128 (eight pairs per thread, two
+// shared-memory axes) up to 2^11 tiles, 256 above — measured per launch:
+// 8-chain batches at n = 18 (2^11 tiles) 6.38 against 6.84 us, single
+// chains at n = 20 (2^12 tiles) 3.41 against 3.95 us; 512 and 1024 threads
+// (more warps, more shared-memory axes) were slower at both. The order of
+// every partner sum is the same in all of them, so the results are too.
+// MQW_REAL_THREADS (128, 256, 512, 1024) fixes it; read once.
+int real_threads(int LT) {
+  static const int t = [] {
+    const char* e = getenv("MQW_REAL_THREADS");
+    const int v = e ? atoi(e) : 0;
+    return v == 128 || v == 256 || v == 512 || v == 1024 ? v : 0;
+  }();
+  return t ? t : LT <= 11 ? 128 : 256;
+}
+template <int LT, int TB>
+cudaError_t launch_real_lt_tb(const RealChainParams& p, cudaStream_t stream) {
+  using S = RealShape<LT, TB>;
+  const size_t smem = S::smem();
+  cudaError_t e = ensure_smem_optin((const void*)real_pass_kernel<LT, TB>, smem, false);
+  if (e != cudaSuccess) return e;
+  real_pass_kernel<LT, TB>
+      <<<(unsigned)((size_t)1 << (p.n - LT)), S::kThreads, smem, stream>>>(p);
+  return cudaGetLastError();
+}
 template <int LT>
 cudaError_t launch_real_lt(const RealChainParams& p, cudaStream_t stream) {
-  using S = RealShape<LT>;
-  const size_t smem = S::smem();
-  cudaError_t e = ensure_smem_optin((const void*)real_pass_kernel<LT>, smem, false);
-  if (e != cudaSuccess) return e;
-  real_pass_kernel<LT><<<(unsigned)((size_t)1 << (p.n - LT)), S::kThreads, smem, stream>>>(p);
-  return cudaGetLastError();
+  switch (real_threads(LT)) {
+    case 128: return launch_real_lt_tb<LT, 128>(p, stream);
+    case 512: return launch_real_lt_tb<LT, 512>(p, stream);
+    case 1024: return launch_real_lt_tb<LT, 1024>(p, stream);
+    default: return launch_real_lt_tb<LT, 256>(p, stream);
+  }
 }
 }  // namespace
 
@@ -1679,15 +1712,24 @@ cudaError_t launch_real_chain(const RealChainBatch& b, cudaStream_t stream) {
 }
 
 namespace {
-template <int LT>
-cudaError_t launch_real_batch_lt(const RealChainBatch& b, int j, cudaStream_t stream) {
-  using S = RealShape<LT>;
+template <int LT, int TB>
+cudaError_t launch_real_batch_lt_tb(const RealChainBatch& b, int j, cudaStream_t stream) {
+  using S = RealShape<LT, TB>;
   const size_t smem = S::smem();
-  cudaError_t e = ensure_smem_optin((const void*)real_batch_kernel<LT>, smem, false);
+  cudaError_t e = ensure_smem_optin((const void*)real_batch_kernel<LT, TB>, smem, false);
   if (e != cudaSuccess) return e;
   const dim3 grid((unsigned)((size_t)1 << (b.p.n - LT)), (unsigned)b.chains);
-  real_batch_kernel<LT><<<grid, S::kThreads, smem, stream>>>(b, j);
+  real_batch_kernel<LT, TB><<<grid, S::kThreads, smem, stream>>>(b, j);
   return cudaGetLastError();
+}
+template <int LT>
+cudaError_t launch_real_batch_lt(const RealChainBatch& b, int j, cudaStream_t stream) {
+  switch (real_threads(LT)) {
+    case 128: return launch_real_batch_lt_tb<LT, 128>(b, j, stream);
+    case 512: return launch_real_batch_lt_tb<LT, 512>(b, j, stream);
+    case 1024: return launch_real_batch_lt_tb<LT, 1024>(b, j, stream);
+    default: return launch_real_batch_lt_tb<LT, 256>(b, j, stream);
+  }
 }
 }  // namespace
 
