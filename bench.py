@@ -697,10 +697,11 @@ def main():
     bytes_per_launch = per_amp * float(1 << n_dom) * pt["walks_per_launch"]
     achieved = bytes_per_launch / (pt["us_per_launch"] * 1e-6) / 1e9
     # Bound tier: the memory tier that holds the concurrent walks' (chains')
-    # working set (3 vectors and the 4 B diagonal per amplitude, per walk in
-    # flight): L2 (126 MB; the library's own L2 copy probe is the
-    # denominator) when it fits in 96 MB, else HBM (MEASURED_PEAKS.json).
-    ws = (3 * vec_bytes + 4) * float(1 << n_dom) * pt["walks_per_launch"] * pt["lanes"]
+    # working set (3 vectors per walk or chain in flight, and the instance's
+    # 4 B diagonal, which they share): L2 (126 MB; the library's own L2 copy
+    # probe is the denominator) when it fits in 96 MB, else HBM
+    # (MEASURED_PEAKS.json).
+    ws = (3 * vec_bytes * pt["walks_per_launch"] * pt["lanes"] + 4) * float(1 << n_dom)
     l2_resident = ws <= 96e6 and tiers is not None
     if l2_resident:
         bound, peak, peak_src = "l2", tiers["l2_copy_gbs"], "l2_copy_gbs of the library's own probe"
