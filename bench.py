@@ -74,6 +74,11 @@ CHAIN_BYTES_PER_AMP = 16
 # profiles/real_pass_kernel_sk_n20_m4.md: 12.63 MB read, 0 written per
 # launch of 2^20 amplitudes (the read set b_{r+1}, P, D).
 CHAIN_DRAM_BYTES_PER_AMP = {"sk_n20_m4": 12.62592e6 / 2**20, "adam_sk20n_m4": 12.62592e6 / 2**20}
+# L1 data-pipe (LSU) wavefronts of one n = 20 chain launch (2^12 tiles, 256
+# threads), the mean of a tiling-1 and a tiling-2 launch (705 028 and
+# 869 270, profiles/real_pass_kernel_sk_n20_m4.md); the pipe takes one
+# wavefront per cycle per SM.
+CHAIN_L1_WAVEFRONTS_PER_AMP = {20: 787149.0 / 2**20}
 # Host memory the CPU legs may use at once (all worker processes together).
 CPU_MEM_BUDGET = 24 << 30
 
@@ -745,6 +750,20 @@ def main():
             (pt["us_per_launch"] * 1e-6) / 1e12
         roofline["fp32_flops"] = {"per_term_amp": 2 * n_dom + 8, "achieved_tflops": ex_tf,
                                   "peak_tflops": peak_tf, "frac": ex_tf / peak_tf}
+    # The chain pass's binding resource, the SM's L1 data pipe: its
+    # wavefronts per launch (ncu) over the launch-to-launch time's cycles on
+    # all SMs (one wavefront per cycle per SM, at the median sampled clock).
+    wf = CHAIN_L1_WAVEFRONTS_PER_AMP.get(n_dom) if chain_dom and pt["walks_per_launch"] == 1 else None
+    if wf:
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        mhz = float((clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0)
+        per_launch = wf * float(1 << n_dom)
+        roofline["l1_pipe"] = {
+            "wavefronts_per_launch": per_launch, "sm_mhz": mhz, "sms": sms,
+            "frac": per_launch / (pt["us_per_launch"] * 1e-6 * mhz * 1e6 * sms),
+            "note": "L1 data-pipe (LSU: shared memory, shuffles, global) wavefronts of one "
+                    "launch from ncu over the launch-to-launch cycles of all SMs at one "
+                    "wavefront per cycle per SM"}
     if tiers:
         roofline["tiers_gbs"] = {k: round(v, 1) for k, v in tiers.items()}
         roofline["frac_of_hbm"] = achieved / pk["hbm_gbs"]

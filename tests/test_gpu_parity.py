@@ -823,3 +823,80 @@ def test_last_two_stage_basis_matches_recurrence(ctx, orc, mqw, monkeypatch, n, 
     assert a_on == 0 < a_off  # no walk ran a recurrence
     r64 = ctx.run_problems(n, 4, raw, samples=samples, precision="fp64", graph=0)
     assert abs(float(np.mean(on)) - r64["p"][0]) <= 1e-5
+
+
+@pytest.mark.parametrize("n,m,samples", [(20, 4, 24), (19, 3, 20)])
+def test_chain_lanes_do_not_change_results(ctx, orc, mqw, monkeypatch, n, m, samples):
+    """The one-chain-per-launch product-basis chains run on four lanes from
+    n = 19 (their slots packed in the state buffer); the lanes only reorder
+    independent chains, so one lane (MQW_CHAIN_LANES=1) and seven give every
+    per-sample P bit for bit as the default."""
+    raw = orc.sk_instances(n, 1, 9100 + n)
+    monkeypatch.setenv("MQW_STAGE2_BASIS", "1")
+
+    def run(lanes):
+        if lanes:
+            monkeypatch.setenv("MQW_CHAIN_LANES", str(lanes))
+        else:
+            monkeypatch.delenv("MQW_CHAIN_LANES", raising=False)
+        plan = mqw.Plan(ctx, n, m, raw, samples=samples, graph=0)
+        plan.execute()
+        out = plan.results(per_sample=True)["p_sample"]
+        plan.close()
+        return out
+
+    ref = run(None)
+    for lanes in (1, 7):
+        assert np.array_equal(run(lanes), ref), lanes
+
+
+_THREADS_SCRIPT = r"""
+import sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+import multistageqw_b200 as M
+out = []
+for n, m in ((20, 4), (18, 3)):
+    raw = M.sk_instances(n, 1, 9300 + n)
+    ctx = M.Context(0)
+    plan = M.Plan(ctx, n, m, raw, samples=12, graph=0)
+    plan.execute()
+    out.append(plan.results(per_sample=True)["p_sample"])
+    plan.close()
+    ctx.close()
+np.save(sys.argv[2], np.concatenate([o.ravel() for o in out]))
+"""
+
+
+def test_real_pass_thread_counts_give_identical_results(mqw, tmp_path):
+    """The real chain passes with 128, 256 (the defaults by tile) and 512
+    or 1024 threads per CTA (MQW_REAL_THREADS, read once per process, so
+    each runs in its own process) sum every partner in the same order:
+    per-sample P bit for bit alike at n = 20 (2^12 tiles) and n = 18
+    (2^11 tiles, eight chains per launch)."""
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(mqw.__file__)))
+    script = tmp_path / "threads.py"
+    script.write_text(_THREADS_SCRIPT)
+    res = {}
+    for t in ("", "128", "256", "512", "1024"):
+        env = dict(os.environ)
+        env.pop("MQW_REAL_THREADS", None)
+        if t:
+            env["MQW_REAL_THREADS"] = t
+        out = tmp_path / f"p_{t or 'default'}.npy"
+        r = subprocess.run([sys.executable, str(script), root, str(out)], env=env,
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        res[t] = np.load(out)
+    for t, v in res.items():
+        assert np.array_equal(v, res[""]), t
+
+
+def test_chain_pass_timing_mirrors_the_plans_launches(ctx):
+    """mqw_chain_pass_timing launches what a plan launches: eight chains per
+    launch at n = 18, one per launch on four lanes at n = 20."""
+    t18 = ctx.chain_pass_timing(18, reps=8)
+    t20 = ctx.chain_pass_timing(20, reps=8)
+    assert t18["walks_per_launch"] == 8 and t18["us_per_launch"] > 0
+    assert t20["walks_per_launch"] == 1 and t20["lanes"] == 4 and t20["us_per_launch"] > 0
