@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define MQW_ABI_VERSION 2
+#define MQW_ABI_VERSION 3  /* 3: mqw_chain_pass_timing reports chains per launch */
 #define MQW_SAMPLES 100  /* time samples per stage, MultiQW.cpp:257 */
 #define MQW_MAX_N 30     /* 2^30 amplitudes; the reference overflows at n >= 31 (MultiQW.cpp:246) */
 #define MQW_MAX_M 64     /* stages per walk */

@@ -16,7 +16,7 @@ def test_exports_every_header_symbol(mqw):
     assert len(names) >= 20
     for name in names:
         assert hasattr(L, name), name
-    assert L.mqw_abi_version() == 2
+    assert L.mqw_abi_version() == 3
 
 
 def test_cli_binary_links(mqw):
